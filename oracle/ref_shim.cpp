@@ -1,0 +1,182 @@
+// extern "C" harness around the UNMODIFIED reference per-slice routines.
+//
+// Test infrastructure only: compiled together with the reference sources
+// (read in place from the reference tree by oracle/Makefile) into
+// oracle/_ref/libverbref.so (plain build) and oracle/_ref/libverbref_lu.so
+// (built with -DLU_CACHING).  It exists so that the CPU restatement in
+// oracle/verb_oracle.c and the golden fixtures can be checked against the
+// reference itself, and so bench.py can time the reference CPU path.
+//
+// Each entry copies plain row-major arrays into the reference's Matrix1D /
+// Matrix2D containers, calls the reference routine, and copies the result
+// back.  Layouts follow the reference: a local (V,K) slice is [V][K], a
+// convection slice is [P][R].
+#include <cstring>
+#include <tuple>
+
+#include "BoundaryConditionType.hpp"
+#include "Convection_1D_ULTIMATE_QUICKEST6.h"
+#include "Convection_2D.h"
+#include "DataAssimilation.h"
+#include "DataAssimilationDiffusion.h"
+#include "Diffusion_1D.h"
+#include "Diffusion_2D.h"
+#include "Matrix.h"
+#include "MatrixSolver.h"
+
+namespace {
+
+Matrix1D<double> vec(const double* p, long n)
+{
+    Matrix1D<double> m(static_cast<size_t>(n));
+    std::memcpy(&m[0], p, sizeof(double) * static_cast<size_t>(n));
+    return m;
+}
+
+Matrix2D<double> mat(const double* p, long n1, long n2)
+{
+    Matrix2D<double> m(static_cast<size_t>(n1), static_cast<size_t>(n2));
+    std::memcpy(m[0], p, sizeof(double) * static_cast<size_t>(n1 * n2));
+    return m;
+}
+
+BoundaryConditionType bct(int t) { return static_cast<BoundaryConditionType>(t); }
+
+}  // namespace
+
+extern "C" {
+
+// src/MatrixSolver.cpp:689 tridag
+int ref_tridag(double* a, double* b, double* c, double* r, double* u, long n)
+{
+    return tridag(a, b, c, r, u, static_cast<size_t>(n)) ? 0 : 1;
+}
+
+// src/Diffusion_1D.cpp:43 Diffusion_1D (psd updated in place)
+int ref_diffusion_1d(double* psd, const double* x, int n, double lbc, double ubc, int lbc_t,
+                     int ubc_t, const double* D, const double* G, const double* S,
+                     const double* loss, double dt)
+{
+    Matrix1D<double> f = vec(psd, n);
+    Diffusion_1D(f, vec(x, n), n, lbc, ubc, bct(lbc_t), bct(ubc_t), vec(D, n), vec(G, n),
+                 vec(S, n), vec(loss, n), dt);
+    std::memcpy(psd, &f[0], sizeof(double) * n);
+    return 0;
+}
+
+// src/Diffusion_1D.cpp:91 getCalculationMatrix1DDiffusion: the three diagonals of A,
+// diag(B) and C of one radial line.
+int ref_radial_matrix(const double* x, int n, double lbc, double ubc, int lbc_t, int ubc_t,
+                      const double* D, const double* G, const double* S, const double* loss,
+                      double dt, double* a_lo, double* a_d, double* a_up, double* b_d,
+                      double* c_d)
+{
+    auto m = getCalculationMatrix1DDiffusion(vec(x, n), n, lbc, ubc, bct(lbc_t), bct(ubc_t),
+                                             vec(D, n), vec(G, n), vec(S, n), vec(loss, n), dt);
+    CalculationMatrix& A = std::get<0>(m);
+    CalculationMatrix& B = std::get<1>(m);
+    CalculationMatrix& C = std::get<2>(m);
+    for (int i = 0; i < n; i++) {
+        a_lo[i] = A[-1][i];
+        a_d[i] = A[0][i];
+        a_up[i] = A[1][i];
+        b_d[i] = B[0][i];
+        c_d[i] = C[0][i];
+    }
+    return 0;
+}
+
+#ifdef LU_CACHING
+// src/Diffusion_2D.cpp:20 Diffusion_2D, LU_CACHING form: lu (ldab*n doubles) and
+// ipiv (n longs, 1-based LAPACK pivots) are the caller-owned cache slot.
+int ref_diffusion_2d_lu(double* psd, const double* x, const double* y, int nx, int ny,
+                        const double* xl, const double* xu, const double* yl, const double* yu,
+                        int xl_t, int xu_t, int yl_t, int yu_t, const double* Dxx,
+                        const double* Dyy, const double* Dxy, const double* Dyx, const double* G,
+                        const double* S, const double* loss, double dt, double sub_dt,
+                        double* lu, long* ipiv, int recompute)
+{
+    Matrix2D<double> f = mat(psd, nx, ny);
+    Diffusion_2D(f, mat(x, nx, ny), mat(y, nx, ny), nx, ny, vec(xl, ny), vec(xu, ny), vec(yl, nx),
+                 vec(yu, nx), bct(xl_t), bct(xu_t), bct(yl_t), bct(yu_t), mat(Dxx, nx, ny),
+                 mat(Dyy, nx, ny), mat(Dxy, nx, ny), mat(Dyx, nx, ny), mat(G, nx, ny),
+                 mat(S, nx, ny), mat(loss, nx, ny), dt, sub_dt, lu, ipiv, recompute != 0);
+    std::memcpy(psd, f[0], sizeof(double) * nx * ny);
+    return 0;
+}
+#else
+// src/Diffusion_2D.cpp:32 Diffusion_2D, plain form (factor + solve every call).
+int ref_diffusion_2d(double* psd, const double* x, const double* y, int nx, int ny,
+                     const double* xl, const double* xu, const double* yl, const double* yu,
+                     int xl_t, int xu_t, int yl_t, int yu_t, const double* Dxx, const double* Dyy,
+                     const double* Dxy, const double* Dyx, const double* G, const double* S,
+                     const double* loss, double dt, double sub_dt)
+{
+    Matrix2D<double> f = mat(psd, nx, ny);
+    Diffusion_2D(f, mat(x, nx, ny), mat(y, nx, ny), nx, ny, vec(xl, ny), vec(xu, ny), vec(yl, nx),
+                 vec(yu, nx), bct(xl_t), bct(xu_t), bct(yl_t), bct(yu_t), mat(Dxx, nx, ny),
+                 mat(Dyy, nx, ny), mat(Dxy, nx, ny), mat(Dyx, nx, ny), mat(G, nx, ny),
+                 mat(S, nx, ny), mat(loss, nx, ny), dt, sub_dt);
+    std::memcpy(psd, f[0], sizeof(double) * nx * ny);
+    return 0;
+}
+#endif
+
+// src/Convection_1D_ULTIMATE_QUICKEST6.cpp:22 (psd updated in place)
+int ref_convection_1d(double* psd, const double* x, int n, double lbc, double ubc, int lbc_t,
+                      int ubc_t, const double* ux, double dt)
+{
+    Matrix1D<double> f = vec(psd, n);
+    Convection_1D_ULTIMATE_QUICKEST6(f, vec(x, n), n, lbc, ubc, bct(lbc_t), bct(ubc_t), vec(ux, n),
+                                     dt);
+    std::memcpy(psd, &f[0], sizeof(double) * n);
+    return 0;
+}
+
+// src/Convection_2D.cpp:36 Convection_2D on one [P][R] slice (psd updated in place)
+int ref_convection_2d(double* psd, const double* P, const double* R, int nP, int nR,
+                      const double* pl, const double* pu, const double* rl, const double* ru,
+                      int pl_t, int pu_t, int rl_t, int ru_t, const double* VP, const double* VR,
+                      const double* S, const double* loss, const double* G, double dt)
+{
+    Matrix2D<double> f = mat(psd, nP, nR);
+    Convection_2D(f, mat(P, nP, nR), mat(R, nP, nR), nP, nR, vec(pl, nR), vec(pu, nR), vec(rl, nP),
+                  vec(ru, nP), bct(pl_t), bct(pu_t), bct(rl_t), bct(ru_t), mat(VP, nP, nR),
+                  mat(VR, nP, nR), mat(S, nP, nR), mat(loss, nP, nR), mat(G, nP, nR), dt);
+    std::memcpy(psd, f[0], sizeof(double) * nP * nR);
+    return 0;
+}
+
+// src/DataAssimilationDiffusion.cpp:151 runKalmanFilterDiffusion1D for one radial column.
+// forecast[n] and Pa[n*n] are updated in place; F[n*n] receives the model matrix and
+// Pf[n*n] the forecast covariance.
+int ref_kf_diffusion_1d(double* forecast, double* Pa, double* F, double* Pf, const double* R,
+                        const double* DLL, const double* G, int n, double lbc, double ubc,
+                        int lbc_t, int ubc_t, const double* obs, double dt, double model_error,
+                        double obs_error)
+{
+    Matrix1D<double> f = vec(forecast, n);
+    Matrix2D<double> pa = mat(Pa, n, n);
+    Matrix2D<double> model(static_cast<size_t>(n), static_cast<size_t>(n));
+    model = 0;
+    data_assimilation::Parameters prm{};
+    prm.runDataAssimilation = true;
+    prm.useLog = false;
+    prm.timeStep = dt;
+    prm.modelError = model_error;
+    prm.observationError = obs_error;
+    try {
+        auto dbg = data_assimilation::runKalmanFilterDiffusion1D(
+            f, pa, model, vec(R, n), vec(DLL, n), vec(G, n), lbc, ubc, bct(lbc_t), bct(ubc_t),
+            vec(obs, n), dt, prm);
+        std::memcpy(Pf, dbg.a_priori_err_cov[0], sizeof(double) * n * n);
+    } catch (...) {
+        return 2;  // the reference throws on NaN after the update (DataAssimilation.cpp:62-67)
+    }
+    std::memcpy(forecast, &f[0], sizeof(double) * n);
+    std::memcpy(Pa, pa[0], sizeof(double) * n * n);
+    std::memcpy(F, model[0], sizeof(double) * n * n);
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,914 @@
+/*
+ * CPU restatement of the VERB-4D operator-split step -- TEST INFRASTRUCTURE.
+ *
+ * This file is the oracle: tests/, the smoke check and bench.py's CPU
+ * baseline leg are its only users.  It is never part of the product path.
+ * Each function restates a reference routine (file:line within the reference
+ * project) with the reference's evaluation order; it is compiled with
+ * -ffp-contract=off so no FMA contraction changes rounding.
+ *
+ * Parity pin: tests/test_oracle.py compares every routine here with the
+ * reference routines compiled from source (oracle/_ref, see oracle/Makefile)
+ * and with the committed golden fixtures in tests/golden/.
+ */
+#include "verb_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define GST 5 /* ghost cells per side, src/Convection_1D_ULTIMATE_QUICKEST6.cpp:18 */
+
+/* ------------------------------------------------------------------------ */
+/* Thomas algorithm: src/MatrixSolver.cpp:689-720 (tridag).                   */
+int orc_tridag(const double* a, const double* b, const double* c, const double* r, double* u,
+               long n)
+{
+    double* gam = (double*)malloc(sizeof(double) * (size_t)n);
+    double bet;
+    u[0] = r[0] / (bet = b[0]);
+    for (long j = 1; j <= n - 1; j++) {
+        gam[j] = c[j - 1] / bet;
+        bet = b[j] - a[j] * gam[j];
+        u[j] = (r[j] - a[j] * u[j - 1]) / bet;
+    }
+    for (long j = n - 1; j >= 1; j--) u[j - 1] -= gam[j] * u[j];
+    free(gam);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* src/MatrixSolver.cpp:353-404 SecondDerivativeApproximation_1D, adding into the
+ * tridiagonal row ix (lo = A[-1], d = A[0], up = A[+1]).                      */
+static void sda_1d(double* lo, double* d, double* up, int ix, int dx1, int dx2, const double* x,
+                   const double* D, const double* G, double mult)
+{
+    double* diag[3] = {lo, d, up};
+    double dh1 = x[ix] - x[ix + dx1];
+    double dh21 = x[ix] - x[ix + dx2];
+    double dh22 = x[ix + dx1] - x[ix + dx1 + dx2];
+    double cp = mult / G[ix] / dh1;
+    diag[1][ix] += +cp / dh21 * D[ix] * G[ix];
+    diag[1 + dx2][ix] += -cp / dh21 * D[ix] * G[ix];
+    diag[1 + dx1][ix] += -cp / dh22 * D[ix + dx1] * G[ix + dx1];
+    diag[1 + dx1 + dx2][ix] += +cp / dh22 * D[ix + dx1] * G[ix + dx1];
+}
+
+/* src/Diffusion_1D.cpp:91-184 getCalculationMatrix1DDiffusion. */
+int orc_radial_matrix(const double* x, int n, double lbc, double ubc, int lbc_t, int ubc_t,
+                      const double* D, const double* G, const double* S, const double* loss,
+                      double dt, double* a_lo, double* a_d, double* a_up, double* b_d,
+                      double* c_d)
+{
+    for (int i = 0; i < n; i++) a_lo[i] = a_d[i] = a_up[i] = b_d[i] = c_d[i] = 0.0;
+    for (int ix = 0; ix < n; ix++) {
+        if (ix == 0 && n >= 3) {
+            c_d[ix] = lbc;
+            double dh = x[ix + 1] - x[ix];
+            if (lbc_t == ORC_BC_CONSTANT_VALUE) {
+                a_d[ix] = 1;
+                a_up[ix] = 0;
+            } else if (lbc_t == ORC_BC_CONSTANT_DERIVATIVE) {
+                a_d[ix] = 1 / dh;
+                a_up[ix] = -1 / dh;
+            } else {
+                return 4;
+            }
+        } else if (ix == n - 1 && n >= 3) {
+            c_d[ix] = ubc;
+            double dh = x[ix] - x[ix - 1];
+            if (ubc_t == ORC_BC_CONSTANT_VALUE) {
+                a_d[ix] = 1;
+                a_lo[ix] = 0;
+            } else if (ubc_t == ORC_BC_CONSTANT_DERIVATIVE) {
+                a_d[ix] = 1 / dh;
+                a_lo[ix] = -1 / dh;
+            } else {
+                return 4;
+            }
+        } else {
+            a_d[ix] += 1.0 / dt;
+            b_d[ix] += 1.0 / dt;
+            c_d[ix] += S[ix];
+            a_d[ix] -= loss[ix];
+            if (n >= 3) {
+                sda_1d(a_lo, a_d, a_up, ix, -1, +1, x, D, G, -0.5);
+                sda_1d(a_lo, a_d, a_up, ix, +1, -1, x, D, G, -0.5);
+            }
+        }
+    }
+    return 0;
+}
+
+/* src/Diffusion_1D.cpp:43-88 Diffusion_1D: RHS = B f + C, then tridag. */
+int orc_diffusion_1d(double* psd, const double* x, int n, double lbc, double ubc, int lbc_t,
+                     int ubc_t, const double* D, const double* G, const double* S,
+                     const double* loss, double dt)
+{
+    double* w = (double*)malloc(sizeof(double) * 6 * (size_t)n);
+    double *lo = w, *d = w + n, *up = w + 2 * n, *bd = w + 3 * n, *cd = w + 4 * n,
+           *rhs = w + 5 * n;
+    int st = orc_radial_matrix(x, n, lbc, ubc, lbc_t, ubc_t, D, G, S, loss, dt, lo, d, up, bd, cd);
+    if (st == 0) {
+        for (int i = 0; i < n; i++) {
+            rhs[i] = cd[i];
+            rhs[i] += bd[i] * psd[i];
+        }
+        orc_tridag(lo, d, up, rhs, psd, n);
+    }
+    free(w);
+    return st;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Local 2-D operator.  Diagonal slot of offset (dx,dy), dx,dy in {-1,0,1}. */
+static inline int dslot(int dx, int dy) { return (dy + 1) * 3 + (dx + 1); }
+
+/* src/MatrixSolver.cpp:413-426 GetDerivativeVector_2D, by code:
+ * 0 x_left, 1 x_right, 2 y_left, 3 y_right. */
+static void dvec(int code, int* dx, int* dy)
+{
+    if (code == 0) *dx = -1;
+    else if (code == 1) *dx = 1;
+    else if (code == 2) *dy = -1;
+    else *dy = 1;
+}
+
+/* src/MatrixSolver.cpp:439-494 SecondDerivativeApproximation_2D for row (ix,iy). */
+static void sda_2d(double* diag, int nx, int ny, int ix, int iy, int first, int second,
+                   const double* x, const double* y, const double* D, const double* G,
+                   double mult)
+{
+    int dx1 = 0, dy1 = 0, dx2 = 0, dy2 = 0;
+    dvec(first, &dx1, &dy1);
+    dvec(second, &dx2, &dy2);
+    long in = (long)iy * nx + ix;
+    long n = (long)nx * ny;
+#define P2(a, b) ((long)(a) * ny + (b))
+    double dh1 = (x[P2(ix, iy)] + y[P2(ix, iy)]) -
+                 (x[P2(ix + dx1, iy + dy1)] + y[P2(ix + dx1, iy + dy1)]);
+    double dh21 = (x[P2(ix, iy)] + y[P2(ix, iy)]) -
+                  (x[P2(ix + dx2, iy + dy2)] + y[P2(ix + dx2, iy + dy2)]);
+    double dh22 = (x[P2(ix + dx1, iy + dy1)] + y[P2(ix + dx1, iy + dy1)]) -
+                  (x[P2(ix + dx1 + dx2, iy + dy1 + dy2)] + y[P2(ix + dx1 + dx2, iy + dy1 + dy2)]);
+    double cp = mult / G[P2(ix, iy)] / dh1;
+    diag[dslot(0, 0) * n + in] += +cp / dh21 * D[P2(ix, iy)] * G[P2(ix, iy)];
+    diag[dslot(dx2, dy2) * n + in] += -cp / dh21 * D[P2(ix, iy)] * G[P2(ix, iy)];
+    diag[dslot(dx1, dy1) * n + in] +=
+        -cp / dh22 * D[P2(ix + dx1, iy + dy1)] * G[P2(ix + dx1, iy + dy1)];
+    diag[dslot(dx1 + dx2, dy1 + dy2) * n + in] +=
+        +cp / dh22 * D[P2(ix + dx1, iy + dy1)] * G[P2(ix + dx1, iy + dy1)];
+#undef P2
+}
+
+/* One boundary row: src/MatrixSolver.cpp:118-213 AddBoundaries_2D. */
+static int bc_row(double* diag, long n, long in, int slot1, int type, double dh)
+{
+    if (type == ORC_BC_CONSTANT_VALUE) {
+        diag[dslot(0, 0) * n + in] = 1;
+        diag[slot1 * n + in] = 0;
+    } else if (type == ORC_BC_CONSTANT_DERIVATIVE) {
+        diag[dslot(0, 0) * n + in] = 1 / dh;
+        diag[slot1 * n + in] = -1 / dh;
+    } else {
+        return 4;
+    }
+    return 0;
+}
+
+/* src/Diffusion_2D.cpp:48-130 (assembly of matr_A, matr_B, matr_C; dt is the
+ * sub-step dt, already divided by the number of sub-steps). */
+int orc_local_matrix(const double* x, const double* y, int nx, int ny, const double* xl,
+                     const double* xu, const double* yl, const double* yu, int xl_t, int xu_t,
+                     int yl_t, int yu_t, const double* Dxx, const double* Dyy, const double* Dxy,
+                     const double* Dyx, const double* G, const double* S, const double* loss,
+                     double dt, double* diag, double* b_d, double* c_d)
+{
+    long n = (long)nx * ny;
+    memset(diag, 0, sizeof(double) * 9 * (size_t)n);
+    memset(b_d, 0, sizeof(double) * (size_t)n);
+    memset(c_d, 0, sizeof(double) * (size_t)n);
+    for (int ix = 0; ix < nx; ix++) {
+        for (int iy = 0; iy < ny; iy++) {
+            long in = (long)iy * nx + ix;
+            long p = (long)ix * ny + iy;
+            int st = 0;
+            if (ix == 0 && nx >= 3) {
+                c_d[in] = xl[iy];
+                st = bc_row(diag, n, in, dslot(1, 0), xl_t, x[p + ny] - x[p]);
+            } else if (ix == nx - 1 && nx >= 3) {
+                c_d[in] = xu[iy];
+                st = bc_row(diag, n, in, dslot(-1, 0), xu_t, x[p] - x[p - ny]);
+            } else if (iy == 0 && ny >= 3) {
+                c_d[in] = yl[ix];
+                st = bc_row(diag, n, in, dslot(0, 1), yl_t, y[p + 1] - y[p]);
+            } else if (iy == ny - 1 && ny >= 3) {
+                c_d[in] = yu[ix];
+                st = bc_row(diag, n, in, dslot(0, -1), yu_t, y[p] - y[p - 1]);
+            } else {
+                diag[dslot(0, 0) * n + in] += 1.0 / dt;
+                b_d[in] += 1.0 / dt;
+                c_d[in] += S[p];
+                diag[dslot(0, 0) * n + in] -= loss[p];
+                if (nx >= 3) {
+                    sda_2d(diag, nx, ny, ix, iy, 0, 1, x, y, Dxx, G, -0.5);
+                    sda_2d(diag, nx, ny, ix, iy, 1, 0, x, y, Dxx, G, -0.5);
+                }
+                if (ny >= 3) {
+                    sda_2d(diag, nx, ny, ix, iy, 2, 3, x, y, Dyy, G, -0.5);
+                    sda_2d(diag, nx, ny, ix, iy, 3, 2, x, y, Dyy, G, -0.5);
+                }
+                if (nx >= 3 && ny >= 3) {
+                    sda_2d(diag, nx, ny, ix, iy, 2, 1, x, y, Dxy, G, -0.25);
+                    sda_2d(diag, nx, ny, ix, iy, 3, 0, x, y, Dxy, G, -0.25);
+                    sda_2d(diag, nx, ny, ix, iy, 2, 0, x, y, Dxy, G, -0.25);
+                    sda_2d(diag, nx, ny, ix, iy, 3, 1, x, y, Dxy, G, -0.25);
+                    sda_2d(diag, nx, ny, ix, iy, 0, 3, x, y, Dyx, G, -0.25);
+                    sda_2d(diag, nx, ny, ix, iy, 1, 2, x, y, Dyx, G, -0.25);
+                    sda_2d(diag, nx, ny, ix, iy, 0, 2, x, y, Dyx, G, -0.25);
+                    sda_2d(diag, nx, ny, ix, iy, 1, 3, x, y, Dyx, G, -0.25);
+                }
+            }
+            if (st) return st;
+        }
+    }
+    return 0;
+}
+
+/* LAPACK band packing of src/MatrixSolver.cpp:253-269: ab[j*ldab + kl+ku+in-j]
+ * = A[in][j] with kl = ku = nx+1, ldab = 2kl+ku+1; ab zero-filled first. */
+void orc_band_pack(const double* diag, int nx, int ny, double* ab)
+{
+    long n = (long)nx * ny, kl = nx + 1, ku = nx + 1, ldab = 2 * kl + ku + 1;
+    memset(ab, 0, sizeof(double) * (size_t)(ldab * n));
+    for (long in = 0; in < n; in++) {
+        for (int dy = -1; dy <= 1; dy++) {
+            for (int dx = -1; dx <= 1; dx++) {
+                long off = (long)dy * nx + dx;
+                long j = in + off;
+                if (j >= 0 && j < n) ab[j * ldab + kl + ku + in - j] = diag[dslot(dx, dy) * n + in];
+            }
+        }
+    }
+}
+
+/* Banded LU with partial pivoting: restatement of LAPACK's published
+ * unblocked algorithm xGBTF2 (0-based; ipiv 0-based).  Returns info (0 ok,
+ * j+1 for an exactly zero pivot in column j). */
+long orc_gbtrf(long n, long kl, long ku, double* ab, long ldab, long* ipiv)
+{
+    long kv = ku + kl, info = 0, ju = 0;
+#define AB(i, j) ab[(i) + (j) * ldab]
+    for (long j = ku + 1; j < (kv < n ? kv : n); j++)
+        for (long i = kv - j; i < kl; i++) AB(i, j) = 0.0;
+    for (long j = 0; j < n; j++) {
+        if (j + kv < n)
+            for (long i = 0; i < kl; i++) AB(i, j + kv) = 0.0;
+        long km = kl < n - 1 - j ? kl : n - 1 - j;
+        long jp = 0;
+        double vmax = fabs(AB(kv, j));
+        for (long i = 1; i <= km; i++) {
+            double v = fabs(AB(kv + i, j));
+            if (v > vmax) {
+                vmax = v;
+                jp = i;
+            }
+        }
+        ipiv[j] = jp + j;
+        if (AB(kv + jp, j) != 0.0) {
+            long jmax = j + ku + jp < n - 1 ? j + ku + jp : n - 1;
+            if (jmax > ju) ju = jmax;
+            if (jp != 0)
+                for (long k = 0; k <= ju - j; k++) {
+                    double t = AB(kv + jp - k, j + k);
+                    AB(kv + jp - k, j + k) = AB(kv - k, j + k);
+                    AB(kv - k, j + k) = t;
+                }
+            if (km > 0) {
+                double r = 1.0 / AB(kv, j);
+                for (long i = 1; i <= km; i++) AB(kv + i, j) *= r;
+                for (long k = 1; k <= ju - j; k++) {
+                    double yk = AB(kv - k, j + k);
+                    if (yk != 0.0) {
+                        double temp = -yk;
+                        for (long i = 1; i <= km; i++) AB(kv + i - k, j + k) += AB(kv + i, j) * temp;
+                    }
+                }
+            }
+        } else if (info == 0) {
+            info = j + 1;
+        }
+    }
+#undef AB
+    return info;
+}
+
+/* Restatement of LAPACK xGBTRS ('N', one right-hand side) followed by the
+ * upper-triangular band solve xTBSV ('U','N','N'). */
+void orc_gbtrs(long n, long kl, long ku, const double* ab, long ldab, const long* ipiv, double* b)
+{
+    long kd = kl + ku;
+    if (kl > 0) {
+        for (long j = 0; j < n - 1; j++) {
+            long lm = kl < n - 1 - j ? kl : n - 1 - j;
+            long l = ipiv[j];
+            if (l != j) {
+                double t = b[l];
+                b[l] = b[j];
+                b[j] = t;
+            }
+            if (b[j] != 0.0) {
+                double temp = -b[j];
+                for (long i = 1; i <= lm; i++) b[j + i] += ab[kd + i + j * ldab] * temp;
+            }
+        }
+    }
+    for (long j = n - 1; j >= 0; j--) {
+        if (b[j] != 0.0) {
+            b[j] = b[j] / ab[kd + j * ldab];
+            double temp = b[j];
+            long i0 = j - kd > 0 ? j - kd : 0;
+            for (long i = j - 1; i >= i0; i--) b[i] = b[i] - temp * ab[kd + i - j + j * ldab];
+        }
+    }
+}
+
+/* src/Diffusion_2D.cpp:19-153 + src/MatrixSolver.cpp:223-340 (Lapack).
+ * psd is [nx][ny].  lu (ldab*n) / ipiv (n) are the LU_CACHING slot; with
+ * recompute == 0 the cached factors are reused. */
+int orc_diffusion_2d(double* psd, const double* x, const double* y, int nx, int ny,
+                     const double* xl, const double* xu, const double* yl, const double* yu,
+                     int xl_t, int xu_t, int yl_t, int yu_t, const double* Dxx, const double* Dyy,
+                     const double* Dxy, const double* Dyx, const double* G, const double* S,
+                     const double* loss, double dt, double sub_dt, double* lu, long* ipiv,
+                     int recompute)
+{
+    int num_substeps = (int)(dt / sub_dt);
+    if (num_substeps < 1) num_substeps = 1;
+    dt /= num_substeps;
+    long n = (long)nx * ny, kl = nx + 1, ku = nx + 1, ldab = 2 * kl + ku + 1;
+    double* diag = (double*)malloc(sizeof(double) * 11 * (size_t)n);
+    double *bd = diag + 9 * n, *cd = diag + 10 * n;
+    double* rhs = (double*)malloc(sizeof(double) * (size_t)n);
+    int st = orc_local_matrix(x, y, nx, ny, xl, xu, yl, yu, xl_t, xu_t, yl_t, yu_t, Dxx, Dyy, Dxy,
+                              Dyx, G, S, loss, dt, diag, bd, cd);
+    if (st == 0 && recompute) {
+        orc_band_pack(diag, nx, ny, lu);
+        if (orc_gbtrf(n, kl, ku, lu, ldab, ipiv) != 0) st = 1;
+    }
+    if (st == 0) {
+        for (int ix = 0; ix < nx; ix++)
+            for (int iy = 0; iy < ny; iy++) rhs[(long)iy * nx + ix] = psd[(long)ix * ny + iy];
+        for (int s = 0; s < num_substeps; s++) {
+            for (long i = 0; i < n; i++) rhs[i] = rhs[i] * bd[i];
+            for (long i = 0; i < n; i++) rhs[i] = rhs[i] + cd[i];
+            orc_gbtrs(n, kl, ku, lu, ldab, ipiv, rhs);
+        }
+        for (int ix = 0; ix < nx; ix++)
+            for (int iy = 0; iy < ny; iy++) psd[(long)ix * ny + iy] = rhs[(long)iy * nx + ix];
+    }
+    free(rhs);
+    free(diag);
+    return st;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Ghost cells of one sweep, src/Convection_1D_ULTIMATE_QUICKEST6.cpp:92-143
+ * (pass 1) and 281-330 (pass 2): `lowsrc` feeds the low ghosts and `highsrc`
+ * the high ones (pass 2 takes the low ones from the pre-step PSD). */
+static void ghosts(double* t, const double* lowsrc, const double* highsrc, const double* x, int n,
+                   double lbc, double ubc, int lbc_t, int ubc_t)
+{
+    int ig;
+    if (lbc_t == ORC_BC_PERIODIC) {
+        for (ig = 1; ig <= GST; ig++) t[GST - ig] = lowsrc[(n - 1) - ig];
+    } else if (lbc_t == ORC_BC_CONSTANT_VALUE) {
+        for (ig = 1; ig <= GST; ig++) t[GST - ig] = lbc;
+    } else if (lbc_t == ORC_BC_CONSTANT_DERIVATIVE) {
+        double dx = x[1] - x[0];
+        t[GST - 1] = lowsrc[0] - lbc * dx;
+        for (ig = 1; ig <= GST; ig++) t[GST - ig] = t[GST - ig + 1] - lbc * dx;
+    }
+    if (ubc_t == ORC_BC_PERIODIC) {
+        for (ig = 1; ig <= GST; ig++) t[GST + (n - 1) + ig] = highsrc[ig];
+    } else if (ubc_t == ORC_BC_CONSTANT_VALUE) {
+        for (ig = 1; ig <= GST; ig++) t[GST + (n - 1) + ig] = ubc;
+    } else if (ubc_t == ORC_BC_CONSTANT_DERIVATIVE) {
+        double dx = x[n - 1] - x[n - 2];
+        t[GST + (n - 1) + 1] = highsrc[n - 1] + ubc * dx;
+        for (ig = 1; ig <= GST; ig++) t[GST + (n - 1) + ig] = t[GST + (n - 1) + ig - 1] + ubc * dx;
+    }
+}
+
+/* Boundary rewrite after a pass, src/Convection_1D_ULTIMATE_QUICKEST6.cpp:257-272. */
+static void bc_rewrite(double* f, int n, double lbc, double ubc, int lbc_t, int ubc_t)
+{
+    if (lbc_t == ORC_BC_PERIODIC) f[n - 1] = f[0];
+    else if (lbc_t == ORC_BC_CONSTANT_VALUE) f[0] = lbc;
+    else if (lbc_t == ORC_BC_CONSTANT_DERIVATIVE) f[0] = f[1];
+    if (ubc_t == ORC_BC_CONSTANT_VALUE) f[n - 1] = ubc;
+    else if (ubc_t == ORC_BC_CONSTANT_DERIVATIVE) f[n - 1] = f[n - 2];
+}
+
+/* 9th-order ULTIMATE-QUICKEST face value, src/...QUICKEST6.cpp:162-241, from the
+ * upwind U[1..4], centre C, downwind D[1..5] values. */
+static double quickest_face(const double* U, double C, const double* D, double cr)
+{
+    const double cs = cr * cr;
+    const double ca = fabs(cr);
+    double f = 0.5 * (C + D[1]);
+    const double d1 = C - D[1];
+    f += 0.5 * ca * d1;
+    const double D2 = (U[1] - C - D[1] + D[2]) / 2;
+    const double d3 = U[1] - 3 * C + 3 * D[1] - D[2];
+    f += (cs - 1) / 6.0 * (D2 + ca / 4 * d3);
+    const double D4 = (U[2] - 3 * U[1] + 2 * C + 2 * D[1] - 3 * D[2] + D[3]) / 2;
+    const double d5 = U[2] - 5 * U[1] + 10 * C - 10 * D[1] + 5 * D[2] - D[3];
+    f += (cs - 1) * (cs - 4) / 120.0 * (D4 + ca / 6 * d5);
+    const double D6 =
+        (U[3] - 5 * U[2] + 9 * U[1] - 5 * C - 5 * D[1] + 9 * D[2] - 5 * D[3] + D[4]) / 2;
+    const double d7 = U[3] - 7 * U[2] + 21 * U[1] - 35 * C + 35 * D[1] - 21 * D[2] + 7 * D[3] - D[4];
+    f += (cs - 1) * (cs - 4) * (cs - 9) / 5040.0 * (D6 + ca / 8 * d7);
+    const double D8 = (U[4] - 7 * U[3] + 20 * U[2] - 28 * U[1] + 14 * C + 14 * D[1] - 28 * D[2] +
+                       20 * D[3] - 7 * D[4] + D[5]) /
+                      2;
+    const double d9 = U[4] - 9 * U[3] + 36 * U[2] - 84 * U[1] + 126 * C - 126 * D[1] + 84 * D[2] -
+                      36 * D[3] + 9 * D[4] - D[5];
+    f += (cs - 1) * (cs - 4) * (cs - 9) * (cs - 16) / 362880.0 * (D8 + d9 / 2);
+    return f;
+}
+
+/* src/Convection_1D_ULTIMATE_QUICKEST6.cpp:22-482.  Returns 3 when the Courant
+ * check fails (the reference exits there, :48-52). */
+int orc_convection_1d(double* psd, const double* x, int n, double lbc, double ubc, int lbc_t,
+                      int ubc_t, const double* ux, double dt_total)
+{
+    double dx = x[1] - x[0];
+    double ux_max = -INFINITY;
+    for (int i = 0; i < n; i++) {
+        double a = fabs(ux[i]);
+        ux_max = (ux_max > a) ? ux_max : a;
+    }
+    double steps_double = dt_total * ux_max / dx / 1.0;
+    int num_steps = (steps_double <= 1) ? 1 : (int)ceil(steps_double);
+    double dt = dt_total / num_steps;
+    int m = n + 2 * GST;
+    double* w = (double*)malloc(sizeof(double) * (size_t)(5 * n + 2 * m));
+    double *cour = w, *unl = w + n, *faces = w + 2 * n, *t = w + 3 * n, *ut = t + m;
+    for (int i = 0; i < n; i++) cour[i] = ux[i] / dx * dt;
+    if (fabs(ux_max / dx * dt) > 1) {
+        free(w);
+        return 3;
+    }
+    for (int it = 0; it < num_steps; it++) {
+        for (int ix = 0; ix <= n - 1; ix++) t[GST + ix] = psd[ix];
+        ghosts(t, psd, psd, x, n, lbc, ubc, lbc_t, ubc_t);
+        double fl = 0.0, cl = 0.0, cr = 0.0;
+        for (int ix = 0; ix <= n - 1; ix++) {
+            if (ix == 0) {
+                if (lbc_t == ORC_BC_PERIODIC) cr = (cour[n - 2] + cour[0]) / 2;
+                else continue;
+            } else {
+                cr = (cour[ix - 1] + cour[ix]) / 2;
+            }
+            double U[5], D[6], C;
+            int ig;
+            if (cr >= 0) {
+                for (ig = 1; ig <= 4; ig++) U[ig] = t[GST + ix - 1 - ig];
+                C = t[GST + ix - 1];
+                for (ig = 1; ig <= 5; ig++) D[ig] = t[GST + ix - 1 + ig];
+            } else {
+                for (ig = 1; ig <= 5; ig++) D[ig] = t[GST + ix - ig];
+                C = t[GST + ix];
+                for (ig = 1; ig <= 4; ig++) U[ig] = t[GST + ix + ig];
+            }
+            double f = quickest_face(U, C, D, cr);
+            if (ix > 0) unl[ix - 1] = psd[ix - 1] - (cr * f - cl * fl);
+            faces[ix] = f;
+            fl = f;
+            cl = cr;
+        }
+        bc_rewrite(unl, n, lbc, ubc, lbc_t, ubc_t);
+
+        for (int ix = 0; ix <= n - 1; ix++) ut[GST + ix] = unl[ix];
+        ghosts(ut, psd, unl, x, n, lbc, ubc, lbc_t, ubc_t);
+        fl = 0.0;
+        cl = 0.0;
+        cr = 0.0;
+        for (int ix = 0; ix <= n - 1; ix++) {
+            if (ix == 0) {
+                if (lbc_t == ORC_BC_PERIODIC) cr = (cour[n - 2] + cour[0]) / 2;
+                else continue;
+            } else {
+                cr = (cour[ix - 1] + cour[ix]) / 2;
+            }
+            const double ca = fabs(cr);
+            double ou, od, oc, UU[5], UD[6], UC;
+            int ig;
+            if (cr >= 0) {
+                for (ig = 1; ig <= 4; ig++) UU[ig] = ut[GST + ix - 1 - ig];
+                ou = t[GST + ix - 2];
+                UC = ut[GST + ix - 1];
+                oc = t[GST + ix - 1];
+                for (ig = 1; ig <= 5; ig++) UD[ig] = ut[GST + ix - 1 + ig];
+                od = t[GST + ix];
+            } else {
+                for (ig = 1; ig <= 5; ig++) UD[ig] = ut[GST + ix - ig];
+                od = t[GST + ix - 1];
+                UC = ut[GST + ix];
+                oc = t[GST + ix];
+                for (ig = 1; ig <= 4; ig++) UU[ig] = ut[GST + ix + ig];
+                ou = t[GST + ix + 1];
+            }
+            const double DEL = od - ou;
+            const double CURV = od - 2 * oc + ou;
+            const double ADEL = fabs(DEL);
+            const double ACURV = fabs(CURV);
+            const double dif1 = UD[2] - UD[3];
+            const double dif2 = UD[1] - UD[2];
+            const double dif3 = UC - UD[1];
+            const double dif4 = UU[1] - UC;
+            const double dif5 = UU[2] - UU[1];
+            const double dif6 = UU[3] - UU[2];
+            const int peak_dw =
+                dif1 > 0 && dif2 > 0 && dif3 < 0 && dif4 < 0 && dif2 < dif1 && dif3 > dif4;
+            const int peak_c =
+                dif2 > 0 && dif3 > 0 && dif4 < 0 && dif5 < 0 && dif3 < dif2 && dif4 > dif5;
+            const int peak_u =
+                dif3 > 0 && dif4 > 0 && dif5 < 0 && dif6 < 0 && dif4 < dif3 && dif5 > dif6;
+            double f = faces[ix];
+            if (!(peak_dw || peak_c || peak_u)) {
+                if (ACURV >= ADEL) {
+                    f = oc;
+                } else if (ca > 1e-31) {
+                    const double ref = ou + (oc - ou) / ca;
+                    if (DEL > 0) {
+                        f = fmax(f, oc);
+                        f = fmin(f, fmin(ref, od));
+                    } else if (DEL < 0) {
+                        f = fmin(f, oc);
+                        f = fmax(f, fmax(ref, od));
+                    }
+                }
+            }
+            if (ix > 0) psd[ix - 1] -= (cr * f - cl * fl);
+            fl = f;
+            cl = cr;
+        }
+        bc_rewrite(psd, n, lbc, ubc, lbc_t, ubc_t);
+    }
+    free(w);
+    return 0;
+}
+
+/* Matrix2D<T>::maxabs, src/Matrix.cpp:1699-1708. */
+static double maxabs2d(const double* a, long n)
+{
+    double tmp = 0;
+    for (long i = 0; i < n; i++) {
+        double c = fabs(a[i]);
+        tmp = (tmp < c) ? c : tmp;
+    }
+    return tmp;
+}
+
+/* src/Convection_2D.cpp:36-169 on one [P][R] slice.  *substeps receives the
+ * slice-level sub-step count (num_steps, :57-86). */
+int orc_convection_2d(double* psd, const double* P, const double* R, int nP, int nR,
+                      const double* pl, const double* pu, const double* rl, const double* ru,
+                      int pl_t, int pu_t, int rl_t, int ru_t, const double* VP, const double* VR,
+                      const double* S, const double* loss, const double* G, double dt_total,
+                      int* substeps)
+{
+    const double maxCourNum = 0.25;
+    long n = (long)nP * nR;
+    double nsP, nsR;
+    if (nP >= 3) {
+        double dP = P[1 * nR + 0] - P[0];
+        double d = (double)dt_total * maxabs2d(VP, n) / dP / maxCourNum;
+        nsP = d <= 1 ? 1 : ceil(d);
+    } else {
+        nsP = 1;
+    }
+    if (nR >= 3) {
+        double dR = R[1] - R[0];
+        double d = (double)dt_total * maxabs2d(VR, n) / dR / maxCourNum;
+        nsR = d <= 1 ? 1 : ceil(d);
+    } else {
+        nsR = 1;
+    }
+    double num_steps = (nsP < nsR) ? nsR : nsP;
+    double dt = dt_total / num_steps;
+    if (substeps) *substeps = (int)num_steps;
+    int mx = nP > nR ? nP : nR;
+    double* w = (double*)malloc(sizeof(double) * (size_t)(2 * n + 4 * mx));
+    double *lexp = w, *pg = w + n, *line = w + 2 * n, *xl = line + mx, *ul = xl + mx;
+    for (long i = 0; i < n; i++) lexp[i] = exp(loss[i] * dt);
+    int st = 0;
+    for (int it = 0; it < num_steps && st == 0; it++) {
+        if (nP >= 3) {
+            for (int iR = 0; iR < nR - 1 && st == 0; iR++) {
+                for (int iP = 0; iP < nP; iP++) {
+                    line[iP] = psd[(long)iP * nR + iR];
+                    xl[iP] = P[(long)iP * nR + iR];
+                    ul[iP] = VP[(long)iP * nR + iR];
+                }
+                st = orc_convection_1d(line, xl, nP, pl[iR], pu[iR], pl_t, pu_t, ul, dt);
+                for (int iP = 0; iP < nP; iP++) psd[(long)iP * nR + iR] = line[iP];
+            }
+        }
+        for (long i = 0; i < n; i++) pg[i] = psd[i] * G[i];
+        if (nR >= 3) {
+            for (int iP = 0; iP < nP && st == 0; iP++) {
+                const double* g = G + (long)iP * nR;
+                for (int iR = 0; iR < nR; iR++) {
+                    line[iR] = pg[(long)iP * nR + iR];
+                }
+                st = orc_convection_1d(line, R + (long)iP * nR, nR, rl[iP] * g[0], ru[iP] * g[nR - 1],
+                                       rl_t, ru_t, VR + (long)iP * nR, dt);
+                for (int iR = 0; iR < nR; iR++) psd[(long)iP * nR + iR] = line[iR] / g[iR];
+            }
+        }
+        for (long i = 0; i < n; i++) psd[i] = psd[i] * lexp[i];
+        for (int iP = 0; iP < nP; iP++)
+            for (int iR = 1; iR < nR - 1; iR++)
+                psd[(long)iP * nR + iR] = psd[(long)iP * nR + iR] + S[(long)iP * nR + iR] * dt;
+    }
+    free(w);
+    return st;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Dense helpers for the radial Kalman filter (row-major, plain loops). */
+static void mm(const double* A, const double* B, double* C, int m, int k, int n)
+{
+    for (int i = 0; i < m; i++)
+        for (int j = 0; j < n; j++) {
+            double s = 0;
+            for (int l = 0; l < k; l++) s += A[i * k + l] * B[l * n + j];
+            C[i * n + j] = s;
+        }
+}
+
+static void mm_bt(const double* A, const double* B, double* C, int m, int k, int n)
+{
+    for (int i = 0; i < m; i++)
+        for (int j = 0; j < n; j++) {
+            double s = 0;
+            for (int l = 0; l < k; l++) s += A[i * k + l] * B[j * k + l];
+            C[i * n + j] = s;
+        }
+}
+
+/* Solve X*A = B for X (A n x n, B m x n, result into B): the reference's
+ * trans_solve, src/MatrixOperations.cpp:761-790 (dgesv on the transposes).
+ * Gaussian elimination with partial pivoting on A^T. */
+static int trans_solve(const double* A, double* B, int n, int m)
+{
+    double* T = (double*)malloc(sizeof(double) * (size_t)n * n);
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++) T[i * n + j] = A[j * n + i];
+    int st = 0;
+    for (int k = 0; k < n && !st; k++) {
+        int p = k;
+        for (int i = k + 1; i < n; i++)
+            if (fabs(T[i * n + k]) > fabs(T[p * n + k])) p = i;
+        if (T[p * n + k] == 0.0) {
+            st = 1;
+            break;
+        }
+        if (p != k) {
+            for (int j = 0; j < n; j++) {
+                double t = T[k * n + j];
+                T[k * n + j] = T[p * n + j];
+                T[p * n + j] = t;
+            }
+            for (int r = 0; r < m; r++) {
+                double t = B[r * n + k];
+                B[r * n + k] = B[r * n + p];
+                B[r * n + p] = t;
+            }
+        }
+        for (int i = k + 1; i < n; i++) {
+            double l = T[i * n + k] / T[k * n + k];
+            T[i * n + k] = l;
+            for (int j = k + 1; j < n; j++) T[i * n + j] -= l * T[k * n + j];
+            for (int r = 0; r < m; r++) B[r * n + i] -= l * B[r * n + k];
+        }
+    }
+    for (int r = 0; r < m && !st; r++) {
+        double* b = B + (long)r * n;
+        for (int i = n - 1; i >= 0; i--) {
+            double s = b[i];
+            for (int j = i + 1; j < n; j++) s -= T[i * n + j] * b[j];
+            b[i] = s / T[i * n + i];
+        }
+    }
+    free(T);
+    return st;
+}
+
+/* src/DataAssimilationDiffusion.cpp:151-253 runKalmanFilterDiffusion1D with
+ * src/DataAssimilationHelper.cpp:174-198 (model matrix), :271-305
+ * (observation space) and src/DataAssimilation.cpp:18-77 (runKalmanFilter). */
+int orc_kf_diffusion_1d(double* forecast, double* Pa, double* F, double* Pf, const double* R,
+                        const double* DLL, const double* G, int n, double lbc, double ubc,
+                        int lbc_t, int ubc_t, const double* obs, double dt, double model_error,
+                        double obs_error)
+{
+    double* w = (double*)calloc((size_t)(8 * n + 6 * n * n), sizeof(double));
+    double *zero = w, *lo = w + n, *d = w + 2 * n, *up = w + 3 * n, *bd = w + 4 * n,
+           *cd = w + 5 * n, *corr = w + 7 * n;
+    double *A = w + 8 * n, *T1 = A + n * n, *KH = T1 + n * n, *T2 = KH + n * n;
+    int st = orc_radial_matrix(R, n, lbc, ubc, lbc_t, ubc_t, DLL, G, zero, zero, dt, lo, d, up,
+                               bd, cd);
+    if (st) {
+        free(w);
+        return st;
+    }
+    /* CalculationMatrix::toMatrix2D (src/Matrix.cpp:6558-6575 with
+     * get_matrix_indices 6495-6535): the last row's sub-diagonal is dropped. */
+    for (int i = 0; i < n; i++) {
+        A[i * n + i] = d[i];
+        if (i >= 1 && i <= n - 2) A[i * n + i - 1] = lo[i];
+        if (i <= n - 2) A[i * n + i + 1] = up[i];
+    }
+    memset(F, 0, sizeof(double) * (size_t)n * n);
+    for (int i = 0; i < n; i++) F[i * n + i] = bd[i];
+    if (trans_solve(A, F, n, n)) {
+        free(w);
+        return 1;
+    }
+    int m = 0;
+    for (int i = 0; i < n; i++)
+        if (isfinite(obs[i])) m++;
+    int mm_ = m > 0 ? m : 1;
+    double* H = (double*)calloc((size_t)mm_ * n, sizeof(double));
+    double* y = (double*)calloc((size_t)mm_, sizeof(double));
+    double* PfHt = (double*)calloc((size_t)n * mm_, sizeof(double));
+    double* Sm = (double*)calloc((size_t)mm_ * mm_, sizeof(double));
+    double* K = PfHt;
+    if (m > 0) {
+        int c = 0;
+        for (int i = 0; i < n; i++)
+            if (isfinite(obs[i])) {
+                y[c] = obs[i];
+                H[c * n + i] = 1.0;
+                c++;
+            }
+    }
+    double pmax = 0;
+    for (long i = 0; i < (long)n * n; i++) pmax = fabs(Pa[i]) > pmax ? fabs(Pa[i]) : pmax;
+    if (pmax == 0)
+        for (int i = 0; i < n; i++) Pa[i * n + i] = 5 * model_error;
+    mm(F, Pa, T1, n, n, n);
+    mm_bt(T1, F, Pf, n, n, n);
+    for (int i = 0; i < n; i++) Pf[i * n + i] += model_error;
+    mm_bt(Pf, H, PfHt, n, n, mm_);
+    mm(H, PfHt, Sm, mm_, n, mm_);
+    for (int i = 0; i < mm_; i++) Sm[i * mm_ + i] += obs_error;
+    st = trans_solve(Sm, K, mm_, n);
+    if (!st) {
+        for (int i = 0; i < mm_; i++) {
+            double s = 0;
+            for (int j = 0; j < n; j++) s += H[i * n + j] * forecast[j];
+            y[i] = y[i] - s;
+        }
+        for (int i = 0; i < n; i++) {
+            double s = 0;
+            for (int j = 0; j < mm_; j++) s += K[i * mm_ + j] * y[j];
+            corr[i] = s;
+        }
+        for (int i = 0; i < n; i++) forecast[i] += corr[i];
+        for (int i = 0; i < n; i++)
+            if (isnan(forecast[i])) st = 2;
+        mm(K, H, KH, n, mm_, n);
+        mm(KH, Pf, T2, n, n, n);
+        for (long i = 0; i < (long)n * n; i++) Pa[i] = Pf[i] - T2[i];
+    }
+    free(H);
+    free(y);
+    free(PfHt);
+    free(Sm);
+    free(w);
+    return st;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Whole step: src/VERB4D_Solver.cpp:747-753 (tensor check), 851-978
+ * (convection), 990-1070 (radial), 1081-1216 (local), 1218-1242 (negative
+ * count).  Returns the negative-point count, or -(status) on error. */
+long orc_step(orc_state* s, double dt, double sub_dt, int recompute_lu)
+{
+    const int P = s->P, R = s->R, V = s->V, K = s->K;
+    const long N = (long)P * R * V * K;
+#define I4(p, r, v, k) ((((long)(p) * R + (r)) * V + (v)) * K + (k))
+    double check = INFINITY;
+    for (long i = 0; i < N; i++) {
+        double c = s->DVV[i] * s->DKK[i] - s->DVK[i] * s->DVK[i];
+        check = c < check ? c : check;
+    }
+    if (check < 0) return -5;
+    if (s->positive_psd)
+        for (long i = 0; i < N; i++) s->psd[i] = s->psd[i] > 1e-21 ? s->psd[i] : 1e-21;
+
+    long mx = (long)(P * R > V * K ? P * R : V * K);
+    if (mx < 4 * (long)(R > P ? R : P)) mx = 4 * (long)(R > P ? R : P);
+    double* buf = (double*)malloc(sizeof(double) * (size_t)(20 * mx));
+    int st = 0;
+
+    if ((3 < P || 3 < R) && s->run_convection) {
+        double *f = buf, *pg = buf + mx, *rg = buf + 2 * mx, *vp = buf + 3 * mx, *vr = buf + 4 * mx,
+               *sr = buf + 5 * mx, *ls = buf + 6 * mx, *gg = buf + 7 * mx, *pl = buf + 8 * mx,
+               *pu = buf + 9 * mx, *rl = buf + 10 * mx, *ru = buf + 11 * mx;
+        for (int iV = V - 1; iV >= 0 && !st; iV--)
+            for (int iK = 0; iK < K && !st; iK++) {
+                for (int iP = 0; iP < P; iP++)
+                    for (int iR = 0; iR < R; iR++) {
+                        long q = (long)iP * R + iR, g = I4(iP, iR, iV, iK);
+                        f[q] = s->psd[g];
+                        pg[q] = s->Pg[g];
+                        rg[q] = s->Rg[g];
+                        vp[q] = s->VP[g];
+                        vr[q] = s->VR[g];
+                        sr[q] = s->S[g];
+                        ls[q] = s->loss_conv[g];
+                        gg[q] = s->G_conv[g];
+                    }
+                for (int iR = 0; iR < R; iR++) {
+                    pl[iR] = s->Pl[((long)iR * V + iV) * K + iK];
+                    pu[iR] = s->Pu[((long)iR * V + iV) * K + iK];
+                }
+                for (int iP = 0; iP < P; iP++) {
+                    rl[iP] = s->Rl[((long)iP * V + iV) * K + iK];
+                    ru[iP] = s->Ru[((long)iP * V + iV) * K + iK];
+                }
+                st = orc_convection_2d(f, pg, rg, P, R, pl, pu, rl, ru, s->Pl_t, s->Pu_t, s->Rl_t,
+                                       s->Ru_t, vp, vr, sr, ls, gg, dt, NULL);
+                for (int iP = 0; iP < P; iP++)
+                    for (int iR = 0; iR < R; iR++) s->psd[I4(iP, iR, iV, iK)] = f[(long)iP * R + iR];
+            }
+    }
+    if (s->positive_psd)
+        for (long i = 0; i < N; i++) s->psd[i] = s->psd[i] > 1e-21 ? s->psd[i] : 1e-21;
+
+    if (R >= 3 && s->run_radial && !st) {
+        double *f = buf, *lg = buf + mx, *dl = buf + 2 * mx, *sr = buf + 3 * mx, *gr = buf + 4 * mx,
+               *ls = buf + 5 * mx;
+        for (int iP = 0; iP < P && !st; iP++)
+            for (int iV = 0; iV < V && !st; iV++)
+                for (int iK = 0; iK < K && !st; iK++) {
+                    for (int iR = 0; iR < R; iR++) {
+                        long g = I4(iP, iR, iV, iK);
+                        f[iR] = s->psd[g];
+                        lg[iR] = s->Lg[g];
+                        dl[iR] = s->DLL[g];
+                        sr[iR] = s->S[g] * s->radial_sources;
+                        gr[iR] = s->G_radial[g];
+                        ls[iR] = s->loss_radial[g];
+                    }
+                    long b = ((long)iP * V + iV) * K + iK;
+                    st = orc_diffusion_1d(f, lg, R, s->Ll[b], s->Lu[b], s->Ll_t, s->Lu_t, dl, gr, sr,
+                                          ls, dt);
+                    for (int iR = 0; iR < R; iR++) s->psd[I4(iP, iR, iV, iK)] = f[iR];
+                }
+    }
+    if (s->positive_psd)
+        for (long i = 0; i < N; i++) s->psd[i] = s->psd[i] > 1e-21 ? s->psd[i] : 1e-21;
+
+    if (V >= 3 && K >= 3 && s->run_local && !st) {
+        long n = (long)V * K, ldab = 3 * (V + 1) + 1;
+        double* lu_tmp = s->lu ? NULL : (double*)malloc(sizeof(double) * (size_t)(ldab * n));
+        long* ip_tmp = s->lu ? NULL : (long*)malloc(sizeof(long) * (size_t)n);
+        double* sl = (double*)malloc(sizeof(double) * (size_t)n);
+        for (int iP = 0; iP < P && !st; iP++)
+            for (int iR = 0; iR < R && !st; iR++) {
+                if (!s->include_boundary && (iR == 0 || iR == R - 1)) continue;
+                long base = I4(iP, iR, 0, 0);
+                long pr = (long)iP * R + iR;
+                for (long i = 0; i < n; i++) sl[i] = s->S[base + i] * s->local_sources;
+                double* lu = s->lu ? s->lu + pr * ldab * n : lu_tmp;
+                long* ip = s->lu ? s->ipiv + pr * n : ip_tmp;
+                st = orc_diffusion_2d(s->psd + base, s->Vg + base, s->Kg + base, V, K, s->Vl + pr * K,
+                                      s->Vu + pr * K, s->Kl + pr * V, s->Ku + pr * V, s->Vl_t,
+                                      s->Vu_t, s->Kl_t, s->Ku_t, s->DVV + base, s->DKK + base,
+                                      s->DVK + base, s->DVK + base, s->G_local + base, sl,
+                                      s->loss_local + base, dt, sub_dt, lu, ip,
+                                      s->lu ? recompute_lu : 1);
+            }
+        free(sl);
+        free(lu_tmp);
+        free(ip_tmp);
+    }
+    free(buf);
+    if (st) return -st;
+    long neg = 0;
+    if (s->positive_psd) {
+        for (long i = 0; i < N; i++) s->psd[i] = s->psd[i] > 1e-21 ? s->psd[i] : 1e-21;
+    } else {
+        for (long i = 0; i < N; i++)
+            if (s->psd[i] < 0) neg++;
+    }
+    return neg;
+#undef I4
+}
