@@ -1,0 +1,192 @@
+/*
+ * verb4d_b200 -- B200 (sm_100a) implementation of the VERB-4D operator-split
+ * Fokker-Planck step behind a plain C ABI.
+ *
+ * Two layers:
+ *
+ *  1. A device-resident, batched context (verb_ctx).  It replaces the four
+ *     per-slice OpenMP loops of the reference driver
+ *       convection  src/VERB4D_Solver.cpp:851-978  -> verb_convection()
+ *       radial      src/VERB4D_Solver.cpp:990-1070 -> verb_radial()
+ *       local       src/VERB4D_Solver.cpp:1081-1216 -> verb_local()
+ *       negatives   src/VERB4D_Solver.cpp:1218-1242 -> verb_negative_count()
+ *       radial KF   src/VERB4D_Solver.cpp:1244-1253 -> verb_assimilate_radial()
+ *     Fields are uploaded when the reference's UpdatableMatrix::update()
+ *     reports a change (src/UpdatableMatrix.cpp:602); the LU factors of the
+ *     local systems live in HBM (the LU_CACHING cache of
+ *     src/VERB4D_Solver.cpp:340-365) and are refactored when DVV, DKK, DVK,
+ *     G_local, Losses_local, the grids, the BC types or dt change.
+ *
+ *  2. Per-slice entry points with the argument meaning of the reference's
+ *     routines (host pointers, one slice per call) for drop-in linking and
+ *     parity tests.
+ *
+ * Array layouts are the reference's: 4-D fields are [P][R][V][K] doubles with
+ * K fastest (src/Matrix.cpp:4211-4220); boundary arrays are 3-D as in
+ * src/ReadInitialData.cpp:541-563: Pl/Pu [R][V][K], Rl/Ru and Ll/Lu
+ * [P][V][K], Vl/Vu [P][R][K], Kl/Ku [P][R][V].  Boundary-condition type codes
+ * are those of src/BoundaryConditionType.hpp:53-88 (0 Periodic,
+ * 1 ConstantValue, 2 ConstantDerivative).
+ *
+ * Errors: every call returns a verb_status.  Where the reference calls
+ * exit(EXIT_FAILURE) (LAPACK info, Courant check, unknown BC, diffusion
+ * tensor check) this library returns the matching code instead; kernels
+ * record the first device-side error in a status word that verb_sync()
+ * returns.  No kernel traps.
+ */
+#ifndef VERB4D_B200_H
+#define VERB4D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    VERB_OK = 0,
+    VERB_ERR_PIVOT = 1,   /* exactly singular pivot (LAPACK info != 0, src/MatrixSolver.cpp:273-276) */
+    VERB_ERR_ARG = 2,     /* bad argument / unsupported size */
+    VERB_ERR_CFL = 3,     /* Courant number > 1 (src/Convection_1D_ULTIMATE_QUICKEST6.cpp:48-52) */
+    VERB_ERR_BC = 4,      /* unsupported boundary-condition type for this operator */
+    VERB_ERR_TENSOR = 5,  /* min(DVV*DKK - DVK^2) < 0 (src/VERB4D_Solver.cpp:747-753) */
+    VERB_ERR_NAN = 6,     /* NaN after the Kalman update (src/DataAssimilation.cpp:62-67) */
+    VERB_ERR_CUDA = 7,    /* CUDA runtime error */
+    VERB_ERR_NOMEM = 8,   /* device allocation failed / would not fit */
+    VERB_ERR_GRID = 9,    /* convection line shorter than 11 points (QUICKEST6.cpp:56-59) */
+    VERB_TIMEOUT = 10     /* a bounded device wait gave up */
+} verb_status;
+
+enum { VERB_BC_PERIODIC = 0, VERB_BC_CONSTANT_VALUE = 1, VERB_BC_CONSTANT_DERIVATIVE = 2 };
+
+/* 4-D fields of the context (names of src/VERB4D_Solver.cpp:210-245). */
+typedef enum {
+    VERB_F_PSD = 0,
+    VERB_F_P, VERB_F_R, VERB_F_V, VERB_F_K, VERB_F_L,
+    VERB_F_DLL, VERB_F_DVV, VERB_F_DKK, VERB_F_DVK,
+    VERB_F_VP, VERB_F_VR,
+    VERB_F_G_LOCAL, VERB_F_G_RADIAL, VERB_F_G_CONV,
+    VERB_F_SOURCES, VERB_F_LOSS_LOCAL, VERB_F_LOSS_RADIAL, VERB_F_LOSS_CONV,
+    VERB_F_COUNT
+} verb_field;
+
+/* 3-D boundary arrays. */
+typedef enum {
+    VERB_BCF_PL = 0, VERB_BCF_PU, VERB_BCF_RL, VERB_BCF_RU, VERB_BCF_LL, VERB_BCF_LU,
+    VERB_BCF_VL, VERB_BCF_VU, VERB_BCF_KL, VERB_BCF_KU, VERB_BCF_COUNT
+} verb_bc_field;
+
+typedef struct verb_ctx verb_ctx;
+
+/* Phase timings (milliseconds, CUDA events on the context stream), filled when
+ * timing is enabled with verb_set_timing(ctx, 1). */
+typedef struct {
+    double convection_ms, radial_ms, radial_factor_ms, local_ms, local_factor_ms,
+        local_solve_ms, reduce_ms, kf_ms;
+    long long steps, local_solve_launches, local_factor_launches;
+} verb_timing;
+
+/* ---- context lifetime ---------------------------------------------------- */
+/* stream: a cudaStream_t (NULL = the context creates its own). */
+int verb_create(verb_ctx** out, int P, int R, int V, int K, void* stream);
+int verb_destroy(verb_ctx* ctx);
+int verb_device_bytes(const verb_ctx* ctx, size_t* bytes);
+
+/* ---- inputs (UpdatableMatrix::update() == true  ->  upload) --------------- */
+int verb_upload_field(verb_ctx* ctx, int field, const double* host);      /* host [P][R][V][K] */
+int verb_upload_field_device(verb_ctx* ctx, int field, const double* dev);/* device pointer */
+/* Scale factor applied on the device as field = base * scale, the reference's
+ * UpdatableMatrix scale queue (src/UpdatableMatrix.cpp:698-708).  Default 1. */
+int verb_set_field_scale(verb_ctx* ctx, int field, double scale);
+int verb_upload_bc(verb_ctx* ctx, int bc_field, const double* host);
+/* types[10] in verb_bc_field order (Pl,Pu,Rl,Ru,Ll,Lu,Vl,Vu,Kl,Ku). */
+int verb_set_bc_types(verb_ctx* ctx, const int* types);
+/* Source/loss routing of src/VERB4D_Solver.cpp:404-426 and the include_boundary
+ * / positive_PSD switches of src/ReadInitialData.cpp:214-230. */
+int verb_set_options(verb_ctx* ctx, int radial_sources, int local_sources, int include_boundary,
+                     int positive_psd);
+/* Force the local LU factors to be recomputed at the next verb_local(). */
+int verb_invalidate_lu(verb_ctx* ctx);
+int verb_download_psd(verb_ctx* ctx, double* host);
+int verb_download_field(verb_ctx* ctx, int field, double* host);
+/* Device pointer of a field (for zero-copy use from the caller's CUDA code). */
+int verb_field_device_ptr(verb_ctx* ctx, int field, double** dev);
+
+/* ---- the step ------------------------------------------------------------ */
+/* Convection_2D over every (V,K) slice (src/Convection_2D.cpp:36-169). */
+int verb_convection(verb_ctx* ctx, double dt);
+/* Diffusion_1D over every (P,V,K) line (src/Diffusion_1D.cpp:43-88). */
+int verb_radial(verb_ctx* ctx, double dt);
+/* Diffusion_2D + Lapack over every (P,R) system with cached factors
+ * (src/Diffusion_2D.cpp:19-153, src/MatrixSolver.cpp:223-340). */
+int verb_local(verb_ctx* ctx, double dt, double sub_dt);
+/* max(PSD, 1e-21) (src/VERB4D_Solver.cpp:621). */
+int verb_clamp_positive(verb_ctx* ctx);
+/* Whole step in the reference order: tensor check, convection, radial, local,
+ * negative count (src/VERB4D_Solver.cpp:747-1242).  run_* select the phases. */
+int verb_step(verb_ctx* ctx, double dt, double sub_dt, int run_convection, int run_radial,
+              int run_local, long long* negative_count);
+/* Number of PSD points < 0 (src/VERB4D_Solver.cpp:1226-1240). */
+int verb_negative_count(verb_ctx* ctx, long long* count);
+/* min(DVV*DKK - DVK*DVK) over the grid (src/VERB4D_Solver.cpp:747-753). */
+int verb_tensor_check(verb_ctx* ctx, double* min_value);
+/* Wait for the context stream; returns the first device-side error. */
+int verb_sync(verb_ctx* ctx);
+int verb_set_timing(verb_ctx* ctx, int enable);
+int verb_get_timing(verb_ctx* ctx, verb_timing* out);
+/* Slice-level convection sub-step counts of the last verb_convection()
+ * ([V][K] ints, src/Convection_2D.cpp:57-86). */
+int verb_convection_substeps(verb_ctx* ctx, int* host_vk);
+/* Local LU pivots (0-based, [P][R][V*K] int32) and one system's factors in
+ * LAPACK band layout (ldab = 3*(V+1)+1 rows, column-major, as dgbtrf leaves
+ * them) for parity checks and LU-cache hand-off. */
+int verb_local_pivots(verb_ctx* ctx, int32_t* host);
+int verb_local_factor_lapack(verb_ctx* ctx, int p, int r, double* ab_host, long* ipiv1_host);
+
+/* ---- radial Kalman filter ------------------------------------------------ */
+/* One assimilation update of every (P,V,K) radial column (the reference
+ * applies it at P index 0 only: src/DataAssimilationDiffusion.cpp:116,139;
+ * p_index >= 0 restricts it the same way, -1 runs all P).  obs is a host
+ * [P][R][V][K] array with NaN where there is no observation.  The analysis
+ * covariances live on the device, initialised to 5*model_error*I on first use
+ * (src/DataAssimilationDiffusion.cpp:212-218). */
+int verb_assimilate_radial(verb_ctx* ctx, const double* obs_host, double dt, double model_error,
+                           double obs_error, int p_index);
+
+/* ---- per-slice entry points (host pointers, one slice per call) ----------- */
+/* tridag, src/MatrixSolver.cpp:689-720 (a,b,c,r,u of length n). */
+int verb_tridag(const double* a, const double* b, const double* c, const double* r, double* u,
+                long n);
+/* Diffusion_1D, src/Diffusion_1D.cpp:43-88 (psd updated in place). */
+int verb_diffusion_1d(double* psd, const double* x, int n, double lbc, double ubc, int lbc_t,
+                      int ubc_t, const double* D, const double* G, const double* S,
+                      const double* loss, double dt);
+/* Diffusion_2D (LU_CACHING form), src/Diffusion_2D.cpp:20-153: psd,x,y,D*,G,S,loss
+ * are [nx][ny]; xl/xu have ny entries, yl/yu nx.  lu_cache (ldab*nx*ny doubles,
+ * LAPACK band layout) and index_cache (nx*ny longs, 1-based) are the caller's
+ * cache slot: written when recompute_lu != 0, read otherwise.  Both may be
+ * NULL, which factors every call (the plain build). */
+int verb_diffusion_2d(double* psd, const double* x, const double* y, int nx, int ny,
+                      const double* xl, const double* xu, const double* yl, const double* yu,
+                      int xl_t, int xu_t, int yl_t, int yu_t, const double* Dxx, const double* Dyy,
+                      const double* Dxy, const double* Dyx, const double* G, const double* S,
+                      const double* loss, double dt, double sub_dt, double* lu_cache,
+                      long* index_cache, int recompute_lu);
+/* Convection_1D_ULTIMATE_QUICKEST6, src/Convection_1D_ULTIMATE_QUICKEST6.cpp:22. */
+int verb_convection_1d(double* psd, const double* x, int n, double lbc, double ubc, int lbc_t,
+                       int ubc_t, const double* ux, double dt);
+/* Convection_2D, src/Convection_2D.cpp:36 on one [P][R] slice. */
+int verb_convection_2d(double* psd, const double* P, const double* R, int nP, int nR,
+                       const double* pl, const double* pu, const double* rl, const double* ru,
+                       int pl_t, int pu_t, int rl_t, int ru_t, const double* VP, const double* VR,
+                       const double* S, const double* loss, const double* G, double dt);
+
+/* ---- library information --------------------------------------------------- */
+const char* verb_version(void);
+const char* verb_status_string(int status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VERB4D_B200_H */

@@ -1,0 +1,50 @@
+"""Synthetic workload generator: shapes, physical ranges and the checks the
+reference applies to its inputs."""
+import numpy as np
+
+from verb4d_b200 import workload as W
+
+
+def test_shapes_and_layout():
+    spec = W.GridSpec(8, 9, 7, 6)
+    wl = W.make_workload(spec, seed=2)
+    f = wl.fields
+    for k in ("psd", "Pg", "Rg", "Vg", "Kg", "Lg", "DLL", "DVV", "DKK", "DVK", "VP", "VR"):
+        assert f[k].shape == spec.shape and f[k].flags.c_contiguous
+    assert f["Rl"].shape == (8, 7, 6) and f["Vl"].shape == (8, 9, 6) and f["Kl"].shape == (8, 9, 7)
+    # K fastest: the pitch-angle grid varies along the last axis
+    assert np.all(np.diff(f["Kg"][0, 0, 0]) > 0)
+    # periodic MLT: endpoint duplicated
+    assert f["Pg"][0, 0, 0, 0] == 0.0 and f["Pg"][-1, 0, 0, 0] == 24.0
+
+
+def test_diffusion_tensor_check_passes():
+    wl = W.make_workload(W.CONFIGS["cfg1"], seed=1)
+    f = wl.fields
+    assert (f["DVV"] * f["DKK"] - f["DVK"] * f["DVK"]).min() >= 0  # src/VERB4D_Solver.cpp:747-753
+
+
+def test_brautigam_albert_range():
+    L = np.array([1.0, 6.6])
+    d = W.dll_brautigam_albert(L, 3.0)
+    assert 1.5e-8 < d[0] < 1.7e-8 and 2.3 < d[1] < 2.6
+
+
+def test_seeded_and_deterministic():
+    a = W.make_workload(W.GridSpec(6, 7, 5, 5), seed=9).fields["DVV"]
+    b = W.make_workload(W.GridSpec(6, 7, 5, 5), seed=9).fields["DVV"]
+    c = W.make_workload(W.GridSpec(6, 7, 5, 5), seed=10).fields["DVV"]
+    assert np.array_equal(a, b) and not np.array_equal(a, c)
+
+
+def test_convection_substeps_cfg1():
+    ns = W.convection_substeps(W.make_workload(W.CONFIGS["cfg1"], seed=1))
+    # gradient-curvature drift of 10 MeV electrons at L = 6.6 needs hundreds of
+    # CFL sub-steps per 5-minute step; the lowest energies need a few
+    assert ns.max() > 300 and ns.min() >= 1
+    assert np.all(np.diff(ns[:, -1]) >= 0)  # monotone in energy
+
+
+def test_kp_series():
+    k = W.kp_series(3, 24)
+    assert k.shape == (24,) and k.min() >= 1 and k.max() <= 6

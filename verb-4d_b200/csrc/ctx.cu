@@ -1,0 +1,1022 @@
+// C ABI: context lifetime, uploads, cache invalidation, phase dispatch, timing,
+// and the per-slice entry points.  See include/verb4d_b200.h.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "verb_internal.cuh"
+
+using namespace verb;
+
+namespace {
+
+enum Phase { PH_CONV = 0, PH_RAD, PH_RADF, PH_LOCAL, PH_LOCF, PH_LOCS, PH_RED, PH_KF, PH_N };
+
+struct EventPair {
+    cudaEvent_t a, b;
+};
+
+}  // namespace
+
+struct verb_ctx {
+    Dims d{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    double* f[VERB_F_COUNT] = {};
+    double* fbase[VERB_F_COUNT] = {};   // unscaled copy when a scale != 1 is set
+    double scale[VERB_F_COUNT];
+    bool uploaded[VERB_F_COUNT] = {};
+    double* bc[VERB_BCF_COUNT] = {};
+    int bct[VERB_BCF_COUNT];
+    int radial_sources = 0, local_sources = 1, include_boundary = 1, positive_psd = 0;
+    // radial Thomas factors
+    double *rfa = nullptr, *rfbet = nullptr, *rfgam = nullptr;
+    bool radial_dirty = true;
+    double radial_dt = -1;
+    // local LU factors
+    double *Lf = nullptr, *Uf = nullptr, *lwork = nullptr;
+    int32_t* ipiv = nullptr;
+    int kl = 0, kv = 0, klp = 0, kvp = 0;
+    bool local_dirty = true;
+    double local_dt = -1;
+    const double* dkv_override = nullptr;  // Dyx for the per-slice entry point
+    // convection
+    double* conv_scratch = nullptr;
+    int* conv_substeps = nullptr;
+    int* ticket = nullptr;
+    int conv_nctas = 0;
+    // reductions / status
+    unsigned long long* red = nullptr;  // [0] negatives, [1] tensor min key
+    int* status = nullptr;
+    bool tensor_dirty = true;
+    double tensor_min = 0;
+    // Kalman filter
+    double *Pa = nullptr, *kfwork = nullptr, *obs = nullptr;
+    size_t kfwork_bytes = 0;
+    int* kfticket = nullptr;
+    // timing
+    bool timing = false;
+    std::vector<EventPair> ev[PH_N];
+    std::vector<EventPair> pool;
+    verb_timing acc{};
+};
+
+namespace {
+
+int cuda_ok(cudaError_t e)
+{
+    if (e == cudaSuccess) return VERB_OK;
+    if (e == cudaErrorMemoryAllocation) return VERB_ERR_NOMEM;
+    return VERB_ERR_CUDA;
+}
+
+int cuda_ok(int s) { return s; }
+
+#define CK(x)                                 \
+    do {                                      \
+        int _s = cuda_ok(x);                  \
+        if (_s != VERB_OK) return _s;         \
+    } while (0)
+
+size_t npts(const verb_ctx* c) { return c->d.npts(); }
+
+size_t bc_elems(const verb_ctx* c, int b)
+{
+    const Dims& d = c->d;
+    switch (b) {
+        case VERB_BCF_PL: case VERB_BCF_PU: return (size_t)d.R * d.V * d.K;
+        case VERB_BCF_RL: case VERB_BCF_RU: case VERB_BCF_LL: case VERB_BCF_LU:
+            return (size_t)d.P * d.V * d.K;
+        case VERB_BCF_VL: case VERB_BCF_VU: return (size_t)d.P * d.R * d.K;
+        default: return (size_t)d.P * d.R * d.V;
+    }
+}
+
+int alloc(void** p, size_t bytes)
+{
+    if (*p) return VERB_OK;
+    return cuda_ok(cudaMalloc(p, bytes));
+}
+
+int ensure_field(verb_ctx* c, int fid)
+{
+    if (c->f[fid]) return VERB_OK;
+    CK(cudaMalloc(&c->f[fid], npts(c) * sizeof(double)));
+    return VERB_OK;
+}
+
+// A field the kernels read: defaults (G = 1, sources/losses = 0) when never uploaded.
+int need_field(verb_ctx* c, int fid)
+{
+    if (c->f[fid]) return VERB_OK;
+    int s = ensure_field(c, fid);
+    if (s) return s;
+    if (fid == VERB_F_G_LOCAL || fid == VERB_F_G_RADIAL || fid == VERB_F_G_CONV) {
+        std::vector<double> ones(npts(c), 1.0);
+        CK(cudaMemcpyAsync(c->f[fid], ones.data(), npts(c) * sizeof(double),
+                           cudaMemcpyHostToDevice, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+    } else if (fid == VERB_F_SOURCES || fid == VERB_F_LOSS_LOCAL || fid == VERB_F_LOSS_RADIAL ||
+               fid == VERB_F_LOSS_CONV) {
+        CK(cudaMemsetAsync(c->f[fid], 0, npts(c) * sizeof(double), c->stream));
+    } else {
+        return VERB_ERR_ARG;  // grids, coefficients and PSD must be provided
+    }
+    return VERB_OK;
+}
+
+int need_bc(verb_ctx* c, int b)
+{
+    if (c->bc[b]) return VERB_OK;
+    CK(cudaMalloc(&c->bc[b], bc_elems(c, b) * sizeof(double)));
+    CK(cudaMemsetAsync(c->bc[b], 0, bc_elems(c, b) * sizeof(double), c->stream));
+    return VERB_OK;
+}
+
+void mark_dirty(verb_ctx* c, int fid)
+{
+    switch (fid) {
+        case VERB_F_L: case VERB_F_DLL: case VERB_F_G_RADIAL: case VERB_F_LOSS_RADIAL:
+            c->radial_dirty = true;
+            break;
+        case VERB_F_V: case VERB_F_K: case VERB_F_G_LOCAL: case VERB_F_LOSS_LOCAL:
+            c->local_dirty = true;
+            break;
+        case VERB_F_DVV: case VERB_F_DKK: case VERB_F_DVK:
+            c->local_dirty = true;
+            c->tensor_dirty = true;
+            break;
+        default: break;
+    }
+}
+
+EventPair get_pair(verb_ctx* c)
+{
+    if (!c->pool.empty()) {
+        EventPair p = c->pool.back();
+        c->pool.pop_back();
+        return p;
+    }
+    EventPair p;
+    cudaEventCreate(&p.a);
+    cudaEventCreate(&p.b);
+    return p;
+}
+
+struct PhaseTimer {
+    verb_ctx* c;
+    int ph;
+    EventPair p{};
+    PhaseTimer(verb_ctx* c_, int ph_) : c(c_), ph(ph_)
+    {
+        if (c->timing) {
+            p = get_pair(c);
+            cudaEventRecord(p.a, c->stream);
+        }
+    }
+    ~PhaseTimer()
+    {
+        if (c->timing) {
+            cudaEventRecord(p.b, c->stream);
+            c->ev[ph].push_back(p);
+        }
+    }
+};
+
+int check_launch() { return cuda_ok(cudaGetLastError()); }
+
+int radial_run(verb_ctx* c, double dt)
+{
+    const Dims& d = c->d;
+    if (d.R < 3) return VERB_OK;
+    if (c->bct[VERB_BCF_LL] == VERB_BC_PERIODIC || c->bct[VERB_BCF_LU] == VERB_BC_PERIODIC)
+        return VERB_ERR_BC;
+    for (int fid : {VERB_F_PSD, VERB_F_L, VERB_F_DLL, VERB_F_G_RADIAL, VERB_F_LOSS_RADIAL}) {
+        int s = need_field(c, fid);
+        if (s) return s;
+    }
+    if (c->radial_sources) {
+        int s = need_field(c, VERB_F_SOURCES);
+        if (s) return s;
+    }
+    for (int b : {VERB_BCF_LL, VERB_BCF_LU}) {
+        int s = need_bc(c, b);
+        if (s) return s;
+    }
+    const size_t nl = (size_t)d.P * d.V * d.K * d.R;
+    CK(alloc((void**)&c->rfa, nl * sizeof(double)));
+    CK(alloc((void**)&c->rfbet, nl * sizeof(double)));
+    CK(alloc((void**)&c->rfgam, nl * sizeof(double)));
+    RadialArgs a{};
+    a.d = d;
+    a.psd = c->f[VERB_F_PSD];
+    a.L = c->f[VERB_F_L];
+    a.DLL = c->f[VERB_F_DLL];
+    a.G = c->f[VERB_F_G_RADIAL];
+    a.S = c->f[VERB_F_SOURCES];
+    a.loss = c->f[VERB_F_LOSS_RADIAL];
+    a.dll_scale = 1.0;  // scales are materialised into the field at upload time
+    a.Ll = c->bc[VERB_BCF_LL];
+    a.Lu = c->bc[VERB_BCF_LU];
+    a.Ll_t = c->bct[VERB_BCF_LL];
+    a.Lu_t = c->bct[VERB_BCF_LU];
+    a.dt = dt;
+    a.radial_sources = c->radial_sources;
+    a.fa = c->rfa;
+    a.fbet = c->rfbet;
+    a.fgam = c->rfgam;
+    a.status = c->status;
+    if (c->radial_dirty || dt != c->radial_dt) {
+        PhaseTimer t(c, PH_RADF);
+        launch_radial_factor(a, c->stream);
+        c->radial_dirty = false;
+        c->radial_dt = dt;
+    }
+    {
+        PhaseTimer t(c, PH_RAD);
+        launch_radial_solve(a, c->stream);
+    }
+    return check_launch();
+}
+
+int local_prepare(verb_ctx* c, LocalArgs& a, double dts)
+{
+    const Dims& d = c->d;
+    if (d.V > 111) return VERB_ERR_ARG;  // solve windows hold kl+1 <= 128 and kv+1 <= 256
+    for (int fid : {VERB_F_PSD, VERB_F_V, VERB_F_K, VERB_F_DVV, VERB_F_DKK, VERB_F_DVK,
+                    VERB_F_G_LOCAL, VERB_F_LOSS_LOCAL, VERB_F_SOURCES}) {
+        int s = need_field(c, fid);
+        if (s) return s;
+    }
+    for (int b : {VERB_BCF_VL, VERB_BCF_VU, VERB_BCF_KL, VERB_BCF_KU}) {
+        int s = need_bc(c, b);
+        if (s) return s;
+        if (c->bct[b] == VERB_BC_PERIODIC) return VERB_ERR_BC;
+    }
+    c->kl = d.V + 1;
+    c->kv = 2 * c->kl;
+    c->klp = (c->kl + 1) & ~1;
+    c->kvp = (c->kv + 2) & ~1;
+    const size_t nsys = (size_t)d.P * d.R, n = (size_t)d.V * d.K;
+    CK(alloc((void**)&c->Lf, nsys * n * c->klp * sizeof(double)));
+    CK(alloc((void**)&c->Uf, nsys * n * c->kvp * sizeof(double)));
+    CK(alloc((void**)&c->ipiv, nsys * n * sizeof(int32_t)));
+    CK(alloc((void**)&c->lwork, nsys * n * sizeof(double)));
+    a.d = d;
+    a.psd = c->f[VERB_F_PSD];
+    a.Vg = c->f[VERB_F_V];
+    a.Kg = c->f[VERB_F_K];
+    a.DVV = c->f[VERB_F_DVV];
+    a.DKK = c->f[VERB_F_DKK];
+    a.DVK = c->f[VERB_F_DVK];
+    a.DKV = c->dkv_override ? c->dkv_override : c->f[VERB_F_DVK];
+    a.G = c->f[VERB_F_G_LOCAL];
+    a.S = c->f[VERB_F_SOURCES];
+    a.loss = c->f[VERB_F_LOSS_LOCAL];
+    a.Vl = c->bc[VERB_BCF_VL];
+    a.Vu = c->bc[VERB_BCF_VU];
+    a.Kl = c->bc[VERB_BCF_KL];
+    a.Ku = c->bc[VERB_BCF_KU];
+    a.Vl_t = c->bct[VERB_BCF_VL];
+    a.Vu_t = c->bct[VERB_BCF_VU];
+    a.Kl_t = c->bct[VERB_BCF_KL];
+    a.Ku_t = c->bct[VERB_BCF_KU];
+    a.dt = dts;
+    a.local_sources = c->local_sources;
+    a.include_boundary = c->include_boundary;
+    a.kl = c->kl;
+    a.kv = c->kv;
+    a.klp = c->klp;
+    a.kvp = c->kvp;
+    a.Lf = c->Lf;
+    a.Uf = c->Uf;
+    a.ipiv = c->ipiv;
+    a.work = c->lwork;
+    a.status = c->status;
+    return VERB_OK;
+}
+
+int local_factor(verb_ctx* c, LocalArgs& a)
+{
+    PhaseTimer t(c, PH_LOCF);
+    const size_t nsys = (size_t)c->d.P * c->d.R, n = (size_t)c->d.V * c->d.K;
+    CK(cudaMemsetAsync(c->Uf, 0, nsys * n * c->kvp * sizeof(double), c->stream));
+    launch_local_factor(a, c->stream);
+    c->local_dirty = false;
+    c->local_dt = a.dt;
+    c->acc.local_factor_launches++;
+    return check_launch();
+}
+
+int local_run(verb_ctx* c, double dt, double sub_dt)
+{
+    const Dims& d = c->d;
+    if (d.V < 3 || d.K < 3) return VERB_OK;
+    int nsub = (int)(dt / sub_dt);
+    if (nsub < 1) nsub = 1;
+    const double dts = dt / nsub;
+    LocalArgs a{};
+    int s = local_prepare(c, a, dts);
+    if (s) return s;
+    PhaseTimer t(c, PH_LOCAL);
+    if (c->local_dirty || dts != c->local_dt) {
+        s = local_factor(c, a);
+        if (s) return s;
+    }
+    for (int k = 0; k < nsub; k++) {
+        launch_local_rhs(a, k > 0, c->stream);
+        {
+            PhaseTimer ts(c, PH_LOCS);
+            launch_local_solve(a, c->stream);
+        }
+        c->acc.local_solve_launches++;
+    }
+    launch_local_store(a, c->stream);
+    return check_launch();
+}
+
+int conv_run(verb_ctx* c, double dt)
+{
+    const Dims& d = c->d;
+    if ((d.P >= 3 && d.P < 11) || (d.R >= 3 && d.R < 11)) return VERB_ERR_GRID;
+    const bool pper = c->bct[VERB_BCF_PL] == VERB_BC_PERIODIC;
+    if (pper != (c->bct[VERB_BCF_PU] == VERB_BC_PERIODIC)) return VERB_ERR_BC;
+    const bool rper = c->bct[VERB_BCF_RL] == VERB_BC_PERIODIC;
+    if (rper != (c->bct[VERB_BCF_RU] == VERB_BC_PERIODIC)) return VERB_ERR_BC;
+    for (int fid : {VERB_F_PSD, VERB_F_P, VERB_F_R, VERB_F_VP, VERB_F_VR, VERB_F_SOURCES,
+                    VERB_F_LOSS_CONV, VERB_F_G_CONV}) {
+        int s = need_field(c, fid);
+        if (s) return s;
+    }
+    for (int b : {VERB_BCF_PL, VERB_BCF_PU, VERB_BCF_RL, VERB_BCF_RU}) {
+        int s = need_bc(c, b);
+        if (s) return s;
+    }
+    if (!c->conv_nctas) c->conv_nctas = conv_ctas(d.P, d.R);
+    CK(alloc((void**)&c->conv_scratch, (size_t)c->conv_nctas * d.P * d.R * sizeof(double)));
+    CK(alloc((void**)&c->conv_substeps, (size_t)d.V * d.K * sizeof(int)));
+    CK(alloc((void**)&c->ticket, sizeof(int)));
+    ConvArgs a{};
+    a.d = d;
+    a.psd = c->f[VERB_F_PSD];
+    a.Pg = c->f[VERB_F_P];
+    a.Rg = c->f[VERB_F_R];
+    a.VP = c->f[VERB_F_VP];
+    a.VR = c->f[VERB_F_VR];
+    a.S = c->f[VERB_F_SOURCES];
+    a.loss = c->f[VERB_F_LOSS_CONV];
+    a.G = c->f[VERB_F_G_CONV];
+    a.Pl = c->bc[VERB_BCF_PL];
+    a.Pu = c->bc[VERB_BCF_PU];
+    a.Rl = c->bc[VERB_BCF_RL];
+    a.Ru = c->bc[VERB_BCF_RU];
+    a.Pl_t = c->bct[VERB_BCF_PL];
+    a.Pu_t = c->bct[VERB_BCF_PU];
+    a.Rl_t = c->bct[VERB_BCF_RL];
+    a.Ru_t = c->bct[VERB_BCF_RU];
+    a.dt = dt;
+    a.scratch = c->conv_scratch;
+    a.substeps = c->conv_substeps;
+    a.ticket = c->ticket;
+    a.status = c->status;
+    PhaseTimer t(c, PH_CONV);
+    CK(cudaMemsetAsync(c->ticket, 0, sizeof(int), c->stream));
+    launch_convection(a, c->conv_nctas, c->stream);
+    return check_launch();
+}
+
+int tensor_check(verb_ctx* c, double* out)
+{
+    if (c->tensor_dirty) {
+        for (int fid : {VERB_F_DVV, VERB_F_DKK, VERB_F_DVK}) {
+            int s = need_field(c, fid);
+            if (s) return s;
+        }
+        CK(alloc((void**)&c->red, 2 * sizeof(unsigned long long)));
+        launch_tensor_min(c->f[VERB_F_DVV], c->f[VERB_F_DKK], c->f[VERB_F_DVK], npts(c), c->red + 1,
+                          c->stream);
+        unsigned long long k = 0;
+        CK(cudaMemcpyAsync(&k, c->red + 1, sizeof(k), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        c->tensor_min = dkey_inv(k);
+        c->tensor_dirty = false;
+    }
+    if (out) *out = c->tensor_min;
+    return VERB_OK;
+}
+
+int harvest_timing(verb_ctx* c)
+{
+    CK(cudaStreamSynchronize(c->stream));
+    double* dst[PH_N] = {&c->acc.convection_ms, &c->acc.radial_ms, &c->acc.radial_factor_ms,
+                         &c->acc.local_ms, &c->acc.local_factor_ms, &c->acc.local_solve_ms,
+                         &c->acc.reduce_ms, &c->acc.kf_ms};
+    for (int p = 0; p < PH_N; p++) {
+        for (EventPair& e : c->ev[p]) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e.a, e.b);
+            *dst[p] += ms;
+            c->pool.push_back(e);
+        }
+        c->ev[p].clear();
+    }
+    return VERB_OK;
+}
+
+}  // namespace
+
+// ============================================================================ C ABI
+
+extern "C" {
+
+const char* verb_version(void) { return "verb4d_b200 0.1 (sm_100a)"; }
+
+const char* verb_status_string(int s)
+{
+    switch (s) {
+        case VERB_OK: return "ok";
+        case VERB_ERR_PIVOT: return "singular pivot in the banded LU";
+        case VERB_ERR_ARG: return "invalid argument";
+        case VERB_ERR_CFL: return "Courant number > 1";
+        case VERB_ERR_BC: return "unsupported boundary condition type";
+        case VERB_ERR_TENSOR: return "DVV*DKK - DVK^2 < 0";
+        case VERB_ERR_NAN: return "NaN after the Kalman update";
+        case VERB_ERR_CUDA: return "CUDA error";
+        case VERB_ERR_NOMEM: return "out of device memory";
+        case VERB_ERR_GRID: return "convection grid shorter than 11 points";
+        case VERB_TIMEOUT: return "device wait timed out";
+        default: return "unknown status";
+    }
+}
+
+int verb_create(verb_ctx** out, int P, int R, int V, int K, void* stream)
+{
+    if (!out || P < 1 || R < 1 || V < 1 || K < 1) return VERB_ERR_ARG;
+    verb_ctx* c = new (std::nothrow) verb_ctx();
+    if (!c) return VERB_ERR_NOMEM;
+    c->d = Dims{P, R, V, K};
+    for (int i = 0; i < VERB_F_COUNT; i++) c->scale[i] = 1.0;
+    // reference defaults (src/ReadInitialData.cpp:495-511): periodic MLT, constant value elsewhere
+    const int def[VERB_BCF_COUNT] = {0, 0, 1, 1, 1, 1, 1, 1, 1, 1};
+    memcpy(c->bct, def, sizeof(def));
+    int st = cuda_ok(cudaGetDevice(&c->device));
+    if (!st) {
+        if (stream) {
+            c->stream = (cudaStream_t)stream;
+        } else {
+            st = cuda_ok(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+            c->own_stream = true;
+        }
+    }
+    if (!st) st = cuda_ok(cudaMalloc(&c->status, sizeof(int)));
+    if (!st) st = cuda_ok(cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
+    if (!st) st = cuda_ok(cudaMalloc(&c->red, 2 * sizeof(unsigned long long)));
+    if (st) {
+        verb_destroy(c);
+        return st;
+    }
+    *out = c;
+    return VERB_OK;
+}
+
+int verb_destroy(verb_ctx* c)
+{
+    if (!c) return VERB_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (int i = 0; i < VERB_F_COUNT; i++) {
+        cudaFree(c->f[i]);
+        cudaFree(c->fbase[i]);
+    }
+    for (int i = 0; i < VERB_BCF_COUNT; i++) cudaFree(c->bc[i]);
+    for (void* p : {(void*)c->rfa, (void*)c->rfbet, (void*)c->rfgam, (void*)c->Lf, (void*)c->Uf,
+                    (void*)c->lwork, (void*)c->ipiv, (void*)c->conv_scratch,
+                    (void*)c->conv_substeps, (void*)c->ticket, (void*)c->red, (void*)c->status,
+                    (void*)c->Pa, (void*)c->kfwork, (void*)c->obs, (void*)c->kfticket})
+        cudaFree(p);
+    for (int p = 0; p < PH_N; p++)
+        for (EventPair& e : c->ev[p]) c->pool.push_back(e);
+    for (EventPair& e : c->pool) {
+        cudaEventDestroy(e.a);
+        cudaEventDestroy(e.b);
+    }
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return VERB_OK;
+}
+
+int verb_device_bytes(const verb_ctx* c, size_t* bytes)
+{
+    if (!c || !bytes) return VERB_ERR_ARG;
+    size_t b = 0;
+    const size_t F = c->d.npts() * sizeof(double);
+    for (int i = 0; i < VERB_F_COUNT; i++) b += (c->f[i] ? F : 0) + (c->fbase[i] ? F : 0);
+    for (int i = 0; i < VERB_BCF_COUNT; i++)
+        if (c->bc[i]) b += bc_elems(c, i) * sizeof(double);
+    if (c->rfa) b += 3 * F;
+    if (c->Lf) {
+        const size_t ns = (size_t)c->d.P * c->d.R * c->d.V * c->d.K;
+        b += ns * (c->klp + c->kvp + 1) * sizeof(double) + ns * sizeof(int32_t);
+    }
+    *bytes = b;
+    return VERB_OK;
+}
+
+static int upload_common(verb_ctx* c, int fid, const void* src, cudaMemcpyKind kind)
+{
+    if (!c || fid < 0 || fid >= VERB_F_COUNT || !src) return VERB_ERR_ARG;
+    const size_t bytes = npts(c) * sizeof(double);
+    int s = ensure_field(c, fid);
+    if (s) return s;
+    if (c->scale[fid] != 1.0) {
+        CK(alloc((void**)&c->fbase[fid], bytes));
+        CK(cudaMemcpyAsync(c->fbase[fid], src, bytes, kind, c->stream));
+        launch_scale_copy(c->f[fid], c->fbase[fid], c->scale[fid], npts(c), c->stream);
+    } else {
+        CK(cudaMemcpyAsync(c->f[fid], src, bytes, kind, c->stream));
+        if (c->fbase[fid]) {
+            cudaFree(c->fbase[fid]);
+            c->fbase[fid] = nullptr;
+        }
+    }
+    c->uploaded[fid] = true;
+    mark_dirty(c, fid);
+    return check_launch();
+}
+
+int verb_upload_field(verb_ctx* c, int fid, const double* host)
+{
+    return upload_common(c, fid, host, cudaMemcpyHostToDevice);
+}
+
+int verb_upload_field_device(verb_ctx* c, int fid, const double* dev)
+{
+    return upload_common(c, fid, dev, cudaMemcpyDeviceToDevice);
+}
+
+int verb_set_field_scale(verb_ctx* c, int fid, double scale)
+{
+    if (!c || fid < 0 || fid >= VERB_F_COUNT) return VERB_ERR_ARG;
+    if (scale == c->scale[fid]) return VERB_OK;
+    const size_t bytes = npts(c) * sizeof(double);
+    if (c->f[fid]) {
+        if (!c->fbase[fid]) {
+            // the current contents are the base (scale 1) field
+            CK(cudaMalloc(&c->fbase[fid], bytes));
+            CK(cudaMemcpyAsync(c->fbase[fid], c->f[fid], bytes, cudaMemcpyDeviceToDevice, c->stream));
+        }
+        if (scale != 1.0)
+            launch_scale_copy(c->f[fid], c->fbase[fid], scale, npts(c), c->stream);
+        else
+            CK(cudaMemcpyAsync(c->f[fid], c->fbase[fid], bytes, cudaMemcpyDeviceToDevice, c->stream));
+        mark_dirty(c, fid);
+    }
+    c->scale[fid] = scale;
+    return check_launch();
+}
+
+int verb_upload_bc(verb_ctx* c, int b, const double* host)
+{
+    if (!c || b < 0 || b >= VERB_BCF_COUNT || !host) return VERB_ERR_ARG;
+    if (!c->bc[b]) CK(cudaMalloc(&c->bc[b], bc_elems(c, b) * sizeof(double)));
+    CK(cudaMemcpyAsync(c->bc[b], host, bc_elems(c, b) * sizeof(double), cudaMemcpyHostToDevice,
+                       c->stream));
+    return VERB_OK;
+}
+
+int verb_set_bc_types(verb_ctx* c, const int* types)
+{
+    if (!c || !types) return VERB_ERR_ARG;
+    for (int i = 0; i < VERB_BCF_COUNT; i++)
+        if (types[i] < 0 || types[i] > 2) return VERB_ERR_BC;
+    bool rad = types[VERB_BCF_LL] != c->bct[VERB_BCF_LL] || types[VERB_BCF_LU] != c->bct[VERB_BCF_LU];
+    bool loc = false;
+    for (int b : {VERB_BCF_VL, VERB_BCF_VU, VERB_BCF_KL, VERB_BCF_KU})
+        loc = loc || types[b] != c->bct[b];
+    memcpy(c->bct, types, sizeof(c->bct));
+    if (rad) c->radial_dirty = true;
+    if (loc) c->local_dirty = true;
+    return VERB_OK;
+}
+
+int verb_set_options(verb_ctx* c, int radial_sources, int local_sources, int include_boundary,
+                     int positive_psd)
+{
+    if (!c) return VERB_ERR_ARG;
+    c->radial_sources = radial_sources;
+    c->local_sources = local_sources;
+    if ((include_boundary != 0) != (c->include_boundary != 0)) c->local_dirty = true;
+    c->include_boundary = include_boundary;
+    c->positive_psd = positive_psd;
+    return VERB_OK;
+}
+
+int verb_invalidate_lu(verb_ctx* c)
+{
+    if (!c) return VERB_ERR_ARG;
+    c->local_dirty = true;
+    c->radial_dirty = true;
+    return VERB_OK;
+}
+
+int verb_download_field(verb_ctx* c, int fid, double* host)
+{
+    if (!c || fid < 0 || fid >= VERB_F_COUNT || !host || !c->f[fid]) return VERB_ERR_ARG;
+    CK(cudaMemcpyAsync(host, c->f[fid], npts(c) * sizeof(double), cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return VERB_OK;
+}
+
+int verb_download_psd(verb_ctx* c, double* host) { return verb_download_field(c, VERB_F_PSD, host); }
+
+int verb_field_device_ptr(verb_ctx* c, int fid, double** dev)
+{
+    if (!c || fid < 0 || fid >= VERB_F_COUNT || !dev) return VERB_ERR_ARG;
+    int s = ensure_field(c, fid);
+    if (s) return s;
+    *dev = c->f[fid];
+    return VERB_OK;
+}
+
+int verb_convection(verb_ctx* c, double dt)
+{
+    if (!c || !(dt > 0)) return VERB_ERR_ARG;
+    return conv_run(c, dt);
+}
+
+int verb_radial(verb_ctx* c, double dt)
+{
+    if (!c || !(dt > 0)) return VERB_ERR_ARG;
+    return radial_run(c, dt);
+}
+
+int verb_local(verb_ctx* c, double dt, double sub_dt)
+{
+    if (!c || !(dt > 0) || !(sub_dt > 0)) return VERB_ERR_ARG;
+    return local_run(c, dt, sub_dt);
+}
+
+int verb_clamp_positive(verb_ctx* c)
+{
+    if (!c || !c->f[VERB_F_PSD]) return VERB_ERR_ARG;
+    launch_clamp_positive(c->f[VERB_F_PSD], npts(c), c->stream);
+    return check_launch();
+}
+
+int verb_negative_count(verb_ctx* c, long long* count)
+{
+    if (!c || !c->f[VERB_F_PSD]) return VERB_ERR_ARG;
+    {
+        PhaseTimer t(c, PH_RED);
+        launch_negative_count(c->f[VERB_F_PSD], npts(c), c->red, c->stream);
+    }
+    if (count) {
+        unsigned long long k = 0;
+        CK(cudaMemcpyAsync(&k, c->red, sizeof(k), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        *count = (long long)k;
+    }
+    return check_launch();
+}
+
+int verb_tensor_check(verb_ctx* c, double* min_value)
+{
+    if (!c) return VERB_ERR_ARG;
+    return tensor_check(c, min_value);
+}
+
+int verb_step(verb_ctx* c, double dt, double sub_dt, int run_convection, int run_radial,
+              int run_local, long long* negative_count)
+{
+    if (!c || !(dt > 0)) return VERB_ERR_ARG;
+    const Dims& d = c->d;
+    int s;
+    if (run_local && d.V >= 3 && d.K >= 3) {
+        double m = 0;
+        s = tensor_check(c, &m);
+        if (s) return s;
+        if (m < 0) return VERB_ERR_TENSOR;
+    }
+    if (c->positive_psd && (s = verb_clamp_positive(c))) return s;
+    if (run_convection && (3 < d.P || 3 < d.R)) {
+        s = conv_run(c, dt);
+        if (s) return s;
+    }
+    if (c->positive_psd && (s = verb_clamp_positive(c))) return s;
+    if (run_radial && d.R >= 3) {
+        s = radial_run(c, dt);
+        if (s) return s;
+    }
+    if (c->positive_psd && (s = verb_clamp_positive(c))) return s;
+    if (run_local && d.V >= 3 && d.K >= 3) {
+        s = local_run(c, dt, sub_dt);
+        if (s) return s;
+    }
+    c->acc.steps++;
+    if (c->positive_psd) {
+        s = verb_clamp_positive(c);
+        if (negative_count) *negative_count = 0;
+        return s;
+    }
+    return verb_negative_count(c, negative_count);
+}
+
+int verb_sync(verb_ctx* c)
+{
+    if (!c) return VERB_ERR_ARG;
+    CK(cudaStreamSynchronize(c->stream));
+    int st = 0;
+    CK(cudaMemcpy(&st, c->status, sizeof(int), cudaMemcpyDeviceToHost));
+    return st;
+}
+
+int verb_set_timing(verb_ctx* c, int enable)
+{
+    if (!c) return VERB_ERR_ARG;
+    if (!enable) harvest_timing(c);
+    c->timing = enable != 0;
+    if (enable) memset(&c->acc, 0, sizeof(c->acc));
+    return VERB_OK;
+}
+
+int verb_get_timing(verb_ctx* c, verb_timing* out)
+{
+    if (!c || !out) return VERB_ERR_ARG;
+    int s = harvest_timing(c);
+    *out = c->acc;
+    return s;
+}
+
+int verb_convection_substeps(verb_ctx* c, int* host)
+{
+    if (!c || !host || !c->conv_substeps) return VERB_ERR_ARG;
+    CK(cudaMemcpyAsync(host, c->conv_substeps, (size_t)c->d.V * c->d.K * sizeof(int),
+                       cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return VERB_OK;
+}
+
+int verb_local_pivots(verb_ctx* c, int32_t* host)
+{
+    if (!c || !host || !c->ipiv) return VERB_ERR_ARG;
+    CK(cudaMemcpyAsync(host, c->ipiv, c->d.npts() * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return VERB_OK;
+}
+
+int verb_local_factor_lapack(verb_ctx* c, int p, int r, double* ab, long* ipiv1)
+{
+    if (!c || !c->Lf || p < 0 || r < 0 || p >= c->d.P || r >= c->d.R) return VERB_ERR_ARG;
+    const int n = c->d.V * c->d.K, kl = c->kl, kv = c->kv, ldab = 2 * kl + kl + 1;
+    const size_t sys = (size_t)p * c->d.R + r;
+    std::vector<double> L((size_t)n * c->klp), U((size_t)n * c->kvp);
+    std::vector<int32_t> ip(n);
+    CK(cudaMemcpyAsync(L.data(), c->Lf + sys * n * c->klp, L.size() * sizeof(double),
+                       cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(U.data(), c->Uf + sys * n * c->kvp, U.size() * sizeof(double),
+                       cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(ip.data(), c->ipiv + sys * n, n * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (ab) {
+        memset(ab, 0, sizeof(double) * (size_t)ldab * n);
+        for (int j = 0; j < n; j++) {
+            for (int t = 0; t <= kv; t++)  // U rows j-kv+t
+                if (j - kv + t >= 0) ab[(size_t)j * ldab + t] = U[(size_t)j * c->kvp + t];
+            for (int i = 1; i <= kl && j + i < n; i++)
+                ab[(size_t)j * ldab + kv + i] = L[(size_t)j * c->klp + (i - 1)];
+        }
+    }
+    if (ipiv1)
+        for (int j = 0; j < n; j++) ipiv1[j] = ip[j] + 1;
+    return VERB_OK;
+}
+
+}  // extern "C"
+
+// ====================================================== per-slice entry points
+namespace {
+
+struct TmpCtx {
+    verb_ctx* c = nullptr;
+    ~TmpCtx() { verb_destroy(c); }
+};
+
+}  // namespace
+
+extern "C" {
+
+int verb_tridag(const double* a, const double* b, const double* c, const double* r, double* u,
+                long n)
+{
+    if (!a || !b || !c || !r || !u || n < 1) return VERB_ERR_ARG;
+    double* dv = nullptr;
+    CK(cudaMalloc(&dv, sizeof(double) * 6 * n));
+    const double* src[4] = {a, b, c, r};
+    int s = VERB_OK;
+    for (int i = 0; i < 4 && !s; i++)
+        s = cuda_ok(cudaMemcpy(dv + i * n, src[i], sizeof(double) * n, cudaMemcpyHostToDevice));
+    if (!s) {
+        launch_tridag(dv, dv + n, dv + 2 * n, dv + 3 * n, dv + 4 * n, n, 0);
+        s = cuda_ok(cudaMemcpy(u, dv + 4 * n, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    }
+    cudaFree(dv);
+    return s;
+}
+
+int verb_diffusion_1d(double* psd, const double* x, int n, double lbc, double ubc, int lbc_t,
+                      int ubc_t, const double* D, const double* G, const double* S,
+                      const double* loss, double dt)
+{
+    if (!psd || !x || !D || !G || !S || !loss || n < 3) return VERB_ERR_ARG;
+    TmpCtx t;
+    int s = verb_create(&t.c, 1, n, 1, 1, nullptr);
+    if (s) return s;
+    int types[VERB_BCF_COUNT] = {0, 0, 1, 1, lbc_t, ubc_t, 1, 1, 1, 1};
+    if ((s = verb_set_bc_types(t.c, types))) return s;
+    if ((s = verb_set_options(t.c, 1, 0, 1, 0))) return s;
+    const int fids[6] = {VERB_F_PSD, VERB_F_L, VERB_F_DLL, VERB_F_G_RADIAL, VERB_F_SOURCES,
+                         VERB_F_LOSS_RADIAL};
+    const double* srcs[6] = {psd, x, D, G, S, loss};
+    for (int i = 0; i < 6; i++)
+        if ((s = verb_upload_field(t.c, fids[i], srcs[i]))) return s;
+    if ((s = verb_upload_bc(t.c, VERB_BCF_LL, &lbc))) return s;
+    if ((s = verb_upload_bc(t.c, VERB_BCF_LU, &ubc))) return s;
+    if ((s = verb_radial(t.c, dt))) return s;
+    if ((s = verb_sync(t.c))) return s;
+    return verb_download_psd(t.c, psd);
+}
+
+int verb_diffusion_2d(double* psd, const double* x, const double* y, int nx, int ny,
+                      const double* xl, const double* xu, const double* yl, const double* yu,
+                      int xl_t, int xu_t, int yl_t, int yu_t, const double* Dxx, const double* Dyy,
+                      const double* Dxy, const double* Dyx, const double* G, const double* S,
+                      const double* loss, double dt, double sub_dt, double* lu_cache,
+                      long* index_cache, int recompute_lu)
+{
+    if (!psd || !x || !y || nx < 3 || ny < 3) return VERB_ERR_ARG;
+    TmpCtx t;
+    int s = verb_create(&t.c, 1, 1, nx, ny, nullptr);
+    if (s) return s;
+    int types[VERB_BCF_COUNT] = {0, 0, 1, 1, 1, 1, xl_t, xu_t, yl_t, yu_t};
+    if ((s = verb_set_bc_types(t.c, types))) return s;
+    if ((s = verb_set_options(t.c, 0, 1, 1, 0))) return s;
+    const int fids[9] = {VERB_F_PSD, VERB_F_V, VERB_F_K, VERB_F_DVV, VERB_F_DKK, VERB_F_DVK,
+                         VERB_F_G_LOCAL, VERB_F_SOURCES, VERB_F_LOSS_LOCAL};
+    const double* srcs[9] = {psd, x, y, Dxx, Dyy, Dxy, G, S, loss};
+    for (int i = 0; i < 9; i++)
+        if ((s = verb_upload_field(t.c, fids[i], srcs[i]))) return s;
+    const size_t n = (size_t)nx * ny;
+    double* dkv = nullptr;
+    CK(cudaMalloc(&dkv, n * sizeof(double)));
+    s = cuda_ok(cudaMemcpy(dkv, Dyx, n * sizeof(double), cudaMemcpyHostToDevice));
+    t.c->dkv_override = dkv;
+    if (!s) s = verb_upload_bc(t.c, VERB_BCF_VL, xl);
+    if (!s) s = verb_upload_bc(t.c, VERB_BCF_VU, xu);
+    if (!s) s = verb_upload_bc(t.c, VERB_BCF_KL, yl);
+    if (!s) s = verb_upload_bc(t.c, VERB_BCF_KU, yu);
+    if (!s && lu_cache && !recompute_lu) {
+        // reuse the caller's LAPACK-layout factors: convert into the device layout
+        LocalArgs a{};
+        int nsub = (int)(dt / sub_dt);
+        if (nsub < 1) nsub = 1;
+        s = local_prepare(t.c, a, dt / nsub);
+        if (!s) {
+            const int kl = t.c->kl, kv = t.c->kv, klp = t.c->klp, kvp = t.c->kvp;
+            const int ldab = 3 * kl + 1;
+            std::vector<double> L(n * klp, 0.0), U(n * kvp, 0.0);
+            std::vector<int32_t> ip(n);
+            for (size_t j = 0; j < n; j++) {
+                for (int q = 0; q <= kv; q++) U[j * kvp + q] = lu_cache[j * ldab + q];
+                for (int i = 1; i <= kl && j + i < n; i++)
+                    L[j * klp + (i - 1)] = lu_cache[j * ldab + kv + i];
+                ip[j] = (int32_t)(index_cache[j] - 1);
+            }
+            s = cuda_ok(cudaMemcpy(t.c->Lf, L.data(), L.size() * 8, cudaMemcpyHostToDevice));
+            if (!s) s = cuda_ok(cudaMemcpy(t.c->Uf, U.data(), U.size() * 8, cudaMemcpyHostToDevice));
+            if (!s) s = cuda_ok(cudaMemcpy(t.c->ipiv, ip.data(), n * 4, cudaMemcpyHostToDevice));
+            t.c->local_dirty = false;
+            t.c->local_dt = dt / nsub;
+        }
+    }
+    if (!s) s = verb_local(t.c, dt, sub_dt);
+    if (!s) s = verb_sync(t.c);
+    if (!s) s = verb_download_psd(t.c, psd);
+    if (!s && lu_cache && recompute_lu) s = verb_local_factor_lapack(t.c, 0, 0, lu_cache, index_cache);
+    cudaFree(dkv);
+    return s;
+}
+
+int verb_convection_1d(double* psd, const double* x, int n, double lbc, double ubc, int lbc_t,
+                       int ubc_t, const double* ux, double dt)
+{
+    if (!psd || !x || !ux || n < 11) return n < 11 ? VERB_ERR_GRID : VERB_ERR_ARG;
+    if ((lbc_t == VERB_BC_PERIODIC) != (ubc_t == VERB_BC_PERIODIC)) return VERB_ERR_BC;
+    double* dv = nullptr;
+    int* st = nullptr;
+    CK(cudaMalloc(&dv, sizeof(double) * 3 * n));
+    int s = cuda_ok(cudaMalloc(&st, sizeof(int)));
+    if (!s) s = cuda_ok(cudaMemset(st, 0, sizeof(int)));
+    if (!s) s = cuda_ok(cudaMemcpy(dv, psd, 8 * n, cudaMemcpyHostToDevice));
+    if (!s) s = cuda_ok(cudaMemcpy(dv + n, x, 8 * n, cudaMemcpyHostToDevice));
+    if (!s) s = cuda_ok(cudaMemcpy(dv + 2 * n, ux, 8 * n, cudaMemcpyHostToDevice));
+    if (!s) {
+        launch_convection_line(dv, dv + n, n, lbc, ubc, lbc_t, ubc_t, dv + 2 * n, dt, st, 0);
+        s = check_launch();
+    }
+    int dst = 0;
+    if (!s) s = cuda_ok(cudaMemcpy(psd, dv, 8 * n, cudaMemcpyDeviceToHost));
+    if (!s) s = cuda_ok(cudaMemcpy(&dst, st, sizeof(int), cudaMemcpyDeviceToHost));
+    cudaFree(dv);
+    cudaFree(st);
+    return s ? s : dst;
+}
+
+int verb_convection_2d(double* psd, const double* P, const double* R, int nP, int nR,
+                       const double* pl, const double* pu, const double* rl, const double* ru,
+                       int pl_t, int pu_t, int rl_t, int ru_t, const double* VP, const double* VR,
+                       const double* S, const double* loss, const double* G, double dt)
+{
+    if (!psd || !P || !R) return VERB_ERR_ARG;
+    TmpCtx t;
+    int s = verb_create(&t.c, nP, nR, 1, 1, nullptr);
+    if (s) return s;
+    int types[VERB_BCF_COUNT] = {pl_t, pu_t, rl_t, ru_t, 1, 1, 1, 1, 1, 1};
+    if ((s = verb_set_bc_types(t.c, types))) return s;
+    const int fids[8] = {VERB_F_PSD, VERB_F_P, VERB_F_R, VERB_F_VP, VERB_F_VR, VERB_F_SOURCES,
+                         VERB_F_LOSS_CONV, VERB_F_G_CONV};
+    const double* srcs[8] = {psd, P, R, VP, VR, S, loss, G};
+    for (int i = 0; i < 8; i++)
+        if ((s = verb_upload_field(t.c, fids[i], srcs[i]))) return s;
+    if ((s = verb_upload_bc(t.c, VERB_BCF_PL, pl))) return s;
+    if ((s = verb_upload_bc(t.c, VERB_BCF_PU, pu))) return s;
+    if ((s = verb_upload_bc(t.c, VERB_BCF_RL, rl))) return s;
+    if ((s = verb_upload_bc(t.c, VERB_BCF_RU, ru))) return s;
+    if ((s = verb_convection(t.c, dt))) return s;
+    if ((s = verb_sync(t.c))) return s;
+    return verb_download_psd(t.c, psd);
+}
+
+int verb_assimilate_radial(verb_ctx* c, const double* obs_host, double dt, double model_error,
+                           double obs_error, int p_index)
+{
+    if (!c || !obs_host || !(dt > 0)) return VERB_ERR_ARG;
+    const Dims& d = c->d;
+    if (d.R < 3 || d.R > 128) return VERB_ERR_ARG;
+    for (int fid : {VERB_F_PSD, VERB_F_R, VERB_F_DLL, VERB_F_G_RADIAL}) {
+        int s = need_field(c, fid);
+        if (s) return s;
+    }
+    for (int b : {VERB_BCF_LL, VERB_BCF_LU}) {
+        int s = need_bc(c, b);
+        if (s) return s;
+    }
+    const size_t cols = (size_t)d.P * d.V * d.K, RR = (size_t)d.R * d.R;
+    if (!c->Pa) {
+        CK(cudaMalloc(&c->Pa, cols * RR * sizeof(double)));
+        CK(cudaMemsetAsync(c->Pa, 0, cols * RR * sizeof(double), c->stream));
+    }
+    CK(alloc((void**)&c->obs, npts(c) * sizeof(double)));
+    CK(cudaMemcpyAsync(c->obs, obs_host, npts(c) * sizeof(double), cudaMemcpyHostToDevice,
+                       c->stream));
+    KFArgs a{};
+    a.d = d;
+    a.psd = c->f[VERB_F_PSD];
+    a.Rg = c->f[VERB_F_R];
+    a.DLL = c->f[VERB_F_DLL];
+    a.G = c->f[VERB_F_G_RADIAL];
+    a.Ll = c->bc[VERB_BCF_LL];
+    a.Lu = c->bc[VERB_BCF_LU];
+    a.dll_scale = 1.0;
+    a.Ll_t = c->bct[VERB_BCF_LL];
+    a.Lu_t = c->bct[VERB_BCF_LU];
+    a.obs = c->obs;
+    a.Pa = c->Pa;
+    a.dt = dt;
+    a.model_error = model_error;
+    a.obs_error = obs_error;
+    a.p_index = p_index;
+    a.status = c->status;
+    const int nctas = kf_ctas(d, p_index);
+    const size_t wb = (size_t)nctas * 5 * RR * sizeof(double);
+    if (wb > c->kfwork_bytes) {
+        cudaFree(c->kfwork);
+        c->kfwork = nullptr;
+        CK(cudaMalloc(&c->kfwork, wb));
+        c->kfwork_bytes = wb;
+    }
+    CK(alloc((void**)&c->kfticket, sizeof(int)));
+    a.work = c->kfwork;
+    a.ticket = c->kfticket;
+    PhaseTimer t(c, PH_KF);
+    launch_kf(a, nctas, c->stream);
+    return check_launch();
+}
+
+}  // extern "C"

@@ -1,0 +1,574 @@
+// Local (V,K) diffusion: banded LU with partial pivoting, factors cached in HBM.
+//
+// Reference: Diffusion_2D (src/Diffusion_2D.cpp:19-153) assembles a
+// 9-diagonal operator over the unknown index in = iK*V + iV
+// (AddBoundaries_2D and SecondDerivativeApproximation_2D,
+// src/MatrixSolver.cpp:118-213, 439-494) and Lapack
+// (src/MatrixSolver.cpp:223-340) factors it with dgbtrf (kl = ku = V+1) and
+// solves with dgbtrs once per diffusion sub-step.  With LU_CACHING the
+// factors are kept per (P,R) system and only recomputed when the local
+// coefficients change (src/VERB4D_Solver.cpp:1091-1096).
+//
+// Kernels:
+//  * local_factor_kernel: one CTA per system.  Rows of A are assembled on the
+//    device with the reference's operation order (bit-identical matrix) and
+//    factored by the unblocked banded LU of LAPACK's xGBTF2 (partial pivoting,
+//    multipliers scaled by the reciprocal pivot, rank-1 updates).
+//    The active (kl+1) x (kv+1) window lives in shared memory as a circular
+//    buffer over rows and columns.  Output: L multipliers (Lf, column j
+//    contiguous), U columns (Uf, rows j-kv..j contiguous) and 0-based pivots.
+//  * local_rhs_kernel / local_store_kernel: tile transposes between the PSD
+//    slab [V][K] and the unknown order, forming RHS = B o f + C.
+//  * local_solve_kernel: one warp per system, the forward (L, interleaved row
+//    swaps as in xGBTRS) and backward (U, column-oriented as in xTBSV)
+//    substitutions.  The solution window lives in shared memory; the factor
+//    columns stream through a per-warp cp.async ring so that each warp keeps
+//    several columns in flight.  This kernel moves the whole factor cache
+//    once per sub-step and is HBM-bound.
+//
+// All arithmetic follows the CPU restatement of xGBTF2/xGBTRS/xTBSV operation
+// by operation without FMA contraction (the file is compiled with
+// -fmad=false), so factors, pivots and solutions are bit-identical to it.
+#include "verb_internal.cuh"
+
+namespace verb {
+
+namespace {
+
+// slot of diagonal offset (dx,dy): offset = dy*nx + dx
+__device__ __forceinline__ int dslot(int dx, int dy) { return (dy + 1) * 3 + (dx + 1); }
+
+struct SysView {
+    const double *x, *y, *Dxx, *Dyy, *Dxy, *Dyx, *G, *S, *loss;
+    const double *xl, *xu, *yl, *yu;
+    int nx, ny;
+};
+
+__device__ __forceinline__ SysView sys_view(const LocalArgs& a, int sys)
+{
+    const size_t n = (size_t)a.d.V * a.d.K;
+    const size_t base = (size_t)sys * n;
+    SysView v;
+    v.x = a.Vg + base;
+    v.y = a.Kg + base;
+    v.Dxx = a.DVV + base;
+    v.Dyy = a.DKK + base;
+    v.Dxy = a.DVK + base;
+    v.Dyx = a.DKV + base;
+    v.G = a.G + base;
+    v.S = a.S + base;
+    v.loss = a.loss + base;
+    v.xl = a.Vl + (size_t)sys * a.d.K;
+    v.xu = a.Vu + (size_t)sys * a.d.K;
+    v.yl = a.Kl + (size_t)sys * a.d.V;
+    v.yu = a.Ku + (size_t)sys * a.d.V;
+    v.nx = a.d.V;
+    v.ny = a.d.K;
+    return v;
+}
+
+// SecondDerivativeApproximation_2D (src/MatrixSolver.cpp:439-494) adding into
+// the 9 diagonal values of row (ix,iy).
+__device__ __forceinline__ void sda2(double* r, const SysView& v, int ix, int iy, int dx1, int dy1,
+                                     int dx2, int dy2, const double* D, double mult)
+{
+    const int ny = v.ny;
+#define P2(a, b) ((a) * ny + (b))
+    const double x0 = v.x[P2(ix, iy)] + v.y[P2(ix, iy)];
+    const double x1 = v.x[P2(ix + dx1, iy + dy1)] + v.y[P2(ix + dx1, iy + dy1)];
+    const double x2 = v.x[P2(ix + dx2, iy + dy2)] + v.y[P2(ix + dx2, iy + dy2)];
+    const double x12 = v.x[P2(ix + dx1 + dx2, iy + dy1 + dy2)] + v.y[P2(ix + dx1 + dx2, iy + dy1 + dy2)];
+    const double dh1 = x0 - x1;
+    const double dh21 = x0 - x2;
+    const double dh22 = x1 - x12;
+    const double G0 = v.G[P2(ix, iy)], G1 = v.G[P2(ix + dx1, iy + dy1)];
+    const double D0 = D[P2(ix, iy)], D1 = D[P2(ix + dx1, iy + dy1)];
+    const double cp = mult / G0 / dh1;
+    r[dslot(0, 0)] += +cp / dh21 * D0 * G0;
+    r[dslot(dx2, dy2)] += -cp / dh21 * D0 * G0;
+    r[dslot(dx1, dy1)] += -cp / dh22 * D1 * G1;
+    r[dslot(dx1 + dx2, dy1 + dy2)] += +cp / dh22 * D1 * G1;
+#undef P2
+}
+
+// One row of matr_A (src/Diffusion_2D.cpp:68-130).  Returns 0 or VERB_ERR_BC.
+__device__ int assemble_row(const SysView& v, int types[4], double dt, int in, double r[9])
+{
+    const int nx = v.nx, ny = v.ny;
+    const int ix = in % nx, iy = in / nx;
+    const int p = ix * ny + iy;
+#pragma unroll
+    for (int s = 0; s < 9; s++) r[s] = 0.0;
+    int t = -1, s1 = 0;
+    double dh = 0.0;
+    if (ix == 0 && nx >= 3) {
+        t = types[0];
+        s1 = dslot(1, 0);
+        dh = v.x[p + ny] - v.x[p];
+    } else if (ix == nx - 1 && nx >= 3) {
+        t = types[1];
+        s1 = dslot(-1, 0);
+        dh = v.x[p] - v.x[p - ny];
+    } else if (iy == 0 && ny >= 3) {
+        t = types[2];
+        s1 = dslot(0, 1);
+        dh = v.y[p + 1] - v.y[p];
+    } else if (iy == ny - 1 && ny >= 3) {
+        t = types[3];
+        s1 = dslot(0, -1);
+        dh = v.y[p] - v.y[p - 1];
+    }
+    if (t >= 0) {
+        if (t == VERB_BC_CONSTANT_VALUE) {
+            r[4] = 1;
+            r[s1] = 0;
+        } else if (t == VERB_BC_CONSTANT_DERIVATIVE) {
+            r[4] = 1 / dh;
+            r[s1] = -1 / dh;
+        } else {
+            return VERB_ERR_BC;
+        }
+        return 0;
+    }
+    r[4] += 1.0 / dt;
+    r[4] -= v.loss[p];
+    if (nx >= 3) {
+        sda2(r, v, ix, iy, -1, 0, 1, 0, v.Dxx, -0.5);
+        sda2(r, v, ix, iy, 1, 0, -1, 0, v.Dxx, -0.5);
+    }
+    if (ny >= 3) {
+        sda2(r, v, ix, iy, 0, -1, 0, 1, v.Dyy, -0.5);
+        sda2(r, v, ix, iy, 0, 1, 0, -1, v.Dyy, -0.5);
+    }
+    if (nx >= 3 && ny >= 3) {
+        sda2(r, v, ix, iy, 0, -1, 1, 0, v.Dxy, -0.25);  // y_left,  x_right
+        sda2(r, v, ix, iy, 0, 1, -1, 0, v.Dxy, -0.25);  // y_right, x_left
+        sda2(r, v, ix, iy, 0, -1, -1, 0, v.Dxy, -0.25); // y_left,  x_left
+        sda2(r, v, ix, iy, 0, 1, 1, 0, v.Dxy, -0.25);   // y_right, x_right
+        sda2(r, v, ix, iy, -1, 0, 0, 1, v.Dyx, -0.25);  // x_left,  y_right (d/dy Dyx d/dx)
+        sda2(r, v, ix, iy, 1, 0, 0, -1, v.Dyx, -0.25);  // x_right, y_left
+        sda2(r, v, ix, iy, -1, 0, 0, -1, v.Dyx, -0.25); // x_left,  y_left
+        sda2(r, v, ix, iy, 1, 0, 0, 1, v.Dyx, -0.25);   // x_right, y_right
+    }
+    return 0;
+}
+
+__device__ __forceinline__ bool skip_system(const LocalArgs& a, int sys)
+{
+    if (a.include_boundary) return false;
+    const int r = sys % a.d.R;
+    return r == 0 || r == a.d.R - 1;
+}
+
+constexpr int FACT_THREADS = 512;
+constexpr int STAGE_ROWS = 128;
+
+__global__ void __launch_bounds__(FACT_THREADS) local_factor_kernel(LocalArgs a)
+{
+    extern __shared__ double sm[];
+    const int sys = blockIdx.x;
+    if (skip_system(a, sys)) return;
+    const int nx = a.d.V;
+    const int n = a.d.V * a.d.K;
+    const int kl = a.kl, ku = a.kl, kv = a.kv;
+    const int RW = kl + 1;          // window rows
+    const int CW = kv + 1;          // window columns (row pitch)
+    double* W = sm;                 // [RW][CW]
+    double* mult = W + (size_t)RW * CW;  // [RW]
+    double* colj = mult + RW;       // [RW]
+    double* stage = colj + RW;      // [STAGE_ROWS][9]
+    __shared__ int s_jp;
+    __shared__ double s_piv;
+    const SysView v = sys_view(a, sys);
+    int types[4] = {a.Vl_t, a.Vu_t, a.Kl_t, a.Ku_t};
+    double* Lf = a.Lf + (size_t)sys * n * a.klp;
+    double* Uf = a.Uf + (size_t)sys * n * a.kvp;
+    int32_t* ip = a.ipiv + (size_t)sys * n;
+    const int tid = threadIdx.x;
+
+    auto stage_rows = [&](int q0) {
+        for (int q = q0 + tid; q < q0 + 32 && q < n; q += blockDim.x) {
+            double r[9];
+            const int st = assemble_row(v, types, a.dt, q, r);
+            if (st) set_error(a.status, st);
+#pragma unroll
+            for (int s = 0; s < 9; s++) stage[(q & (STAGE_ROWS - 1)) * 9 + s] = r[s];
+        }
+    };
+    // value of original row q at window column slot cs, when the window's
+    // first column is c0 (column of slot cs is c0 + ((cs - c0%CW) mod CW))
+    auto row_value = [&](int q, int col) -> double {
+        const int d = col - q;
+        const int dy = (d < -1) ? -1 : (d > 1 ? 1 : 0);
+        const int dx = d - dy * nx;
+        if (dx < -1 || dx > 1 || col < 0 || col >= n) return 0.0;
+        return stage[(q & (STAGE_ROWS - 1)) * 9 + dslot(dx, dy)];
+    };
+
+    for (int i = tid; i < RW * CW; i += blockDim.x) W[i] = 0.0;
+    for (int q0 = 0; q0 < STAGE_ROWS; q0 += 32) stage_rows(q0);
+    __syncthreads();
+    // rows 0..kl into the window (columns 0..kv)
+    for (int i = tid; i < RW * CW; i += blockDim.x) {
+        const int q = i / CW, c = i - q * CW;
+        if (q < n) W[q * CW + c] = row_value(q, c);
+    }
+    __syncthreads();
+
+    int ju = 0;
+    for (int j = 0; j < n; j++) {
+        const int km = min(kl, n - 1 - j);
+        const int rsj = j % RW, csj = j % CW;
+        // [A] pivot: first index of max |column j| over rows j..j+km (idamax)
+        if (tid < 32) {
+            double best = -1.0;
+            int bi = 0;
+            for (int i = tid; i <= km; i += 32) {
+                const double val = W[((j + i) % RW) * CW + csj];
+                colj[i] = val;
+                const double av = fabs(val);
+                if (av > best) {
+                    best = av;
+                    bi = i;
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi)) {
+                    best = ob;
+                    bi = oi;
+                }
+            }
+            if (tid == 0) {
+                s_jp = bi;
+                s_piv = W[((j + bi) % RW) * CW + csj];
+                ip[j] = j + bi;
+            }
+        }
+        __syncthreads();
+        const int jp = s_jp;
+        const double piv = s_piv;
+        const bool nz = piv != 0.0;
+        if (nz) {
+            ju = max(ju, min(j + ku + jp, n - 1));
+            // [B] multipliers (from the pre-swap column) and the row swap
+            const double rcp = 1.0 / piv;
+            for (int i = 1 + tid; i <= km; i += blockDim.x) {
+                const double val = (i == jp) ? colj[0] : colj[i];
+                const double m = val * rcp;
+                mult[i] = m;
+                Lf[(size_t)j * a.klp + (i - 1)] = m;
+            }
+            if (jp != 0) {
+                const int rp = (j + jp) % RW;
+                for (int c = j + tid; c <= ju; c += blockDim.x) {
+                    const int cs = c % CW;
+                    const double t = W[rsj * CW + cs];
+                    W[rsj * CW + cs] = W[rp * CW + cs];
+                    W[rp * CW + cs] = t;
+                }
+            }
+        } else {
+            set_error(a.status, VERB_ERR_PIVOT);
+            for (int i = 1 + tid; i <= km; i += blockDim.x) Lf[(size_t)j * a.klp + (i - 1)] = colj[i];
+        }
+        __syncthreads();
+        // [C] U row j out; rank-1 update of rows j+1..j+km, columns j+1..ju
+        for (int c = j + tid; c <= ju && c <= j + kv; c += blockDim.x)
+            Uf[(size_t)c * a.kvp + (kv - (c - j))] = W[rsj * CW + (c % CW)];
+        if (nz && km > 0 && ju > j) {
+            const int ncol = ju - j;
+            const int cg = tid & 127;        // column lane
+            const int rg = tid >> 7;         // row group 0..3
+            for (int cc = cg; cc < ncol; cc += 128) {
+                const int cs = (j + 1 + cc) % CW;
+                const double yv = W[rsj * CW + cs];
+                if (yv != 0.0) {
+                    const double tmp = -yv;
+                    for (int i = 1 + rg; i <= km; i += 4) {
+                        double* w = &W[((j + i) % RW) * CW + cs];
+                        *w = *w + mult[i] * tmp;  // xGER: A(i,k) + x(i)*temp
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        // [D] slide: row slot j <- original row j+kl+1, column slot j <- column j+kv+1
+        const int q = j + kl + 1;
+        if (q < n && (q & 31) == 0 && q >= STAGE_ROWS) {
+            stage_rows(q);
+            __syncthreads();
+        }
+        for (int cs = tid; cs < CW; cs += blockDim.x) {
+            double val = 0.0;
+            if (q < n) {
+                const int c0 = j + 1;
+                const int col = c0 + ((cs - (c0 % CW)) % CW + CW) % CW;
+                val = row_value(q, col);
+            }
+            W[rsj * CW + cs] = val;
+        }
+        for (int rs = tid; rs < RW; rs += blockDim.x)
+            if (rs != rsj) W[rs * CW + csj] = 0.0;
+        __syncthreads();
+    }
+}
+
+// RHS = B o f + C in unknown order (src/MatrixSolver.cpp:309-320), through a
+// 32x32 shared-memory tile transpose of the [V][K] slab.
+__global__ void local_rhs_kernel(LocalArgs a, int from_work)
+{
+    __shared__ double tile[32][33];
+    const int sys = blockIdx.z;
+    if (skip_system(a, sys)) return;
+    const int V = a.d.V, K = a.d.K;
+    const size_t n = (size_t)V * K;
+    const double* psd = a.psd + (size_t)sys * n;
+    double* w = a.work + (size_t)sys * n;
+    const int v0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+    if (!from_work) {
+        for (int r = ty; r < 32; r += 8) {
+            const int iv = v0 + r, ik = k0 + tx;
+            if (iv < V && ik < K) tile[r][tx] = psd[(size_t)iv * K + ik];
+        }
+    } else {
+        for (int r = ty; r < 32; r += 8) {
+            const int ik = k0 + r, iv = v0 + tx;
+            if (iv < V && ik < K) tile[tx][r] = w[(size_t)ik * V + iv];
+        }
+    }
+    __syncthreads();
+    const SysView sv = sys_view(a, sys);
+    const double bint = 0.0 + 1.0 / a.dt;
+    const double ls = (double)a.local_sources;
+    for (int r = ty; r < 32; r += 8) {
+        const int ik = k0 + r, iv = v0 + tx;
+        if (iv >= V || ik >= K) continue;
+        const int ix = iv, iy = ik;
+        double b, c;
+        if (ix == 0 && V >= 3) {
+            b = 0.0;
+            c = sv.xl[iy];
+        } else if (ix == V - 1 && V >= 3) {
+            b = 0.0;
+            c = sv.xu[iy];
+        } else if (iy == 0 && K >= 3) {
+            b = 0.0;
+            c = sv.yl[ix];
+        } else if (iy == K - 1 && K >= 3) {
+            b = 0.0;
+            c = sv.yu[ix];
+        } else {
+            b = bint;
+            c = 0.0;
+            c += sv.S[(size_t)ix * K + iy] * ls;
+        }
+        double rhs = tile[tx][r];
+        rhs *= b;
+        rhs += c;
+        w[(size_t)ik * V + iv] = rhs;
+    }
+}
+
+__global__ void local_store_kernel(LocalArgs a)
+{
+    __shared__ double tile[32][33];
+    const int sys = blockIdx.z;
+    if (skip_system(a, sys)) return;
+    const int V = a.d.V, K = a.d.K;
+    const size_t n = (size_t)V * K;
+    double* psd = a.psd + (size_t)sys * n;
+    const double* w = a.work + (size_t)sys * n;
+    const int v0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    for (int r = ty; r < 32; r += 8) {
+        const int ik = k0 + r, iv = v0 + tx;
+        if (iv < V && ik < K) tile[tx][r] = w[(size_t)ik * V + iv];
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        const int iv = v0 + r, ik = k0 + tx;
+        if (iv < V && ik < K) psd[(size_t)iv * K + ik] = tile[r][tx];
+    }
+}
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+constexpr int SOLVE_WARPS = 4;
+constexpr int FWD_DEPTH = 4;   // L columns in flight per warp
+constexpr int BWD_DEPTH = 2;   // U columns in flight per warp
+constexpr int FWD_WIN = 128;   // >= kl + 1
+constexpr int BWD_WIN = 256;   // >= kv + 1
+
+__host__ __device__ constexpr size_t solve_ring_doubles(int klp, int kvp)
+{
+    return (size_t)(FWD_DEPTH * klp > BWD_DEPTH * kvp ? FWD_DEPTH * klp : BWD_DEPTH * kvp);
+}
+
+__global__ void __launch_bounds__(SOLVE_WARPS * 32) local_solve_kernel(LocalArgs a, int nsys)
+{
+    extern __shared__ double sm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int sys = blockIdx.x * SOLVE_WARPS + warp;
+    if (sys >= nsys || skip_system(a, sys)) return;
+    const int n = a.d.V * a.d.K;
+    const int kl = a.kl, kv = a.kv, klp = a.klp, kvp = a.kvp;
+    const size_t per_warp = BWD_WIN + solve_ring_doubles(klp, kvp);
+    double* win = sm + (size_t)warp * per_warp;
+    double* ring = win + BWD_WIN;
+    double* w = a.work + (size_t)sys * n;
+    const double* Lf = a.Lf + (size_t)sys * n * klp;
+    const double* Uf = a.Uf + (size_t)sys * n * kvp;
+    const int32_t* ip = a.ipiv + (size_t)sys * n;
+
+    // ---------------- forward: L with interleaved row interchanges (xGBTRS) --------
+    for (int i = lane; i < FWD_WIN && i < n; i += 32) win[i] = w[i];
+    auto issue_L = [&](int col) {
+        if (col < n - 1) {
+            double* dst = ring + (col % FWD_DEPTH) * klp;
+            const double* src = Lf + (size_t)col * klp;
+            for (int c = lane; c < klp / 2; c += 32) cp_async16(dst + 2 * c, src + 2 * c);
+        }
+    };
+    for (int c = 0; c < FWD_DEPTH; c++) {
+        issue_L(c);
+        cp_commit();
+    }
+    int pv_cur = (lane < n) ? ip[lane] : 0;
+    int pv_next = (32 + lane < n) ? ip[32 + lane] : 0;
+    __syncwarp();
+    for (int j = 0; j < n - 1; j++) {
+        if ((j & 31) == 0 && j > 0) {
+            pv_cur = pv_next;
+            const int nx = j + 32 + lane;
+            pv_next = (nx < n) ? ip[nx] : 0;
+        }
+        cp_wait<FWD_DEPTH - 1>();
+        __syncwarp();
+        const int lm = min(kl, n - 1 - j);
+        const int l = __shfl_sync(0xffffffffu, pv_cur, j & 31);
+        const double bj_old = win[j & (FWD_WIN - 1)];
+        const double bl = win[l & (FWD_WIN - 1)];
+        const double bj = (l != j) ? bl : bj_old;
+        const double* Lc = ring + (j % FWD_DEPTH) * klp;
+        const double tmp = -bj;
+        const bool upd = bj != 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int t = lane + 32 * k;
+            const int i = j + 1 + t;
+            if (t < lm) {
+                double cur = (i == l) ? bj_old : win[i & (FWD_WIN - 1)];
+                if (upd) cur = cur + Lc[t] * tmp;  // xGER in xGBTRS
+                win[i & (FWD_WIN - 1)] = cur;
+            }
+        }
+        __syncwarp();
+        if (lane == 0) {
+            w[j] = bj;
+            if (j + FWD_WIN < n) cp_async8(&win[j & (FWD_WIN - 1)], &w[j + FWD_WIN]);
+        }
+        issue_L(j + FWD_DEPTH);
+        cp_commit();
+    }
+    cp_wait<0>();
+    __syncwarp();
+    if (lane == 0) w[n - 1] = win[(n - 1) & (FWD_WIN - 1)];
+    __syncwarp();
+
+    // ---------------- backward: U, column oriented (xTBSV 'U','N','N') ------------
+    for (int i = n - 1 - lane; i >= 0 && i > n - 1 - BWD_WIN; i -= 32) win[i & (BWD_WIN - 1)] = w[i];
+    auto issue_U = [&](int col) {
+        if (col >= 0) {
+            double* dst = ring + ((n - 1 - col) % BWD_DEPTH) * kvp;
+            const double* src = Uf + (size_t)col * kvp;
+            for (int c = lane; c < kvp / 2; c += 32) cp_async16(dst + 2 * c, src + 2 * c);
+        }
+    };
+    for (int c = 0; c < BWD_DEPTH; c++) {
+        issue_U(n - 1 - c);
+        cp_commit();
+    }
+    __syncwarp();
+    for (int j = n - 1; j >= 0; j--) {
+        cp_wait<BWD_DEPTH - 1>();
+        __syncwarp();
+        const double* Uc = ring + ((n - 1 - j) % BWD_DEPTH) * kvp;
+        double bj = win[j & (BWD_WIN - 1)];
+        if (bj != 0.0) {
+            bj = bj / Uc[kv];
+#pragma unroll
+            for (int k = 0; k < 7; k++) {
+                const int d = 1 + lane + 32 * k;
+                const int i = j - d;
+                if (d <= kv && i >= 0) {
+                    double* x = &win[i & (BWD_WIN - 1)];
+                    *x = *x - bj * Uc[kv - d];  // xTBSV: X(I) - TEMP*A(L+I,J)
+                }
+            }
+        }
+        __syncwarp();
+        if (lane == 0) {
+            w[j] = bj;
+            if (j - BWD_WIN >= 0) cp_async8(&win[j & (BWD_WIN - 1)], &w[j - BWD_WIN]);
+        }
+        issue_U(j - BWD_DEPTH);
+        cp_commit();
+    }
+    cp_wait<0>();
+}
+
+}  // namespace
+
+size_t local_factor_smem(int V)
+{
+    const int kl = V + 1, kv = 2 * kl;
+    return ((size_t)(kl + 1) * (kv + 1) + 2 * (kl + 1) + STAGE_ROWS * 9) * sizeof(double);
+}
+
+void launch_local_factor(const LocalArgs& a, cudaStream_t s)
+{
+    const size_t smem = local_factor_smem(a.d.V);
+    cudaFuncSetAttribute(local_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    local_factor_kernel<<<a.d.P * a.d.R, FACT_THREADS, smem, s>>>(a);
+}
+
+void launch_local_rhs(const LocalArgs& a, bool from_work, cudaStream_t s)
+{
+    dim3 grid((a.d.K + 31) / 32, (a.d.V + 31) / 32, a.d.P * a.d.R);
+    local_rhs_kernel<<<grid, dim3(32, 8), 0, s>>>(a, from_work ? 1 : 0);
+}
+
+void launch_local_store(const LocalArgs& a, cudaStream_t s)
+{
+    dim3 grid((a.d.K + 31) / 32, (a.d.V + 31) / 32, a.d.P * a.d.R);
+    local_store_kernel<<<grid, dim3(32, 8), 0, s>>>(a);
+}
+
+void launch_local_solve(const LocalArgs& a, cudaStream_t s)
+{
+    const int nsys = a.d.P * a.d.R;
+    const size_t smem =
+        (size_t)SOLVE_WARPS * (BWD_WIN + solve_ring_doubles(a.klp, a.kvp)) * sizeof(double);
+    cudaFuncSetAttribute(local_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    local_solve_kernel<<<(nsys + SOLVE_WARPS - 1) / SOLVE_WARPS, SOLVE_WARPS * 32, smem, s>>>(a, nsys);
+}
+
+}  // namespace verb

@@ -1,0 +1,109 @@
+// Step reductions and elementwise passes over whole 4-D fields.
+//  * negative-point count  (src/VERB4D_Solver.cpp:1226-1240), exact integer
+//  * min(DVV*DKK - DVK*DVK) (src/VERB4D_Solver.cpp:747-753), exact min
+//  * max(PSD, 1e-21)        (src/VERB4D_Solver.cpp:621, 980, 1072, 1219)
+//  * field = base * scale   (UpdatableMatrix scale queue, src/UpdatableMatrix.cpp:698-708)
+// Grid-stride loops sized to a multiple of the SM count; one atomic per block.
+#include "verb_internal.cuh"
+
+namespace verb {
+
+namespace {
+
+constexpr int RT = 256;
+
+int grid_for(size_t n)
+{
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    size_t want = (n + RT - 1) / RT;
+    size_t cap = (size_t)sms * 8;
+    return (int)(want < cap ? (want > 0 ? want : 1) : cap);
+}
+
+__global__ void negative_count_kernel(const double* __restrict__ psd, size_t n,
+                                      unsigned long long* out)
+{
+    unsigned long long c = 0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        c += psd[i] < 0 ? 1ull : 0ull;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    __shared__ unsigned long long red[RT / 32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int i = 0; i < RT / 32; i++) t += red[i];
+        atomicAdd(out, t);
+    }
+}
+
+__global__ void tensor_min_kernel(const double* __restrict__ dvv, const double* __restrict__ dkk,
+                                  const double* __restrict__ dvk, size_t n,
+                                  unsigned long long* out)
+{
+    double m = INFINITY;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const double v = dvv[i] * dkk[i] - dvk[i] * dvk[i];
+        m = (v < m) ? v : m;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const double t = __shfl_xor_sync(0xffffffffu, m, o);
+        m = (t < m) ? t : m;
+    }
+    __shared__ double red[RT / 32];
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = red[0];
+        for (int i = 1; i < RT / 32; i++) t = (red[i] < t) ? red[i] : t;
+        atomicMin(out, dkey(t));
+    }
+}
+
+__global__ void clamp_kernel(double* psd, size_t n)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const double v = psd[i];
+        psd[i] = (v < 1e-21) ? 1e-21 : v;  // std::max(v, 1e-21)
+    }
+}
+
+__global__ void scale_copy_kernel(double* dst, const double* __restrict__ src, double scale,
+                                  size_t n)
+{
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = src[i] * scale;
+}
+
+}  // namespace
+
+void launch_negative_count(const double* psd, size_t n, unsigned long long* out, cudaStream_t s)
+{
+    cudaMemsetAsync(out, 0, sizeof(unsigned long long), s);
+    negative_count_kernel<<<grid_for(n), RT, 0, s>>>(psd, n, out);
+}
+
+void launch_tensor_min(const double* dvv, const double* dkk, const double* dvk, size_t n,
+                       unsigned long long* out, cudaStream_t s)
+{
+    cudaMemsetAsync(out, 0xff, sizeof(unsigned long long), s);
+    tensor_min_kernel<<<grid_for(n), RT, 0, s>>>(dvv, dkk, dvk, n, out);
+}
+
+void launch_clamp_positive(double* psd, size_t n, cudaStream_t s)
+{
+    clamp_kernel<<<grid_for(n), RT, 0, s>>>(psd, n);
+}
+
+void launch_scale_copy(double* dst, const double* src, double scale, size_t n, cudaStream_t s)
+{
+    scale_copy_kernel<<<grid_for(n), RT, 0, s>>>(dst, src, scale, n);
+}
+
+}  // namespace verb
