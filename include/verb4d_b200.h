@@ -85,6 +85,7 @@ typedef struct {
     double convection_ms, radial_ms, radial_factor_ms, local_ms, local_factor_ms,
         local_solve_ms, reduce_ms, kf_ms;
     long long steps, local_solve_launches, local_factor_launches;
+    long long kernel_launches;  /* every kernel this context launched since timing was enabled */
 } verb_timing;
 
 /* ---- context lifetime ---------------------------------------------------- */

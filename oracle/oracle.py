@@ -200,7 +200,7 @@ class OracleStepper:
               "G_radial", "G_conv", "S", "loss_local", "loss_radial", "loss_conv", "Pl", "Pu", "Rl",
               "Ru", "Ll", "Lu", "Vl", "Vu", "Kl", "Ku")
 
-    def __init__(self, inputs: dict, lib: "_Lib | None" = None):
+    def __init__(self, inputs: dict, lib: "_Lib | None" = None, lu_cache: bool = True):
         self.lib = lib or oracle()
         self.keep = {k: _f64(inputs[k]) for k in self.FIELDS}
         self.psd = _f64(inputs["psd"]).copy()
@@ -222,12 +222,14 @@ class OracleStepper:
         st.positive_psd = int(flags.get("positive_psd", 0))
         n = V * K
         ldab = 3 * (V + 1) + 1
-        self.lu = np.zeros(P * R * ldab * n)
-        self.ipiv = np.zeros(P * R * n, dtype=np.int64)
-        st.lu = _p(self.lu)
-        st.ipiv = self.ipiv.ctypes.data_as(_lp)
+        if lu_cache:
+            self.lu = np.zeros(P * R * ldab * n)
+            self.ipiv = np.zeros(P * R * n, dtype=np.int64)
+            st.lu = _p(self.lu)
+            st.ipiv = self.ipiv.ctypes.data_as(_lp)
         self.st = st
-        self.lib.lib.orc_step.restype = C.c_long
+        if self.lib.has("orc_step"):
+            self.lib.lib.orc_step.restype = C.c_long
 
     def step(self, dt: float, sub_dt: float, recompute_lu: bool) -> int:
         return int(self.lib.lib.orc_step(C.byref(self.st), C.c_double(dt), C.c_double(sub_dt),

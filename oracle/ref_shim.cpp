@@ -180,3 +180,105 @@ int ref_kf_diffusion_1d(double* forecast, double* Pa, double* F, double* Pf, con
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Phase loops for timing the reference CPU path: the OpenMP loops of
+// src/VERB4D_Solver.cpp (convection :885-978, radial :1009-1070, local
+// :1101-1216) over a caller-chosen list of slices, each slice solved by the
+// reference routine.  Slices are copied out of and back into the 4-D arrays
+// as the reference's yzSlice / wyzSlice / wxSlice do.  `st` points to the
+// oracle's orc_state (oracle/verb_oracle.h), which carries the same fields.
+#include <omp.h>
+
+#include "../oracle/verb_oracle.h"
+
+extern "C" {
+
+int ref_conv_slices(orc_state* s, double dt, const int* vk, int nlist, int nthreads)
+{
+    const int P = s->P, R = s->R, V = s->V, K = s->K;
+    auto I4 = [&](int p, int r, int v, int k) { return (((size_t)p * R + r) * V + v) * K + k; };
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+    for (int t = 0; t < nlist; t++) {
+        const int iV = vk[2 * t], iK = vk[2 * t + 1];
+        Matrix2D<double> f(P, R), pg(P, R), rg(P, R), vp(P, R), vr(P, R), sr(P, R), ls(P, R), gg(P, R);
+        Matrix1D<double> pl(R), pu(R), rl(P), ru(P);
+        for (int iP = 0; iP < P; iP++)
+            for (int iR = 0; iR < R; iR++) {
+                const size_t g = I4(iP, iR, iV, iK);
+                f[iP][iR] = s->psd[g];
+                pg[iP][iR] = s->Pg[g];
+                rg[iP][iR] = s->Rg[g];
+                vp[iP][iR] = s->VP[g];
+                vr[iP][iR] = s->VR[g];
+                sr[iP][iR] = s->S[g];
+                ls[iP][iR] = s->loss_conv[g];
+                gg[iP][iR] = s->G_conv[g];
+            }
+        for (int iR = 0; iR < R; iR++) {
+            pl[iR] = s->Pl[((size_t)iR * V + iV) * K + iK];
+            pu[iR] = s->Pu[((size_t)iR * V + iV) * K + iK];
+        }
+        for (int iP = 0; iP < P; iP++) {
+            rl[iP] = s->Rl[((size_t)iP * V + iV) * K + iK];
+            ru[iP] = s->Ru[((size_t)iP * V + iV) * K + iK];
+        }
+        Convection_2D(f, pg, rg, P, R, pl, pu, rl, ru, bct(s->Pl_t), bct(s->Pu_t), bct(s->Rl_t),
+                      bct(s->Ru_t), vp, vr, sr, ls, gg, dt);
+        for (int iP = 0; iP < P; iP++)
+            for (int iR = 0; iR < R; iR++) s->psd[I4(iP, iR, iV, iK)] = f[iP][iR];
+    }
+    return 0;
+}
+
+int ref_radial_lines(orc_state* s, double dt, const int* pvk, int nlist, int nthreads)
+{
+    const int R = s->R, V = s->V, K = s->K;
+    const double rs = (double)s->radial_sources;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+    for (int t = 0; t < nlist; t++) {
+        const int iP = pvk[3 * t], iV = pvk[3 * t + 1], iK = pvk[3 * t + 2];
+        Matrix1D<double> f(R), lg(R), dl(R), sr(R), gr(R), ls(R);
+        for (int iR = 0; iR < R; iR++) {
+            const size_t g = (((size_t)iP * R + iR) * V + iV) * K + iK;
+            f[iR] = s->psd[g];
+            lg[iR] = s->Lg[g];
+            dl[iR] = s->DLL[g];
+            sr[iR] = s->S[g];
+            gr[iR] = s->G_radial[g];
+            ls[iR] = s->loss_radial[g];
+        }
+        sr *= rs;
+        const size_t b = ((size_t)iP * V + iV) * K + iK;
+        Diffusion_1D(f, lg, R, s->Ll[b], s->Lu[b], bct(s->Ll_t), bct(s->Lu_t), dl, gr, sr, ls, dt);
+        for (int iR = 0; iR < R; iR++) s->psd[(((size_t)iP * R + iR) * V + iV) * K + iK] = f[iR];
+    }
+    return 0;
+}
+
+#ifdef LU_CACHING
+// lu / ipiv: one cache slot per list entry ((2kl+ku+1)*n doubles, n longs).
+int ref_local_systems(orc_state* s, double dt, double sub_dt, const int* pr, int nlist,
+                      double* lu, long* ipiv, int recompute, int nthreads)
+{
+    const int R = s->R, V = s->V, K = s->K;
+    const size_t n = (size_t)V * K, ldab = 3 * (V + 1) + 1;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+    for (int t = 0; t < nlist; t++) {
+        const int iP = pr[2 * t], iR = pr[2 * t + 1];
+        const size_t base = ((size_t)iP * R + iR) * n, q = (size_t)iP * R + iR;
+        Matrix2D<double> f = mat(s->psd + base, V, K);
+        Matrix2D<double> src = mat(s->S + base, V, K) * s->local_sources;
+        Diffusion_2D(f, mat(s->Vg + base, V, K), mat(s->Kg + base, V, K), V, K, vec(s->Vl + q * K, K),
+                     vec(s->Vu + q * K, K), vec(s->Kl + q * V, V), vec(s->Ku + q * V, V),
+                     bct(s->Vl_t), bct(s->Vu_t), bct(s->Kl_t), bct(s->Ku_t), mat(s->DVV + base, V, K),
+                     mat(s->DKK + base, V, K), mat(s->DVK + base, V, K), mat(s->DVK + base, V, K),
+                     mat(s->G_local + base, V, K), src, mat(s->loss_local + base, V, K), dt, sub_dt,
+                     lu + t * ldab * n, ipiv + t * n, recompute != 0);
+        std::memcpy(s->psd + base, f[0], sizeof(double) * n);
+    }
+    return 0;
+}
+#endif
+
+}  // extern "C"

@@ -55,14 +55,27 @@ def test_convection_1d_bitexact(gpu, gold):
         assert np.array_equal(out, gold[f"c1_{c}_out"]), c
 
 
-def test_convection_2d_bitexact(gpu, gold):
+# exp(Loss*dt) (src/Convection_2D.cpp:101) comes from CUDA's exp on the device and
+# from the host libm in the reference; the two may differ by one ulp, so with
+# non-zero loss rates convection agrees to rounding, and bit for bit without.
+EXP_RTOL = 1e-13
+
+
+def test_convection_2d(gpu, gold, oracle_lib):
     for c in range(3):
         g = sub(gold, f"c2_{c}_")
         nP, nR = g["psd"].shape
-        out = ops.Convection_2D(g["psd"], g["P"], g["R"], nP, nR, g["pl"], g["pu"], g["rl"], g["ru"],
-                                0, 0, 1, 1, g["VP"], g["VR"], g["S"], g["loss"], g["G"],
-                                float(g["dt"]))
-        assert np.array_equal(out, g["out"]), c
+        args = (g["P"], g["R"], nP, nR, g["pl"], g["pu"], g["rl"], g["ru"], 0, 0, 1, 1, g["VP"],
+                g["VR"], g["S"])
+        out = ops.Convection_2D(g["psd"], *args, g["loss"], g["G"], float(g["dt"]))
+        assert rel(out, g["out"]) < EXP_RTOL, c
+        # without loss rates: bit-identical to the oracle (itself bit-identical to the reference)
+        zero = np.zeros_like(g["loss"])
+        out0 = ops.Convection_2D(g["psd"], *args, zero, g["G"], float(g["dt"]))
+        _, ref0, _ = oracle_lib.convection_2d(g["psd"], g["P"], g["R"], g["pl"], g["pu"], g["rl"],
+                                              g["ru"], (0, 0, 1, 1), g["VP"], g["VR"], g["S"], zero,
+                                              g["G"], float(g["dt"]))
+        assert np.array_equal(out0, ref0), c
 
 
 def test_diffusion_2d_vs_reference_and_oracle(gpu, gold, oracle_lib):

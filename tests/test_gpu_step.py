@@ -19,6 +19,15 @@ from verb4d_b200 import workload as W
 
 pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
+# exp(Loss_conv*dt) uses CUDA's exp on the device and the host libm in the
+# oracle (one-ulp differences), so steps with convection loss rates agree to
+# rounding; everything else is compared bit for bit.
+EXP_RTOL = 1e-13
+
+
+def without_conv_loss(wl):
+    wl.fields["loss_conv"] = np.zeros_like(wl.fields["loss_conv"])
+    return wl
 
 
 def load_ctx(wl):
@@ -39,10 +48,9 @@ def load_ctx(wl):
 def test_small_grid_steps_bitexact(gpu, oracle_lib):
     import make_golden as MG
 
-    wl = MG.step_workload()
+    wl = without_conv_loss(MG.step_workload())
     c = load_ctx(wl)
     st = O.OracleStepper(W.oracle_inputs(wl), oracle_lib)
-    g = np.load(os.path.join(GOLD, "step.npz"))
     for k in range(3):
         n_gpu = c.step(wl.dt, wl.sub_dt, count_negatives=True)
         c.sync()
@@ -50,9 +58,24 @@ def test_small_grid_steps_bitexact(gpu, oracle_lib):
         psd = c.download()
         assert np.array_equal(psd, st.psd), f"step {k}: max diff {np.abs(psd - st.psd).max()}"
         assert n_gpu == n_orc
-        if k < 2:  # against the reference-driven fixture (rounding-level tolerance)
-            ref = g[f"psd{k + 1}"]
-            assert np.abs(psd - ref).max() / np.abs(ref).max() < 1e-10
+    c.close()
+
+
+def test_small_grid_steps_vs_reference_fixture(gpu, oracle_lib):
+    import make_golden as MG
+
+    wl = MG.step_workload()
+    c = load_ctx(wl)
+    st = O.OracleStepper(W.oracle_inputs(wl), oracle_lib)
+    g = np.load(os.path.join(GOLD, "step.npz"))
+    for k in range(2):
+        c.step(wl.dt, wl.sub_dt)
+        c.sync()
+        st.step(wl.dt, wl.sub_dt, k == 0)
+        psd = c.download()
+        assert np.abs(psd - st.psd).max() / np.abs(st.psd).max() < EXP_RTOL
+        ref = g[f"psd{k + 1}"]  # the reference-driven fixture (LU rounding-level tolerance)
+        assert np.abs(psd - ref).max() / np.abs(ref).max() < 1e-10
     P, R, V, K = wl.spec.shape
     assert np.array_equal(c.local_pivots().reshape(P * R, V * K), st.ipiv.reshape(P * R, V * K))
     assert np.array_equal(c.local_pivots().reshape(P * R, V * K) + 1, g["ipiv"])
@@ -60,7 +83,8 @@ def test_small_grid_steps_bitexact(gpu, oracle_lib):
 
 
 def test_phases_separately(gpu, oracle_lib):
-    wl = W.make_workload(W.GridSpec(14, 15, 12, 13), seed=21, sources=True, losses=True)
+    wl = without_conv_loss(W.make_workload(W.GridSpec(14, 15, 12, 13), seed=21, sources=True,
+                                           losses=True))
     wl.fields["VP"] = wl.fields["VP"] * 3e-3
     inp = W.oracle_inputs(wl)
     for phase in ("convection", "radial", "local"):
@@ -80,7 +104,8 @@ def test_phases_separately(gpu, oracle_lib):
 def test_sub_steps_and_options(gpu, oracle_lib):
     # two local sub-steps, sources routed to the radial step, positive_PSD clamp,
     # and include_boundary = false (src/VERB4D_Solver.cpp:1117)
-    wl = W.make_workload(W.GridSpec(12, 12, 11, 11), seed=4, sources=True, losses=True)
+    wl = without_conv_loss(W.make_workload(W.GridSpec(12, 12, 11, 11), seed=4, sources=True,
+                                           losses=True))
     wl.fields["VP"] = wl.fields["VP"] * 3e-3
     wl.sub_dt = wl.dt / 2.0
     wl.flags.update(radial_sources=1, local_sources=0, include_boundary=0, positive_psd=1)

@@ -234,12 +234,14 @@ int radial_run(verb_ctx* c, double dt)
     if (c->radial_dirty || dt != c->radial_dt) {
         PhaseTimer t(c, PH_RADF);
         launch_radial_factor(a, c->stream);
+        c->acc.kernel_launches++;
         c->radial_dirty = false;
         c->radial_dt = dt;
     }
     {
         PhaseTimer t(c, PH_RAD);
         launch_radial_solve(a, c->stream);
+        c->acc.kernel_launches++;
     }
     return check_launch();
 }
@@ -307,6 +309,7 @@ int local_factor(verb_ctx* c, LocalArgs& a)
     const size_t nsys = (size_t)c->d.P * c->d.R, n = (size_t)c->d.V * c->d.K;
     CK(cudaMemsetAsync(c->Uf, 0, nsys * n * c->kvp * sizeof(double), c->stream));
     launch_local_factor(a, c->stream);
+    c->acc.kernel_launches++;
     c->local_dirty = false;
     c->local_dt = a.dt;
     c->acc.local_factor_launches++;
@@ -330,13 +333,16 @@ int local_run(verb_ctx* c, double dt, double sub_dt)
     }
     for (int k = 0; k < nsub; k++) {
         launch_local_rhs(a, k > 0, c->stream);
+        c->acc.kernel_launches++;
         {
             PhaseTimer ts(c, PH_LOCS);
             launch_local_solve(a, c->stream);
+            c->acc.kernel_launches++;
         }
         c->acc.local_solve_launches++;
     }
     launch_local_store(a, c->stream);
+    c->acc.kernel_launches++;
     return check_launch();
 }
 
@@ -387,6 +393,7 @@ int conv_run(verb_ctx* c, double dt)
     PhaseTimer t(c, PH_CONV);
     CK(cudaMemsetAsync(c->ticket, 0, sizeof(int), c->stream));
     launch_convection(a, c->conv_nctas, c->stream);
+    c->acc.kernel_launches++;
     return check_launch();
 }
 
@@ -400,6 +407,7 @@ int tensor_check(verb_ctx* c, double* out)
         CK(alloc((void**)&c->red, 2 * sizeof(unsigned long long)));
         launch_tensor_min(c->f[VERB_F_DVV], c->f[VERB_F_DKK], c->f[VERB_F_DVK], npts(c), c->red + 1,
                           c->stream);
+        c->acc.kernel_launches++;
         unsigned long long k = 0;
         CK(cudaMemcpyAsync(&k, c->red + 1, sizeof(k), cudaMemcpyDeviceToHost, c->stream));
         CK(cudaStreamSynchronize(c->stream));
@@ -536,6 +544,7 @@ static int upload_common(verb_ctx* c, int fid, const void* src, cudaMemcpyKind k
         CK(alloc((void**)&c->fbase[fid], bytes));
         CK(cudaMemcpyAsync(c->fbase[fid], src, bytes, kind, c->stream));
         launch_scale_copy(c->f[fid], c->fbase[fid], c->scale[fid], npts(c), c->stream);
+        c->acc.kernel_launches++;
     } else {
         CK(cudaMemcpyAsync(c->f[fid], src, bytes, kind, c->stream));
         if (c->fbase[fid]) {
@@ -569,10 +578,12 @@ int verb_set_field_scale(verb_ctx* c, int fid, double scale)
             CK(cudaMalloc(&c->fbase[fid], bytes));
             CK(cudaMemcpyAsync(c->fbase[fid], c->f[fid], bytes, cudaMemcpyDeviceToDevice, c->stream));
         }
-        if (scale != 1.0)
+        if (scale != 1.0) {
             launch_scale_copy(c->f[fid], c->fbase[fid], scale, npts(c), c->stream);
-        else
+            c->acc.kernel_launches++;
+        } else {
             CK(cudaMemcpyAsync(c->f[fid], c->fbase[fid], bytes, cudaMemcpyDeviceToDevice, c->stream));
+        }
         mark_dirty(c, fid);
     }
     c->scale[fid] = scale;
@@ -665,6 +676,7 @@ int verb_clamp_positive(verb_ctx* c)
 {
     if (!c || !c->f[VERB_F_PSD]) return VERB_ERR_ARG;
     launch_clamp_positive(c->f[VERB_F_PSD], npts(c), c->stream);
+    c->acc.kernel_launches++;
     return check_launch();
 }
 
@@ -674,6 +686,7 @@ int verb_negative_count(verb_ctx* c, long long* count)
     {
         PhaseTimer t(c, PH_RED);
         launch_negative_count(c->f[VERB_F_PSD], npts(c), c->red, c->stream);
+        c->acc.kernel_launches++;
     }
     if (count) {
         unsigned long long k = 0;
@@ -1016,6 +1029,7 @@ int verb_assimilate_radial(verb_ctx* c, const double* obs_host, double dt, doubl
     a.ticket = c->kfticket;
     PhaseTimer t(c, PH_KF);
     launch_kf(a, nctas, c->stream);
+    c->acc.kernel_launches++;
     return check_launch();
 }
 

@@ -43,7 +43,7 @@ class Timing(C.Structure):
                                             "local_ms", "local_factor_ms", "local_solve_ms",
                                             "reduce_ms", "kf_ms")] + \
                [(n, C.c_longlong) for n in ("steps", "local_solve_launches",
-                                              "local_factor_launches")]
+                                              "local_factor_launches", "kernel_launches")]
 
 
 _dp = C.POINTER(C.c_double)
