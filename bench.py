@@ -115,7 +115,9 @@ def run_ours(args):
                                 timeout=__import__("datetime").timedelta(seconds=600))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    stream = torch.cuda.current_stream(dev)
+    # a dedicated (non-default) stream: the library launches every kernel on it and
+    # the CUDA events below are recorded on it
+    stream = torch.cuda.Stream(dev)
     spec = W.CONFIGS[args.config]
     hours = int(np.ceil((args.warmup + args.steps + 1) * W.DT_5MIN * 24)) + 1
     kp = W.kp_series(args.seed + rank, max(hours, 24))
@@ -127,9 +129,7 @@ def run_ours(args):
     # ---------------- device-resident run (value)
     vel_dev = {h: (torch.from_numpy(vp).to(dev), torch.from_numpy(vr).to(dev))
                for h, (vp, vr) in vel_host.items()}
-
-    def dev_provider(h):
-        return vel_dev[h]
+    torch.cuda.synchronize(dev)
 
     solver = Solver(wl, stream=stream.cuda_stream, velocity_provider=None)
     ctx = solver.ctx
