@@ -55,7 +55,8 @@ typedef enum {
     VERB_ERR_CUDA = 7,    /* CUDA runtime error */
     VERB_ERR_NOMEM = 8,   /* device allocation failed / would not fit */
     VERB_ERR_GRID = 9,    /* convection line shorter than 11 points (QUICKEST6.cpp:56-59) */
-    VERB_TIMEOUT = 10     /* a bounded device wait gave up */
+    VERB_TIMEOUT = 10,    /* a bounded device wait gave up */
+    VERB_ERR_SIZE = 11    /* larger than the fixed scratch of verb_convection_2d_noalloc */
 } verb_status;
 
 enum { VERB_BC_PERIODIC = 0, VERB_BC_CONSTANT_VALUE = 1, VERB_BC_CONSTANT_DERIVATIVE = 2 };
@@ -182,6 +183,26 @@ int verb_convection_2d(double* psd, const double* P, const double* R, int nP, in
                        const double* pl, const double* pu, const double* rl, const double* ru,
                        int pl_t, int pu_t, int rl_t, int ru_t, const double* VP, const double* VR,
                        const double* S, const double* loss, const double* G, double dt);
+
+/* ---- no-allocation entry point ---------------------------------------------- */
+/* No counterpart in the reference.  Convection_2D on one [P][R] slice whose
+ * arrays (same meaning and layout as verb_convection_2d) already live in the
+ * caller's DEVICE memory, for callers that cannot allocate device memory (a
+ * host application or plugin that owns every allocation, or a path where an
+ * allocation is not allowed).  It calls no allocator: the kernel's scratch is
+ * a fixed array of VERB_NOALLOC_MAX_POINTS doubles (plus a few status words)
+ * that the library reserves on every device that loads it, until exit.
+ * nP*nR > VERB_NOALLOC_MAX_POINTS returns VERB_ERR_SIZE.  All calls share that
+ * array, so calls that overlap on the GPU race: serialise them.  The first
+ * call on a device looks up the array's address; make it before any stream
+ * capture.  `stream` is a cudaStream_t (NULL = default stream); the call
+ * returns after the slice is done, with the device-side status. */
+#define VERB_NOALLOC_MAX_POINTS 8192
+int verb_convection_2d_noalloc(double* psd, const double* P, const double* R, int nP, int nR,
+                               const double* pl, const double* pu, const double* rl,
+                               const double* ru, int pl_t, int pu_t, int rl_t, int ru_t,
+                               const double* VP, const double* VR, const double* S,
+                               const double* loss, const double* G, double dt, void* stream);
 
 /* ---- library information --------------------------------------------------- */
 const char* verb_version(void);

@@ -458,6 +458,7 @@ const char* verb_status_string(int s)
         case VERB_ERR_NOMEM: return "out of device memory";
         case VERB_ERR_GRID: return "convection grid shorter than 11 points";
         case VERB_TIMEOUT: return "device wait timed out";
+        case VERB_ERR_SIZE: return "slice larger than the no-allocation scratch";
         default: return "unknown status";
     }
 }

@@ -16,7 +16,7 @@ VERB_OK = 0
 STATUS_NAMES = {
     0: "VERB_OK", 1: "VERB_ERR_PIVOT", 2: "VERB_ERR_ARG", 3: "VERB_ERR_CFL", 4: "VERB_ERR_BC",
     5: "VERB_ERR_TENSOR", 6: "VERB_ERR_NAN", 7: "VERB_ERR_CUDA", 8: "VERB_ERR_NOMEM",
-    9: "VERB_ERR_GRID", 10: "VERB_TIMEOUT",
+    9: "VERB_ERR_GRID", 10: "VERB_TIMEOUT", 11: "VERB_ERR_SIZE",
 }
 
 # 4-D fields (verb_field)
@@ -93,6 +93,9 @@ SIGNATURES = {
     "verb_convection_2d": (C.c_int, [_dp, _dp, _dp, C.c_int, C.c_int, _dp, _dp, _dp, _dp, C.c_int,
                                      C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp,
                                      C.c_double]),
+    "verb_convection_2d_noalloc": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp,
+                                             C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp,
+                                             _vp, _vp, C.c_double, _vp]),
     "verb_version": (C.c_char_p, []),
     "verb_status_string": (C.c_char_p, [C.c_int]),
 }
