@@ -60,6 +60,55 @@ __device__ __forceinline__ double quickest_face(double U1, double U2, double U3,
     return f;
 }
 
+// Courant-number factors of the face polynomial (QUICKEST6.cpp:209-238); they
+// depend only on the face Courant number, which is constant over a slice's
+// sub-steps, so they are computed once per slice with the same expressions.
+struct FaceCoef {
+    double k3, c6, k5, k7, k9;
+};
+
+__device__ __forceinline__ FaceCoef face_coef(double cr)
+{
+    const double cs = cr * cr;
+    const double ca = fabs(cr);
+    FaceCoef k;
+    k.k3 = (cs - 1) / 6.0;
+    k.c6 = ca / 6;
+    k.k5 = (cs - 1) * (cs - 4) / 120.0;
+    k.k7 = (cs - 1) * (cs - 4) * (cs - 9) / 5040.0;
+    k.k9 = (cs - 1) * (cs - 4) * (cs - 9) * (cs - 16) / 362880.0;
+    return k;
+}
+
+// quickest_face with the Courant factors supplied: the same operations in the
+// same order, the factor sub-expressions taken from the table.
+__device__ __forceinline__ double quickest_face_k(double U1, double U2, double U3, double U4,
+                                                  double C, double D1, double D2v, double D3v,
+                                                  double D4v, double D5v, double cr,
+                                                  const FaceCoef& k)
+{
+    const double ca = fabs(cr);
+    double f = 0.5 * (C + D1);
+    const double d1 = C - D1;
+    f += 0.5 * ca * d1;
+    const double D2 = (U1 - C - D1 + D2v) / 2;
+    const double d3 = U1 - 3 * C + 3 * D1 - D2v;
+    f += k.k3 * (D2 + ca / 4 * d3);
+    const double D4 = (U2 - 3 * U1 + 2 * C + 2 * D1 - 3 * D2v + D3v) / 2;
+    const double d5 = U2 - 5 * U1 + 10 * C - 10 * D1 + 5 * D2v - D3v;
+    f += k.k5 * (D4 + k.c6 * d5);
+    const double D6 = (U3 - 5 * U2 + 9 * U1 - 5 * C - 5 * D1 + 9 * D2v - 5 * D3v + D4v) / 2;
+    const double d7 = U3 - 7 * U2 + 21 * U1 - 35 * C + 35 * D1 - 21 * D2v + 7 * D3v - D4v;
+    f += k.k7 * (D6 + ca / 8 * d7);
+    const double D8 = (U4 - 7 * U3 + 20 * U2 - 28 * U1 + 14 * C + 14 * D1 - 28 * D2v + 20 * D3v -
+                       7 * D4v + D5v) /
+                      2;
+    const double d9 = U4 - 9 * U3 + 36 * U2 - 84 * U1 + 126 * C - 126 * D1 + 84 * D2v - 36 * D3v +
+                      9 * D4v - D5v;
+    f += k.k9 * (D8 + d9 / 2);
+    return f;
+}
+
 // Limiter of src/Convection_1D_ULTIMATE_QUICKEST6.cpp:394-447 applied to the
 // unlimited face value f.
 __device__ __forceinline__ double quickest_limit(double f, double cr, double ou, double oc,
@@ -298,35 +347,313 @@ __device__ __forceinline__ double block_max(double v, double* red)
     return m;
 }
 
+// ---------------------------------------------------------------------------
+// Slice kernel: warp-per-line 1-D passes.
+//
+// A warp owns whole lines (two P-lines or one R-line at a time).  It copies a
+// line into a per-warp buffer E with its GST ghost cells materialised (so the
+// 10-point stencils are branch-free shared-memory loads), runs the four phases
+// of one ULTIMATE-QUICKEST sub-step with warp-level synchronisation only,
+// and writes the result back into the slice plane S.  Block barriers remain
+// only between the P-sweep and the R-sweep.  Face Courant numbers are
+// precomputed once per slice (they are constant over its sub-steps) with the
+// reference's expression (Ux[i-1]/dx*dt + Ux[i]/dx*dt)/2.  The R-sweep folds
+// PSD*G into its load and /G, *exp(Loss dt), +S dt into its store, in the
+// reference's order (src/Convection_2D.cpp:122-165).
+
+constexpr int NW = CONV_THREADS / 32;
+
+struct WLine {
+    int base, stride;    // element ix of the line is S[base + ix*stride]
+    const double* cf;    // face Courant numbers of the line, [n]
+    const double* co;    // face coefficient table of the line (5 planes, stride nf) or nullptr
+    double lbc, ubc, dxl, dxu;
+    int ns;              // the line's own CFL sub-steps (QUICKEST6.cpp:37-52)
+    int row;             // R-sweep: the MLT row iP
+};
+
+// per-line buffer: E [n+10] (orig values + ghosts), UE [n+10] (unlimited +
+// ghosts), F [n] (face values)
+__device__ __forceinline__ int line_buf(int n) { return 3 * n + 20; }
+
+// Ghost cells t[k], k in [-GST,-1] and [n, n+GST-1], of an extended line whose
+// interior sits at X[5..n+4] (QUICKEST6.cpp:92-143, 281-330).  Lane l < 5
+// fills low ghost l+1, lanes 5..9 fill high ghost l-4.
+__device__ __forceinline__ void fill_ghosts(double* X, const double* lowsrc, int n, int lt, int ut,
+                                            const WLine& L, int lane)
+{
+    if (lane < 5) {
+        const int ig = lane + 1;
+        double g;
+        if (lt == VERB_BC_PERIODIC) {
+            g = lowsrc[5 + (n - 1) - ig];
+        } else if (lt == VERB_BC_CONSTANT_VALUE) {
+            g = L.lbc;
+        } else {
+            g = lowsrc[5] - L.lbc * L.dxl;
+            for (int i = 2; i <= ig; i++) g = g - L.lbc * L.dxl;
+        }
+        X[5 - ig] = g;
+    } else if (lane < 10) {
+        const int ig = lane - 4;
+        double g;
+        if (ut == VERB_BC_PERIODIC) {
+            g = X[5 + ig];
+        } else if (ut == VERB_BC_CONSTANT_VALUE) {
+            g = L.ubc;
+        } else {
+            g = X[5 + n - 1] + L.ubc * L.dxu;
+            for (int i = 2; i <= ig; i++) g = g + L.ubc * L.dxu;
+        }
+        X[5 + (n - 1) + ig] = g;
+    }
+}
+
+__device__ __forceinline__ double wcell_raw(const double* E, const double* F, const double* cf,
+                                            int lt, int c)
+{
+    const double cr = cf[c + 1];
+    const double fr = F[c + 1];
+    double cl = 0.0, fl = 0.0;
+    if (c > 0 || lt == VERB_BC_PERIODIC) {
+        cl = cf[c];
+        fl = F[c];
+    }
+    return E[5 + c] - (cr * fr - cl * fl);
+}
+
+__device__ __forceinline__ double wcell_final(const double* E, const double* F, const WLine& L, int n,
+                                              int lt, int ut, int c)
+{
+    if (c == n - 1) {
+        if (ut == VERB_BC_CONSTANT_VALUE) return L.ubc;
+        if (ut == VERB_BC_CONSTANT_DERIVATIVE) return wcell_raw(E, F, L.cf, lt, n - 2);
+        return wcell_raw(E, F, L.cf, lt, 0);
+    }
+    if (c == 0) {
+        if (lt == VERB_BC_CONSTANT_VALUE) return L.lbc;
+        if (lt == VERB_BC_CONSTANT_DERIVATIVE) return wcell_raw(E, F, L.cf, lt, 1);
+    }
+    return wcell_raw(E, F, L.cf, lt, c);
+}
+
+struct SliceIO {
+    const double* G;     // global G_conv
+    const double* src;   // global Sources
+    const double* lexp;  // per-CTA exp(Loss dt) plane [P][R]
+    const double* gpl;   // per-CTA G plane [P][R] (PRE only)
+    const double* spl;   // per-CTA Sources*dt plane [P][R] (PRE only)
+    size_t VK, off;
+    int R;
+    double dtc;
+};
+
+// Face value of face ix of an extended line E (QUICKEST6.cpp:162-241).  The
+// upwind side comes from the sign of the Courant number: centre c and
+// direction s give U_k = E[c - s k], D_k = E[c + s k] (:169-186).
+template <bool PRE>
+__device__ __forceinline__ double face_at(const double* E, const double* cf, const double* co,
+                                          int nf, int ix)
+{
+    const double cr = cf[ix];
+    const int up = cr >= 0 ? 1 : 0;
+    const int c = 5 + ix - up;
+    const int s = up ? 1 : -1;
+    const double U1 = E[c - s], U2 = E[c - 2 * s], U3 = E[c - 3 * s], U4 = E[c - 4 * s];
+    const double C = E[c];
+    const double D1 = E[c + s], D2 = E[c + 2 * s], D3 = E[c + 3 * s], D4 = E[c + 4 * s],
+                 D5 = E[c + 5 * s];
+    if (PRE) {
+        FaceCoef fk;
+        fk.k3 = co[ix];
+        fk.c6 = co[nf + ix];
+        fk.k5 = co[2 * nf + ix];
+        fk.k7 = co[3 * nf + ix];
+        fk.k9 = co[4 * nf + ix];
+        return quickest_face_k(U1, U2, U3, U4, C, D1, D2, D3, D4, D5, cr, fk);
+    }
+    return quickest_face(U1, U2, U3, U4, C, D1, D2, D3, D4, D5, cr);
+}
+
+// Limited face value (QUICKEST6.cpp:357-447) from the original line E, the
+// unlimited line UE and the unlimited face value f.
+__device__ __forceinline__ double limit_at(const double* E, const double* UE, const double* cf,
+                                           double f, int ix)
+{
+    const double cr = cf[ix];
+    const int up = cr >= 0 ? 1 : 0;
+    const int c = 5 + ix - up;
+    const int s = up ? 1 : -1;
+    return quickest_limit(f, cr, E[c - s], E[c], E[c + s], UE[c - s], UE[c - 2 * s], UE[c - 3 * s],
+                          UE[c], UE[c + s], UE[c + 2 * s], UE[c + 3 * s]);
+}
+
+// One group of nl (1 or 2) lines of length n through all of their CFL
+// sub-steps.  RS: R-line (load *G, store /G *lexp +src dt).
+template <bool RS, bool PRE>
+__device__ void warp_lines(double* S, double* buf, const WLine L0, const WLine L1, int nl, int n,
+                           int lt, int ut, int lane, const SliceIO& io, int nf)
+{
+    // the two line descriptors stay in registers: fields are selected, never indexed
+#define LQ(q) ((q) ? L1 : L0)
+    const int lb = line_buf(n);
+    const int ix0 = (lt == VERB_BC_PERIODIC) ? 0 : 1;
+    auto gidx = [&](int row, int c) { return ((size_t)row * io.R + c) * io.VK + io.off; };
+    for (int q = 0; q < nl; q++) {
+        double* E = buf + q * lb;
+        for (int k = lane; k < n; k += 32) {
+            const double v = S[LQ(q).base + k * LQ(q).stride];
+            if (RS) E[5 + k] = v * (PRE ? io.gpl[LQ(q).row * io.R + k] : io.G[gidx(LQ(q).row, k)]);
+            else E[5 + k] = v;
+        }
+    }
+    __syncwarp();
+    for (int q = 0; q < nl; q++) fill_ghosts(buf + q * lb, buf + q * lb, n, lt, ut, LQ(q), lane);
+    __syncwarp();
+    int nsmax = L0.ns;
+    if (nl > 1 && L1.ns > nsmax) nsmax = L1.ns;
+    const int tot = nl * n;
+    for (int sub = 0; sub < nsmax; sub++) {
+        // A: unlimited faces (QUICKEST6.cpp:148-256), two faces per lane and
+        // iteration so that their FP64 chains interleave
+        for (int f0 = lane; f0 < tot; f0 += 64) {
+            const int f1 = f0 + 32;
+            int qa = f0 >= n ? 1 : 0, ia = f0 - qa * n;
+            int qb = f1 >= n ? 1 : 0, ib = f1 - qb * n;
+            const bool va = ia >= ix0 && sub < LQ(qa).ns;
+            const bool vb = f1 < tot && ib >= ix0 && sub < LQ(qb).ns;
+            if (!va && !vb) continue;
+            if (!vb) { qb = qa; ib = ia; }
+            if (!va) { qa = qb; ia = ib; }
+            const double fa = face_at<PRE>(buf + qa * lb, LQ(qa).cf, LQ(qa).co, nf, ia);
+            const double fbv = face_at<PRE>(buf + qb * lb, LQ(qb).cf, LQ(qb).co, nf, ib);
+            if (va) buf[qa * lb + 2 * (n + 10) + ia] = fa;
+            if (vb) buf[qb * lb + 2 * (n + 10) + ib] = fbv;
+        }
+        __syncwarp();
+        // B: unlimited cells + boundary rewrite (:243-272) into UE
+        for (int f = lane; f < tot; f += 32) {
+            const int q = f >= n ? 1 : 0;
+            const int c = f - q * n;
+            if (sub >= LQ(q).ns) continue;
+            const double* E = buf + q * lb;
+            double* UE = buf + q * lb + (n + 10);
+            const double* F = buf + q * lb + 2 * (n + 10);
+            UE[5 + c] = wcell_final(E, F, LQ(q), n, lt, ut, c);
+        }
+        __syncwarp();
+        // UE ghosts: low ones from the pre-step PSD (= E's), high ones from UE
+        for (int q = 0; q < nl; q++) {
+            if (sub >= LQ(q).ns) continue;
+            double* E = buf + q * lb;
+            double* UE = E + (n + 10);
+            if (lane < 5) UE[lane] = E[lane];
+            fill_ghosts(UE, E, n, lt, ut, LQ(q), lane < 5 ? 32 : lane);
+        }
+        __syncwarp();
+        // C: limited faces, in place (:332-455), two per lane and iteration
+        for (int f0 = lane; f0 < tot; f0 += 64) {
+            const int f1 = f0 + 32;
+            int qa = f0 >= n ? 1 : 0, ia = f0 - qa * n;
+            int qb = f1 >= n ? 1 : 0, ib = f1 - qb * n;
+            const bool va = ia >= ix0 && sub < LQ(qa).ns;
+            const bool vb = f1 < tot && ib >= ix0 && sub < LQ(qb).ns;
+            if (!va && !vb) continue;
+            if (!vb) { qb = qa; ib = ia; }
+            if (!va) { qa = qb; ia = ib; }
+            const double* Ea = buf + qa * lb;
+            const double* Eb = buf + qb * lb;
+            double* Fa = buf + qa * lb + 2 * (n + 10);
+            double* Fb = buf + qb * lb + 2 * (n + 10);
+            const double la = limit_at(Ea, Ea + (n + 10), LQ(qa).cf, Fa[ia], ia);
+            const double lbv = limit_at(Eb, Eb + (n + 10), LQ(qb).cf, Fb[ib], ib);
+            if (va) Fa[ia] = la;
+            if (vb) Fb[ib] = lbv;
+        }
+        __syncwarp();
+        // D: final cells + rewrite (:448-477)
+        for (int f = lane; f < tot; f += 32) {
+            const int q = f >= n ? 1 : 0;
+            const int c = f - q * n;
+            if (sub >= LQ(q).ns) continue;
+            const double* E = buf + q * lb;
+            double* UE = buf + q * lb + (n + 10);
+            const double* F = buf + q * lb + 2 * (n + 10);
+            const double v = wcell_final(E, F, LQ(q), n, lt, ut, c);
+            if (sub == LQ(q).ns - 1) {
+                if (RS && PRE) {
+                    const int pi = LQ(q).row * io.R + c;
+                    double x = v / io.gpl[pi];
+                    x = x * io.lexp[pi];
+                    if (c >= 1 && c < io.R - 1) x = x + io.spl[pi];
+                    S[LQ(q).base + c * LQ(q).stride] = x;
+                } else if (RS) {
+                    const size_t gi = gidx(LQ(q).row, c);
+                    double x = v / io.G[gi];
+                    x = x * io.lexp[LQ(q).row * io.R + c];
+                    if (c >= 1 && c < io.R - 1) x = x + io.src[gi] * io.dtc;
+                    S[LQ(q).base + c * LQ(q).stride] = x;
+                } else {
+                    S[LQ(q).base + c * LQ(q).stride] = v;
+                }
+            } else {
+                UE[5 + c] = v;
+            }
+        }
+        __syncwarp();
+        if (sub + 1 < nsmax) {
+            // lines that continue: the new values become E (ghosts rebuilt from them)
+            for (int q = 0; q < nl; q++) {
+                if (sub + 1 >= LQ(q).ns) continue;
+                double* E = buf + q * lb;
+                const double* UE = E + (n + 10);
+                for (int k = lane; k < n; k += 32) E[5 + k] = UE[5 + k];
+            }
+            __syncwarp();
+            for (int q = 0; q < nl; q++)
+                if (sub + 1 < LQ(q).ns) fill_ghosts(buf + q * lb, buf + q * lb, n, lt, ut, LQ(q), lane);
+            __syncwarp();
+        }
+    }
+#undef LQ
+}
+
+template <bool PRE>
 __global__ void __launch_bounds__(CONV_THREADS) convection_kernel(ConvArgs a)
 {
     extern __shared__ double sm[];
     const Dims d = a.d;
     const int P = d.P, R = d.R, V = d.V, K = d.K;
     const int PR = P * R;
-    double* S = sm;
-    double* U = sm + PR;
-    double* F = sm + 2 * PR;
-    double* CP = sm + 3 * PR;
-    double* CR = sm + 4 * PR;
-    int* nsP = (int*)(sm + 5 * PR);       // inner steps of P-lines [R]
-    int* nsR = nsP + R;                   // inner steps of R-lines [P]
-    // per-line boundary values and spacings: P-lines [R], R-lines [P]
-    double* lbP = (double*)(((uintptr_t)(nsR + P) + 15) & ~(uintptr_t)15);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double* S = sm;                                   // [P][R]
+    double* CFP = S + PR;                             // P-line face Courants [R-1][P]
+    double* CFR = CFP + (size_t)(R > 1 ? R - 1 : 1) * P;  // R-line face Courants [P][R]
+    double* lbP = CFR + PR;                           // per P-line [R]: lbc, ubc, dxl, dxu
     double* ubP = lbP + R;
     double* dxP = ubP + R;
     double* dxPu = dxP + R;
-    double* lbR = dxPu + R;
+    double* lbR = dxPu + R;                           // per R-line [P]
     double* ubR = lbR + P;
     double* dxR = ubR + P;
     double* dxRu = dxR + P;
-    double* red = dxRu + P;               // [32]
+    double* red = dxRu + P;                           // [32]
+    int* nsP = (int*)(red + 32);                      // [R]
+    int* nsR = nsP + R;                               // [P]
+    const int wbuf = 2 * line_buf(P) > line_buf(R) ? 2 * line_buf(P) : line_buf(R);
+    double* wb = (double*)(((uintptr_t)(nsR + P) + 15) & ~(uintptr_t)15) + (size_t)warp * wbuf;
     __shared__ int s_ticket;
-    __shared__ int s_maxP, s_maxR;
 
     const size_t VK = (size_t)V * K;
     double* lexp = a.scratch + (size_t)blockIdx.x * PR;
+    // face coefficient table: P-line faces [R-1][P] then R-line faces [P][R], 5 planes
+    const int nfP = (R > 1 ? R - 1 : 1) * P;
+    const int nf = nfP + PR;
+    double* coef = PRE ? a.coef + (size_t)blockIdx.x * (5 * (size_t)nf + 2 * (size_t)PR) : nullptr;
+    double* gpl = PRE ? coef + 5 * (size_t)nf : nullptr;     // G of the slice
+    double* spl = PRE ? gpl + PR : nullptr;                  // Sources*dt of the slice
     const int nslices = V * K;
+    const int nw = blockDim.x >> 5;
 
     for (;;) {
         if (threadIdx.x == 0) s_ticket = atomicAdd(a.ticket, 1);
@@ -339,7 +666,7 @@ __global__ void __launch_bounds__(CONV_THREADS) convection_kernel(ConvArgs a)
         const size_t off = (size_t)iV * K + iK;
         auto g = [&](int iP, int iR) { return ((size_t)iP * R + iR) * VK + off; };
 
-        // slice load and slice-level maxima (src/Convection_2D.cpp:57-86)
+        // slice load and slice-level sub-step count (src/Convection_2D.cpp:57-86)
         double vpm = 0.0, vrm = 0.0;
         for (int i = threadIdx.x; i < PR; i += blockDim.x) {
             const int iP = i / R, iR = i - iP * R;
@@ -372,19 +699,18 @@ __global__ void __launch_bounds__(CONV_THREADS) convection_kernel(ConvArgs a)
             continue;
         }
         const double dtc = a.dt / num_steps;
-        if (threadIdx.x == 0) {
-            a.substeps[off] = (int)num_steps;
-            s_maxP = 1;
-            s_maxR = 1;
-        }
+        if (threadIdx.x == 0) a.substeps[off] = (int)num_steps;
         for (int i = threadIdx.x; i < PR; i += blockDim.x) {
             const int iP = i / R, iR = i - iP * R;
             lexp[i] = exp(a.loss[g(iP, iR)] * dtc);
+            if (PRE) {
+                gpl[i] = a.G[g(iP, iR)];
+                spl[i] = a.S[g(iP, iR)] * dtc;
+            }
         }
-        __syncthreads();
 
-        // per-line CFL sub-cycle and Courant numbers (QUICKEST6.cpp:37-52), one warp per line
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+        // per-line CFL sub-cycles and face Courant numbers (QUICKEST6.cpp:37-52,
+        // 150-160), one warp per line
         if (P >= 3) {
             for (int iR = warp; iR < R - 1; iR += nw) {
                 double m = -INFINITY;
@@ -403,7 +729,22 @@ __global__ void __launch_bounds__(CONV_THREADS) convection_kernel(ConvArgs a)
                 else if (sd > 1) ns = (int)ceil(sd);
                 const double dtl = dtc / ns;
                 if (fabs(m / dx * dtl) > 1) set_error(a.status, VERB_ERR_CFL);
-                for (int iP = lane; iP < P; iP += 32) CP[iP * R + iR] = a.VP[g(iP, iR)] / dx * dtl;
+                for (int ix = lane; ix < P; ix += 32) {
+                    const int i0 = ix == 0 ? P - 2 : ix - 1;
+                    const double c0 = a.VP[g(i0, iR)] / dx * dtl;
+                    const double c1 = a.VP[g(ix, iR)] / dx * dtl;
+                    const double cr = (c0 + c1) / 2;
+                    CFP[iR * P + ix] = cr;
+                    if (PRE) {
+                        const FaceCoef fk = face_coef(cr);
+                        double* co = coef + iR * P + ix;
+                        co[0] = fk.k3;
+                        co[nf] = fk.c6;
+                        co[2 * nf] = fk.k5;
+                        co[3 * nf] = fk.k7;
+                        co[4 * nf] = fk.k9;
+                    }
+                }
                 if (lane == 0) {
                     nsP[iR] = ns;
                     dxP[iR] = dx;
@@ -411,7 +752,6 @@ __global__ void __launch_bounds__(CONV_THREADS) convection_kernel(ConvArgs a)
                     const size_t bo = ((size_t)iR * V + iV) * K + iK;
                     lbP[iR] = a.Pl[bo];
                     ubP[iR] = a.Pu[bo];
-                    if (ns > 1) atomicMax(&s_maxP, ns);
                 }
             }
         }
@@ -433,7 +773,22 @@ __global__ void __launch_bounds__(CONV_THREADS) convection_kernel(ConvArgs a)
                 else if (sd > 1) ns = (int)ceil(sd);
                 const double dtl = dtc / ns;
                 if (fabs(m / dx * dtl) > 1) set_error(a.status, VERB_ERR_CFL);
-                for (int iR = lane; iR < R; iR += 32) CR[iP * R + iR] = a.VR[g(iP, iR)] / dx * dtl;
+                for (int ix = lane; ix < R; ix += 32) {
+                    const int i0 = ix == 0 ? R - 2 : ix - 1;
+                    const double c0 = a.VR[g(iP, i0)] / dx * dtl;
+                    const double c1 = a.VR[g(iP, ix)] / dx * dtl;
+                    const double cr = (c0 + c1) / 2;
+                    CFR[iP * R + ix] = cr;
+                    if (PRE) {
+                        const FaceCoef fk = face_coef(cr);
+                        double* co = coef + nfP + iP * R + ix;
+                        co[0] = fk.k3;
+                        co[nf] = fk.c6;
+                        co[2 * nf] = fk.k5;
+                        co[3 * nf] = fk.k7;
+                        co[4 * nf] = fk.k9;
+                    }
+                }
                 if (lane == 0) {
                     nsR[iP] = ns;
                     dxR[iP] = dx;
@@ -441,87 +796,76 @@ __global__ void __launch_bounds__(CONV_THREADS) convection_kernel(ConvArgs a)
                     const size_t bo = ((size_t)iP * V + iV) * K + iK;
                     lbR[iP] = a.Rl[bo] * a.G[g(iP, 0)];
                     ubR[iP] = a.Ru[bo] * a.G[g(iP, R - 1)];
-                    if (ns > 1) atomicMax(&s_maxR, ns);
                 }
             }
         }
         __syncthreads();
-        const int maxP = s_maxP, maxR = s_maxR;
 
-        const Sweep wP{P, a.Pl_t, a.Pu_t};
-        const Sweep wR{R, a.Rl_t, a.Ru_t};
+        SliceIO io;
+        io.G = a.G;
+        io.src = a.S;
+        io.lexp = lexp;
+        io.VK = VK;
+        io.off = off;
+        io.R = R;
+        io.dtc = dtc;
+        io.gpl = gpl;
+        io.spl = spl;
+        const int npairs = (R - 1 + 1) / 2;
         for (int it = 0; it < num_steps; it++) {
             if (P >= 3) {
-                // P-lines iR = 0 .. R-2 (the last R row is not swept, :104)
-                for (int sub = 0; sub < maxP; sub++) {
-                    auto line = [&](int l) {
-                        Line L;
-                        L.base = l;
-                        L.stride = R;
-                        L.lbc = lbP[l];
-                        L.ubc = ubP[l];
-                        L.dxl = dxP[l];
-                        L.dxu = dxPu[l];
-                        return L;
-                    };
-                    auto active = [&](int l) { return sub < nsP[l]; };
-                    quickest_pass(S, U, F, CP, R - 1, wP, false, line, active);
-                    double* tmp = S;
-                    S = U;
-                    U = tmp;
-                }
-                // the untouched last R row lives in the old buffer: carry it over
-                if (maxP & 1) {
-                    for (int iP = threadIdx.x; iP < P; iP += blockDim.x)
-                        S[iP * R + (R - 1)] = U[iP * R + (R - 1)];
-                    __syncthreads();
-                }
-            }
-            if (R >= 3) {
-                // PSD * G, then R-lines with BC*G (:122-145)
-                for (int i = threadIdx.x; i < PR; i += blockDim.x) {
-                    const int iP = i / R, iR = i - iP * R;
-                    S[i] = S[i] * a.G[g(iP, iR)];
+                // P-lines iR = 0 .. R-2 in pairs (the last R row is not swept, :104)
+                for (int gp = warp; gp < npairs; gp += nw) {
+                    WLine L[2];
+                    const int nl = (2 * gp + 1 < R - 1) ? 2 : 1;
+                    for (int q = 0; q < nl; q++) {
+                        const int iR = 2 * gp + q;
+                        L[q].base = iR;
+                        L[q].stride = R;
+                        L[q].cf = CFP + iR * P;
+                        L[q].co = PRE ? coef + iR * P : nullptr;
+                        L[q].lbc = lbP[iR];
+                        L[q].ubc = ubP[iR];
+                        L[q].dxl = dxP[iR];
+                        L[q].dxu = dxPu[iR];
+                        L[q].ns = nsP[iR];
+                        L[q].row = 0;
+                    }
+                    warp_lines<false, PRE>(S, wb, L[0], L[1], nl, P, a.Pl_t, a.Pu_t, lane, io, nf);
                 }
                 __syncthreads();
-                for (int sub = 0; sub < maxR; sub++) {
-                    auto line = [&](int l) {
-                        Line L;
-                        L.base = l * R;
-                        L.stride = 1;
-                        L.lbc = lbR[l];
-                        L.ubc = ubR[l];
-                        L.dxl = dxR[l];
-                        L.dxu = dxRu[l];
-                        return L;
-                    };
-                    auto active = [&](int l) { return sub < nsR[l]; };
-                    quickest_pass(S, U, F, CR, P, wR, true, line, active);
-                    double* tmp = S;
-                    S = U;
-                    U = tmp;
+            }
+            if (R >= 3) {
+                for (int iP = warp; iP < P; iP += nw) {
+                    WLine L[2];
+                    L[0].base = iP * R;
+                    L[0].stride = 1;
+                    L[0].cf = CFR + iP * R;
+                    L[0].co = PRE ? coef + nfP + iP * R : nullptr;
+                    L[0].lbc = lbR[iP];
+                    L[0].ubc = ubR[iP];
+                    L[0].dxl = dxR[iP];
+                    L[0].dxu = dxRu[iP];
+                    L[0].ns = nsR[iP];
+                    L[0].row = iP;
+                    warp_lines<true, PRE>(S, wb, L[0], L[0], 1, R, a.Rl_t, a.Ru_t, lane, io, nf);
                 }
+                __syncthreads();
+            } else {
+                // no R-sweep: exp(loss dt) and sources only (:147-165)
+                for (int i = threadIdx.x; i < PR; i += blockDim.x) {
+                    const int iP = i / R, iR = i - iP * R;
+                    double x = S[i] * lexp[i];
+                    if (iR >= 1 && iR < R - 1) x = x + a.S[g(iP, iR)] * dtc;
+                    S[i] = x;
+                }
+                __syncthreads();
             }
-            // /G, exp(loss dt), sources on interior R (:141-165)
-            for (int i = threadIdx.x; i < PR; i += blockDim.x) {
-                const int iP = i / R, iR = i - iP * R;
-                const size_t gi = g(iP, iR);
-                double x = S[i];
-                if (R >= 3) x = x / a.G[gi];
-                x = x * lexp[i];
-                if (iR >= 1 && iR < R - 1) x = x + a.S[gi] * dtc;
-                S[i] = x;
-            }
-            __syncthreads();
         }
         for (int i = threadIdx.x; i < PR; i += blockDim.x) {
             const int iP = i / R, iR = i - iP * R;
             a.psd[g(iP, iR)] = S[i];
         }
-        // the S/U roles may have swapped an odd number of times; the next
-        // slice simply starts from the canonical order again
-        S = sm;
-        U = sm + PR;
         __syncthreads();
     }
 }
@@ -578,8 +922,16 @@ __global__ void __launch_bounds__(CONV_THREADS)
 size_t conv_smem_bytes(int P, int R)
 {
     const size_t PR = (size_t)P * R;
-    return 5 * PR * sizeof(double) + (size_t)(P + R) * sizeof(int) + 16 +
-           (size_t)(4 * R + 4 * P) * sizeof(double) + 32 * sizeof(double);
+    const size_t lbP = 3 * (size_t)P + 20, lbR = 3 * (size_t)R + 20;
+    const size_t wbuf = 2 * lbP > lbR ? 2 * lbP : lbR;
+    return (PR + (size_t)(R > 1 ? R - 1 : 1) * P + PR + 4 * (size_t)R + 4 * (size_t)P + 32) *
+               sizeof(double) +
+           (size_t)(R + P) * sizeof(int) + 16 + (size_t)(CONV_THREADS / 32) * wbuf * sizeof(double);
+}
+
+size_t conv_coef_doubles(int P, int R)
+{
+    return 5 * ((size_t)(R > 1 ? R - 1 : 1) * P + (size_t)P * R) + 2 * (size_t)P * R;
 }
 
 int conv_ctas(int P, int R)
@@ -588,8 +940,9 @@ int conv_ctas(int P, int R)
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const size_t smem = conv_smem_bytes(P, R);
-    cudaFuncSetAttribute(convection_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, convection_kernel, CONV_THREADS, smem);
+    cudaFuncSetAttribute(convection_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, convection_kernel<true>, CONV_THREADS, smem);
     if (per < 1) per = 1;
     return sms * per;
 }
@@ -597,8 +950,15 @@ int conv_ctas(int P, int R)
 void launch_convection(const ConvArgs& a, int nctas, cudaStream_t s)
 {
     const size_t smem = conv_smem_bytes(a.d.P, a.d.R);
-    cudaFuncSetAttribute(convection_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    convection_kernel<<<nctas, CONV_THREADS, smem, s>>>(a);
+    if (a.coef) {
+        cudaFuncSetAttribute(convection_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        convection_kernel<true><<<nctas, CONV_THREADS, smem, s>>>(a);
+    } else {
+        cudaFuncSetAttribute(convection_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        convection_kernel<false><<<nctas, CONV_THREADS, smem, s>>>(a);
+    }
 }
 
 void launch_convection_line(double* psd, const double* x, int n, double lbc, double ubc, int lbc_t,

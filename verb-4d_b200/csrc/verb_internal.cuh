@@ -51,12 +51,14 @@ struct ConvArgs {
     int Pl_t, Pu_t, Rl_t, Ru_t;
     double dt;
     double* scratch;     // per-CTA P*R doubles (exp(loss*dt))
+    double* coef;        // per-CTA face coefficient table (conv_coef_doubles), or nullptr
     int* substeps;       // [V][K] out
     int* ticket;         // work counter (zeroed before launch)
     int* status;
 };
 int conv_ctas(int P, int R);
 size_t conv_smem_bytes(int P, int R);
+size_t conv_coef_doubles(int P, int R);
 void launch_convection(const ConvArgs& a, int nctas, cudaStream_t s);
 void launch_convection_line(double* psd, const double* x, int n, double lbc, double ubc, int lbc_t,
                             int ubc_t, const double* ux, double dt, int* status, cudaStream_t s);

@@ -71,6 +71,9 @@ CONFIGS = {
     "cfg1": GridSpec(24, 25, 31, 31),
     # 48 MLT x 101 L x 101 E x 91 alpha, hourly Kp in [1, 6], 288 steps of 5 min
     "cfg2": GridSpec(48, 101, 101, 91),
+    # profiling case: the production (MLT, L) slice shape over a coarse (E, alpha)
+    # grid that still spans 0.01-10 MeV (small enough for full ncu captures)
+    "cfg2s": GridSpec(48, 101, 12, 12),
 }
 
 
