@@ -348,312 +348,395 @@ __device__ __forceinline__ double block_max(double v, double* red)
 }
 
 // ---------------------------------------------------------------------------
-// Slice kernel: warp-per-line 1-D passes.
+// Slice kernel.
 //
-// A warp owns whole lines (two P-lines or one R-line at a time).  It copies a
-// line into a per-warp buffer E with its GST ghost cells materialised (so the
-// 10-point stencils are branch-free shared-memory loads), runs the four phases
-// of one ULTIMATE-QUICKEST sub-step with warp-level synchronisation only,
-// and writes the result back into the slice plane S.  Block barriers remain
-// only between the P-sweep and the R-sweep.  Face Courant numbers are
-// precomputed once per slice (they are constant over its sub-steps) with the
-// reference's expression (Ux[i-1]/dx*dt + Ux[i]/dx*dt)/2.  The R-sweep folds
-// PSD*G into its load and /G, *exp(Loss dt), +S dt into its store, in the
-// reference's order (src/Convection_2D.cpp:122-165).
+// A CTA of C3_WARPS warps owns one [P][R] slice at a time; the slice stays in
+// shared memory (plane S) for all of its CFL sub-steps.  A sweep is a set of
+// independent lines (P-lines: fixed L, R-lines: fixed MLT).  A warp takes
+// 32/lpl lines per job with lpl lanes per line, and lane j of a line owns the
+// cells x = j + lpl*t, t < T = ceil(n/lpl): at every step of a phase the lanes
+// of a line touch consecutive shared-memory words.  A job copies its lines
+// into per-warp buffers extended by the GST = 5 ghost cells of
+// QUICKEST6.cpp:89-143, stages the lines' face Courant numbers next to them,
+// and runs the four phases of one ULTIMATE-QUICKEST sub-step with warp
+// synchronisation only:
+//   A  unlimited face values into F                    (QUICKEST6.cpp:148-241)
+//   B  unlimited cells + boundary rewrite into UE      (:243-272)
+//   C  limited face values into F                      (:277-447)
+//   D  final cells + rewrite; into S on the last sub-step (:448-477)
+// The Courant factors of the face polynomial are recomputed from the face
+// Courant number with exactly rounded divisions by the constant denominators
+// (div_const).  All faces of a job usually have
+// the same upwind direction (the drift velocities are smooth along MLT and the
+// radial velocity depends on MLT only), so a job is dispatched to a
+// direction-specialised body in which the upwind stencil roles are fixed
+// registers; jobs with mixed directions select the roles per face.
+//
+// The radial sweep works on PSD*G: a pass over the plane multiplies by G
+// before it, and the epilogue pass /G, *exp(Loss dt), +S dt (interior L)
+// follows it, in the reference's order (src/Convection_2D.cpp:122-165).  The
+// per-slice planes G, exp(Loss dt), S dt and the face Courant tables live in a
+// per-CTA scratch region that stays resident in L2.
 
-constexpr int NW = CONV_THREADS / 32;
+constexpr int C3_WARPS = 8;
+constexpr int C3_THREADS = C3_WARPS * 32;
+constexpr int TMAX = 8;  // cells per lane: lines of up to 32*TMAX points
 
-struct WLine {
-    int base, stride;    // element ix of the line is S[base + ix*stride]
-    const double* cf;    // face Courant numbers of the line, [n]
-    const double* co;    // face coefficient table of the line (5 planes, stride nf) or nullptr
+// a / b rounded to nearest, for the constants b = 6, 120, 5040 and 362880 with
+// y = RN(1/b) (Markstein's correction step: P. Markstein, IBM J. Res. Dev.
+// 34(1), 1990).  q = RN(a*y) is within 1.5 ulp of a/b, so the residual a - b*q
+// is a representable number (at most 6B units of 2^(e_b+e_q-1), B <= 2835 the
+// odd part of b) and the fused multiply-add returns it exactly.  q + r*y then
+// differs from a/b by |r|*|y - 1/b| < 1.5*2^-53 ulp, whereas a/b lies at
+// least ulp/(2B) away from every rounding midpoint (b's odd part B >= 3 makes
+// a midpoint times b need more than 53 significant bits), so a single
+// rounding of q + r*y gives RN(a/b).  A zero residual returns q, which keeps
+// the sign that division gives to a zero quotient.
+__device__ __forceinline__ double div_const(double a, double b, double y)
+{
+    const double q = __dmul_rn(a, y);
+    const double r = __fma_rn(-q, b, a);
+    return r == 0.0 ? q : __fma_rn(r, y, q);
+}
+
+// Courant factors of the face polynomial (QUICKEST6.cpp:209-238), the same
+// expressions as face_coef().
+__device__ __forceinline__ FaceCoef face_coef_exact(double cr)
+{
+    const double cs = cr * cr;
+    const double ca = fabs(cr);
+    const double t1 = cs - 1;
+    const double p2 = t1 * (cs - 4);
+    const double p3 = p2 * (cs - 9);
+    const double p4 = p3 * (cs - 16);
+    FaceCoef k;
+    k.k3 = div_const(t1, 6.0, 1.0 / 6.0);
+    k.c6 = div_const(ca, 6.0, 1.0 / 6.0);
+    k.k5 = div_const(p2, 120.0, 1.0 / 120.0);
+    k.k7 = div_const(p3, 5040.0, 1.0 / 5040.0);
+    k.k9 = div_const(p4, 362880.0, 1.0 / 362880.0);
+    return k;
+}
+
+enum { DIR_POS = 0, DIR_NEG = 1, DIR_MIX = 2 };
+
+// Face value of face x from w[k] = E[x-5+k].  Courant >= 0: upwind centre
+// x-1, U_k = E[x-1-k], D_k = E[x-1+k]; Courant < 0: centre x, U_k = E[x+k],
+// D_k = E[x-k] (QUICKEST6.cpp:169-186).
+template <int DIR>
+__device__ __forceinline__ double face3(const double (&w)[10], double cr)
+{
+    const FaceCoef k = face_coef_exact(cr);
+    if (DIR == DIR_POS)
+        return quickest_face_k(w[3], w[2], w[1], w[0], w[4], w[5], w[6], w[7], w[8], w[9], cr, k);
+    if (DIR == DIR_NEG)
+        return quickest_face_k(w[6], w[7], w[8], w[9], w[5], w[4], w[3], w[2], w[1], w[0], cr, k);
+    const bool up = cr >= 0;
+    return quickest_face_k(up ? w[3] : w[6], up ? w[2] : w[7], up ? w[1] : w[8], up ? w[0] : w[9],
+                           up ? w[4] : w[5], up ? w[5] : w[4], up ? w[6] : w[3], up ? w[7] : w[2],
+                           up ? w[8] : w[1], up ? w[9] : w[0], cr, k);
+}
+
+// Limited face value of face x from u[k] = UE[x-4+k] and ev[k] = E[x-2+k].
+template <int DIR>
+__device__ __forceinline__ double limit3(double f, double cr, const double (&u)[8],
+                                         const double (&ev)[4])
+{
+    if (DIR == DIR_POS)
+        return quickest_limit(f, cr, ev[0], ev[1], ev[2], u[2], u[1], u[0], u[3], u[4], u[5], u[6]);
+    if (DIR == DIR_NEG)
+        return quickest_limit(f, cr, ev[3], ev[2], ev[1], u[5], u[6], u[7], u[4], u[3], u[2], u[1]);
+    const bool up = cr >= 0;
+    return quickest_limit(f, cr, up ? ev[0] : ev[3], up ? ev[1] : ev[2], up ? ev[2] : ev[1],
+                          up ? u[2] : u[5], up ? u[1] : u[6], up ? u[0] : u[7], up ? u[3] : u[4],
+                          up ? u[4] : u[3], up ? u[5] : u[2], up ? u[6] : u[1]);
+}
+
+// Work split of one sweep: nlines lines of n points, lpl lanes per line.
+struct SweepCfg {
+    int lpl, T, nlw, njobs, nb;  // nb: doubles per line buffer (E, UE, F and CR each)
+};
+
+__host__ __device__ inline SweepCfg sweep_cfg(int n, int nlines)
+{
+    SweepCfg best{0, 0, 0, 0, 0};
+    double be = -1.0;
+    for (int lpl = 32; lpl >= 8; lpl >>= 1) {
+        const int T = (n + lpl - 1) / lpl;
+        if (T > TMAX) continue;
+        const int nlw = 32 / lpl;
+        const int jobs = (nlines + nlw - 1) / nlw;
+        const int rounds = (jobs + C3_WARPS - 1) / C3_WARPS;
+        const double eff = (double)nlines * n / ((double)(rounds > 0 ? rounds : 1) * C3_WARPS * 32 * T);
+        if (eff > be + 1e-12) {
+            be = eff;
+            best = SweepCfg{lpl, T, nlw, jobs, lpl * T + 10};
+        }
+    }
+    return best;  // lpl == 0: lines longer than 32*TMAX points
+}
+
+// per-warp buffer size in doubles (both sweeps share it)
+__host__ __device__ inline int conv_wstride(int P, int R)
+{
+    int w = 0;
+    if (P >= 3) {
+        const SweepCfg c = sweep_cfg(P, R - 1);
+        w = c.nlw * 4 * c.nb;
+    }
+    if (R >= 3) {
+        const SweepCfg c = sweep_cfg(R, P);
+        if (c.nlw * 4 * c.nb > w) w = c.nlw * 4 * c.nb;
+    }
+    return (w + 1) & ~1;  // keep every warp's buffer 16-byte aligned
+}
+
+// One job's lines as seen by one lane.
+struct LineJob {
+    double *E, *UE, *F, *CR;  // the lane's line buffers; E/UE slot x+5 holds cell x,
+                              // F and CR slot x hold face x and its Courant number
+    int n, lpl, T, j;         // line length, lanes per line, cells per lane, lane in line
+    int li;                   // line index (P-sweep: iR, R-sweep: iP)
+    int lt, ut;               // boundary types
+    int ns, nsmax;            // the line's sub-steps; the maximum over the warp
+    int R;                    // row length of the plane S
+    bool lv;                  // the lane's line exists
     double lbc, ubc, dxl, dxu;
-    int ns;              // the line's own CFL sub-steps (QUICKEST6.cpp:37-52)
-    int row;             // R-sweep: the MLT row iP
 };
 
-// per-line buffer: E [n+10] (orig values + ghosts), UE [n+10] (unlimited +
-// ghosts), F [n] (face values)
-__device__ __forceinline__ int line_buf(int n) { return 3 * n + 20; }
-
-// Ghost cells t[k], k in [-GST,-1] and [n, n+GST-1], of an extended line whose
-// interior sits at X[5..n+4] (QUICKEST6.cpp:92-143, 281-330).  Lane l < 5
-// fills low ghost l+1, lanes 5..9 fill high ghost l-4.
-__device__ __forceinline__ void fill_ghosts(double* X, const double* lowsrc, int n, int lt, int ut,
-                                            const WLine& L, int lane)
+// Stores cell x of the E buffer together with the ghost cells it determines:
+// periodic mirrors (QUICKEST6.cpp:96-100, 123-127) and the constant-derivative
+// extrapolation from the end cells (:108-115, 134-140).
+__device__ __forceinline__ void store_e(const LineJob& J, int x, double v)
 {
-    if (lane < 5) {
-        const int ig = lane + 1;
-        double g;
-        if (lt == VERB_BC_PERIODIC) {
-            g = lowsrc[5 + (n - 1) - ig];
-        } else if (lt == VERB_BC_CONSTANT_VALUE) {
-            g = L.lbc;
-        } else {
-            g = lowsrc[5] - L.lbc * L.dxl;
-            for (int i = 2; i <= ig; i++) g = g - L.lbc * L.dxl;
+    double* X = J.E;
+    X[x + 5] = v;
+    if (J.lt == VERB_BC_PERIODIC) {
+        if (x >= J.n - 6 && x <= J.n - 2) X[x - (J.n - 1) + 5] = v;
+        if (x >= 1 && x <= 5) X[x + (J.n - 1) + 5] = v;
+    } else if (x == 0 && J.lt == VERB_BC_CONSTANT_DERIVATIVE) {
+        double g = v - J.lbc * J.dxl;
+        X[4] = g;
+        for (int ig = 2; ig <= 5; ig++) {
+            g = g - J.lbc * J.dxl;
+            X[5 - ig] = g;
         }
-        X[5 - ig] = g;
-    } else if (lane < 10) {
-        const int ig = lane - 4;
-        double g;
-        if (ut == VERB_BC_PERIODIC) {
-            g = X[5 + ig];
-        } else if (ut == VERB_BC_CONSTANT_VALUE) {
-            g = L.ubc;
-        } else {
-            g = X[5 + n - 1] + L.ubc * L.dxu;
-            for (int i = 2; i <= ig; i++) g = g + L.ubc * L.dxu;
+    }
+    if (x == J.n - 1 && J.ut == VERB_BC_CONSTANT_DERIVATIVE) {
+        double g = v + J.ubc * J.dxu;
+        X[J.n + 5] = g;
+        for (int ig = 2; ig <= 5; ig++) {
+            g = g + J.ubc * J.dxu;
+            X[J.n + 4 + ig] = g;
         }
-        X[5 + (n - 1) + ig] = g;
     }
 }
 
-__device__ __forceinline__ double wcell_raw(const double* E, const double* F, const double* cf,
-                                            int lt, int c)
+// Stores cell x of the UE buffer: high ghosts from UE (periodic mirror or
+// constant-derivative extrapolation, :307-326); the low ghosts are the
+// pre-step ones of E (:281-304) and are copied separately.
+__device__ __forceinline__ void store_ue(const LineJob& J, int x, double v)
 {
-    const double cr = cf[c + 1];
-    const double fr = F[c + 1];
-    double cl = 0.0, fl = 0.0;
-    if (c > 0 || lt == VERB_BC_PERIODIC) {
-        cl = cf[c];
-        fl = F[c];
+    double* X = J.UE;
+    X[x + 5] = v;
+    if (J.ut == VERB_BC_PERIODIC) {
+        if (x >= 1 && x <= 5) X[x + (J.n - 1) + 5] = v;
+    } else if (x == J.n - 1 && J.ut == VERB_BC_CONSTANT_DERIVATIVE) {
+        double g = v + J.ubc * J.dxu;
+        X[J.n + 5] = g;
+        for (int ig = 2; ig <= 5; ig++) {
+            g = g + J.ubc * J.dxu;
+            X[J.n + 4 + ig] = g;
+        }
     }
-    return E[5 + c] - (cr * fr - cl * fl);
 }
 
-__device__ __forceinline__ double wcell_final(const double* E, const double* F, const WLine& L, int n,
-                                              int lt, int ut, int c)
+// Flux update of cell k, E[k] - (cr[k+1]*F[k+1] - cr[k]*F[k]) (:245-249,
+// 448-452).  A non-periodic line's cell 0 is always rewritten, so its left
+// flux (zero in the reference) is never used.
+__device__ __forceinline__ double cell_raw3(const LineJob& J, int k)
 {
-    if (c == n - 1) {
-        if (ut == VERB_BC_CONSTANT_VALUE) return L.ubc;
-        if (ut == VERB_BC_CONSTANT_DERIVATIVE) return wcell_raw(E, F, L.cf, lt, n - 2);
-        return wcell_raw(E, F, L.cf, lt, 0);
-    }
-    if (c == 0) {
-        if (lt == VERB_BC_CONSTANT_VALUE) return L.lbc;
-        if (lt == VERB_BC_CONSTANT_DERIVATIVE) return wcell_raw(E, F, L.cf, lt, 1);
-    }
-    return wcell_raw(E, F, L.cf, lt, c);
+    return J.E[k + 5] - (J.CR[k + 1] * J.F[k + 1] - J.CR[k] * J.F[k]);
 }
 
-struct SliceIO {
-    const double* G;     // global G_conv
-    const double* src;   // global Sources
-    const double* lexp;  // per-CTA exp(Loss dt) plane [P][R]
-    const double* gpl;   // per-CTA G plane [P][R] (PRE only)
-    const double* spl;   // per-CTA Sources*dt plane [P][R] (PRE only)
-    size_t VK, off;
-    int R;
-    double dtc;
+// Cell x after the boundary rewrite (:257-272 / 457-477).
+__device__ __forceinline__ double cell_final3(const LineJob& J, int x)
+{
+    if (x == J.n - 1) {
+        if (J.ut == VERB_BC_CONSTANT_VALUE) return J.ubc;
+        return cell_raw3(J, J.ut == VERB_BC_CONSTANT_DERIVATIVE ? J.n - 2 : 0);
+    }
+    if (x == 0) {
+        if (J.lt == VERB_BC_CONSTANT_VALUE) return J.lbc;
+        if (J.lt == VERB_BC_CONSTANT_DERIVATIVE) return cell_raw3(J, 1);
+    }
+    return cell_raw3(J, x);
+}
+
+__device__ __forceinline__ void store_plane(double* S, const LineJob& J, bool RS, int x, double v)
+{
+    if (RS) S[J.li * J.R + x] = v;
+    else S[x * J.R + J.li] = v;
+}
+
+// All sub-steps of one job (QUICKEST6.cpp:37-52 sub-cycle, one pass per
+// sub-step).  The loops over a lane's cells stay rolled (one copy of the face
+// code per phase keeps the kernel small enough for the instruction caches);
+// the per-cell state between phases lives in the line buffers.
+template <bool RS, int DIR>
+__device__ __forceinline__ void job_substeps(double* S, const LineJob& J)
+{
+    for (int sub = 0; sub < J.nsmax; sub++) {
+        // A: unlimited faces
+#pragma unroll 1
+        for (int x = J.j; x < J.lpl * J.T; x += J.lpl) {
+            double w[10];
+#pragma unroll
+            for (int k = 0; k < 10; k++) w[k] = J.E[x + k];
+            J.F[x] = face3<DIR>(w, J.CR[x]);
+        }
+        __syncwarp();
+        // B: unlimited cells into UE
+#pragma unroll 1
+        for (int x = J.j; x < J.lpl * J.T; x += J.lpl)
+            if (J.lv && x < J.n) store_ue(J, x, cell_final3(J, x));
+        if (J.lv && J.j < 5) J.UE[J.j] = J.E[J.j];
+        __syncwarp();
+        // C: limited faces, in place (each lane reads only its own faces)
+#pragma unroll 1
+        for (int x = J.j; x < J.lpl * J.T; x += J.lpl) {
+            double u[8], ev[4];
+#pragma unroll
+            for (int k = 0; k < 8; k++) u[k] = J.UE[x + 1 + k];
+#pragma unroll
+            for (int k = 0; k < 4; k++) ev[k] = J.E[x + 3 + k];
+            J.F[x] = limit3<DIR>(J.F[x], J.CR[x], u, ev);
+        }
+        __syncwarp();
+        // D: final cells; lines that go on stage the new values in UE (free
+        // after phase C) and copy them into E once every lane is done with E
+        const bool last = sub == J.ns - 1;
+#pragma unroll 1
+        for (int x = J.j; x < J.lpl * J.T; x += J.lpl) {
+            if (J.lv && x < J.n) {
+                const double v = cell_final3(J, x);
+                if (last) store_plane(S, J, RS, x, v);
+                else J.UE[x + 5] = v;
+            }
+        }
+        if (sub + 1 < J.nsmax) {
+            __syncwarp();
+#pragma unroll 1
+            for (int x = J.j; x < J.lpl * J.T; x += J.lpl)
+                if (J.lv && x < J.n) store_e(J, x, J.UE[x + 5]);
+            __syncwarp();
+        }
+    }
+}
+
+struct LineArrays {
+    const double *lb, *ub, *dxl, *dxu;
+    const int* ns;
 };
 
-// Face value of face ix of an extended line E (QUICKEST6.cpp:162-241).  The
-// upwind side comes from the sign of the Courant number: centre c and
-// direction s give U_k = E[c - s k], D_k = E[c + s k] (:169-186).
-template <bool PRE>
-__device__ __forceinline__ double face_at(const double* E, const double* cf, const double* co,
-                                          int nf, int ix)
+// One job of a sweep: load the lines into the warp's buffers, pick the
+// direction-specialised body, run the line sub-steps.
+template <bool RS>
+__device__ __forceinline__ void sweep_job(double* S, double* wb, const SweepCfg& c, int job, int n,
+                                          int nlines, int R, int lt, int ut, const double* crtab,
+                                          const LineArrays& la)
 {
-    const double cr = cf[ix];
-    const int up = cr >= 0 ? 1 : 0;
-    const int c = 5 + ix - up;
-    const int s = up ? 1 : -1;
-    const double U1 = E[c - s], U2 = E[c - 2 * s], U3 = E[c - 3 * s], U4 = E[c - 4 * s];
-    const double C = E[c];
-    const double D1 = E[c + s], D2 = E[c + 2 * s], D3 = E[c + 3 * s], D4 = E[c + 4 * s],
-                 D5 = E[c + 5 * s];
-    if (PRE) {
-        FaceCoef fk;
-        fk.k3 = co[ix];
-        fk.c6 = co[nf + ix];
-        fk.k5 = co[2 * nf + ix];
-        fk.k7 = co[3 * nf + ix];
-        fk.k9 = co[4 * nf + ix];
-        return quickest_face_k(U1, U2, U3, U4, C, D1, D2, D3, D4, D5, cr, fk);
-    }
-    return quickest_face(U1, U2, U3, U4, C, D1, D2, D3, D4, D5, cr);
-}
-
-// Limited face value (QUICKEST6.cpp:357-447) from the original line E, the
-// unlimited line UE and the unlimited face value f.
-__device__ __forceinline__ double limit_at(const double* E, const double* UE, const double* cf,
-                                           double f, int ix)
-{
-    const double cr = cf[ix];
-    const int up = cr >= 0 ? 1 : 0;
-    const int c = 5 + ix - up;
-    const int s = up ? 1 : -1;
-    return quickest_limit(f, cr, E[c - s], E[c], E[c + s], UE[c - s], UE[c - 2 * s], UE[c - 3 * s],
-                          UE[c], UE[c + s], UE[c + 2 * s], UE[c + 3 * s]);
-}
-
-// One group of nl (1 or 2) lines of length n through all of their CFL
-// sub-steps.  RS: R-line (load *G, store /G *lexp +src dt).
-template <bool RS, bool PRE>
-__device__ void warp_lines(double* S, double* buf, const WLine L0, const WLine L1, int nl, int n,
-                           int lt, int ut, int lane, const SliceIO& io, int nf)
-{
-    // the two line descriptors stay in registers: fields are selected, never indexed
-#define LQ(q) ((q) ? L1 : L0)
-    const int lb = line_buf(n);
+    const int lane = threadIdx.x & 31;
+    const int q = lane / c.lpl;
+    LineJob J;
+    J.n = n;
+    J.lpl = c.lpl;
+    J.T = c.T;
+    J.j = lane - q * c.lpl;
+    J.li = job * c.nlw + q;
+    J.lv = J.li < nlines;
+    J.lt = lt;
+    J.ut = ut;
+    J.R = R;
+    J.E = wb + (size_t)q * 4 * c.nb;
+    J.UE = J.E + c.nb;
+    J.F = J.UE + c.nb;
+    J.CR = J.F + c.nb;
+    J.lbc = J.lv ? la.lb[J.li] : 0.0;
+    J.ubc = J.lv ? la.ub[J.li] : 0.0;
+    J.dxl = J.lv ? la.dxl[J.li] : 0.0;
+    J.dxu = J.lv ? la.dxu[J.li] : 0.0;
+    J.ns = J.lv ? la.ns[J.li] : 0;
+    J.nsmax = __reduce_max_sync(0xffffffffu, J.ns);
     const int ix0 = (lt == VERB_BC_PERIODIC) ? 0 : 1;
-    auto gidx = [&](int row, int c) { return ((size_t)row * io.R + c) * io.VK + io.off; };
-    for (int q = 0; q < nl; q++) {
-        double* E = buf + q * lb;
-        for (int k = lane; k < n; k += 32) {
-            const double v = S[LQ(q).base + k * LQ(q).stride];
-            if (RS) E[5 + k] = v * (PRE ? io.gpl[LQ(q).row * io.R + k] : io.G[gidx(LQ(q).row, k)]);
-            else E[5 + k] = v;
-        }
-    }
-    __syncwarp();
-    for (int q = 0; q < nl; q++) fill_ghosts(buf + q * lb, buf + q * lb, n, lt, ut, LQ(q), lane);
-    __syncwarp();
-    int nsmax = L0.ns;
-    if (nl > 1 && L1.ns > nsmax) nsmax = L1.ns;
-    const int tot = nl * n;
-    for (int sub = 0; sub < nsmax; sub++) {
-        // A: unlimited faces (QUICKEST6.cpp:148-256), two faces per lane and
-        // iteration so that their FP64 chains interleave
-        for (int f0 = lane; f0 < tot; f0 += 64) {
-            const int f1 = f0 + 32;
-            int qa = f0 >= n ? 1 : 0, ia = f0 - qa * n;
-            int qb = f1 >= n ? 1 : 0, ib = f1 - qb * n;
-            const bool va = ia >= ix0 && sub < LQ(qa).ns;
-            const bool vb = f1 < tot && ib >= ix0 && sub < LQ(qb).ns;
-            if (!va && !vb) continue;
-            if (!vb) { qb = qa; ib = ia; }
-            if (!va) { qa = qb; ia = ib; }
-            const double fa = face_at<PRE>(buf + qa * lb, LQ(qa).cf, LQ(qa).co, nf, ia);
-            const double fbv = face_at<PRE>(buf + qb * lb, LQ(qb).cf, LQ(qb).co, nf, ib);
-            if (va) buf[qa * lb + 2 * (n + 10) + ia] = fa;
-            if (vb) buf[qb * lb + 2 * (n + 10) + ib] = fbv;
-        }
-        __syncwarp();
-        // B: unlimited cells + boundary rewrite (:243-272) into UE
-        for (int f = lane; f < tot; f += 32) {
-            const int q = f >= n ? 1 : 0;
-            const int c = f - q * n;
-            if (sub >= LQ(q).ns) continue;
-            const double* E = buf + q * lb;
-            double* UE = buf + q * lb + (n + 10);
-            const double* F = buf + q * lb + 2 * (n + 10);
-            UE[5 + c] = wcell_final(E, F, LQ(q), n, lt, ut, c);
-        }
-        __syncwarp();
-        // UE ghosts: low ones from the pre-step PSD (= E's), high ones from UE
-        for (int q = 0; q < nl; q++) {
-            if (sub >= LQ(q).ns) continue;
-            double* E = buf + q * lb;
-            double* UE = E + (n + 10);
-            if (lane < 5) UE[lane] = E[lane];
-            fill_ghosts(UE, E, n, lt, ut, LQ(q), lane < 5 ? 32 : lane);
-        }
-        __syncwarp();
-        // C: limited faces, in place (:332-455), two per lane and iteration
-        for (int f0 = lane; f0 < tot; f0 += 64) {
-            const int f1 = f0 + 32;
-            int qa = f0 >= n ? 1 : 0, ia = f0 - qa * n;
-            int qb = f1 >= n ? 1 : 0, ib = f1 - qb * n;
-            const bool va = ia >= ix0 && sub < LQ(qa).ns;
-            const bool vb = f1 < tot && ib >= ix0 && sub < LQ(qb).ns;
-            if (!va && !vb) continue;
-            if (!vb) { qb = qa; ib = ia; }
-            if (!va) { qa = qb; ia = ib; }
-            const double* Ea = buf + qa * lb;
-            const double* Eb = buf + qb * lb;
-            double* Fa = buf + qa * lb + 2 * (n + 10);
-            double* Fb = buf + qb * lb + 2 * (n + 10);
-            const double la = limit_at(Ea, Ea + (n + 10), LQ(qa).cf, Fa[ia], ia);
-            const double lbv = limit_at(Eb, Eb + (n + 10), LQ(qb).cf, Fb[ib], ib);
-            if (va) Fa[ia] = la;
-            if (vb) Fb[ib] = lbv;
-        }
-        __syncwarp();
-        // D: final cells + rewrite (:448-477)
-        for (int f = lane; f < tot; f += 32) {
-            const int q = f >= n ? 1 : 0;
-            const int c = f - q * n;
-            if (sub >= LQ(q).ns) continue;
-            const double* E = buf + q * lb;
-            double* UE = buf + q * lb + (n + 10);
-            const double* F = buf + q * lb + 2 * (n + 10);
-            const double v = wcell_final(E, F, LQ(q), n, lt, ut, c);
-            if (sub == LQ(q).ns - 1) {
-                if (RS && PRE) {
-                    const int pi = LQ(q).row * io.R + c;
-                    double x = v / io.gpl[pi];
-                    x = x * io.lexp[pi];
-                    if (c >= 1 && c < io.R - 1) x = x + io.spl[pi];
-                    S[LQ(q).base + c * LQ(q).stride] = x;
-                } else if (RS) {
-                    const size_t gi = gidx(LQ(q).row, c);
-                    double x = v / io.G[gi];
-                    x = x * io.lexp[LQ(q).row * io.R + c];
-                    if (c >= 1 && c < io.R - 1) x = x + io.src[gi] * io.dtc;
-                    S[LQ(q).base + c * LQ(q).stride] = x;
-                } else {
-                    S[LQ(q).base + c * LQ(q).stride] = v;
-                }
-            } else {
-                UE[5 + c] = v;
+    bool pos = true, neg = true;
+    for (int x = J.j; x <= J.lpl * J.T; x += J.lpl) {
+        double cr = 0.0;
+        if (J.lv && x < n) {
+            cr = crtab[(size_t)J.li * n + x];
+            store_e(J, x, RS ? S[J.li * R + x] : S[x * R + J.li]);
+            if (x >= ix0) {
+                pos = pos && cr >= 0;
+                neg = neg && cr < 0;
             }
         }
-        __syncwarp();
-        if (sub + 1 < nsmax) {
-            // lines that continue: the new values become E (ghosts rebuilt from them)
-            for (int q = 0; q < nl; q++) {
-                if (sub + 1 >= LQ(q).ns) continue;
-                double* E = buf + q * lb;
-                const double* UE = E + (n + 10);
-                for (int k = lane; k < n; k += 32) E[5 + k] = UE[5 + k];
-            }
-            __syncwarp();
-            for (int q = 0; q < nl; q++)
-                if (sub + 1 < LQ(q).ns) fill_ghosts(buf + q * lb, buf + q * lb, n, lt, ut, LQ(q), lane);
-            __syncwarp();
-        }
+        J.CR[x] = cr;
     }
-#undef LQ
+    if (J.lv && J.j == 0 && lt == VERB_BC_CONSTANT_VALUE)
+        for (int k = 0; k < 5; k++) J.E[k] = J.lbc;
+    if (J.lv && J.j == (n - 1) % J.lpl && ut == VERB_BC_CONSTANT_VALUE)
+        for (int k = 0; k < 5; k++) J.E[n + 5 + k] = J.UE[n + 5 + k] = J.ubc;
+    pos = __all_sync(0xffffffffu, pos);
+    neg = __all_sync(0xffffffffu, neg);
+    __syncwarp();
+    if (pos) job_substeps<RS, DIR_POS>(S, J);
+    else if (neg) job_substeps<RS, DIR_NEG>(S, J);
+    else job_substeps<RS, DIR_MIX>(S, J);
 }
 
-template <bool PRE>
-__global__ void __launch_bounds__(CONV_THREADS) convection_kernel(ConvArgs a)
+__host__ __device__ inline size_t conv_scratch_per_cta(int P, int R)
+{
+    return (size_t)(R > 1 ? R - 1 : 1) * P + 4 * (size_t)P * R;
+}
+
+__global__ void __launch_bounds__(C3_THREADS, 2) convection_kernel(ConvArgs a)
 {
     extern __shared__ double sm[];
     const Dims d = a.d;
     const int P = d.P, R = d.R, V = d.V, K = d.K;
     const int PR = P * R;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double* S = sm;                                   // [P][R]
-    double* CFP = S + PR;                             // P-line face Courants [R-1][P]
-    double* CFR = CFP + (size_t)(R > 1 ? R - 1 : 1) * P;  // R-line face Courants [P][R]
-    double* lbP = CFR + PR;                           // per P-line [R]: lbc, ubc, dxl, dxu
+    double* S = sm;                // [P][R]
+    double* lbP = S + PR;          // per P-line (index iR): lbc, ubc, dxl, dxu
     double* ubP = lbP + R;
     double* dxP = ubP + R;
     double* dxPu = dxP + R;
-    double* lbR = dxPu + R;                           // per R-line [P]
+    double* lbR = dxPu + R;        // per R-line (index iP)
     double* ubR = lbR + P;
     double* dxR = ubR + P;
     double* dxRu = dxR + P;
-    double* red = dxRu + P;                           // [32]
-    int* nsP = (int*)(red + 32);                      // [R]
-    int* nsR = nsP + R;                               // [P]
-    const int wbuf = 2 * line_buf(P) > line_buf(R) ? 2 * line_buf(P) : line_buf(R);
-    double* wb = (double*)(((uintptr_t)(nsR + P) + 15) & ~(uintptr_t)15) + (size_t)warp * wbuf;
+    double* red = dxRu + P;        // [32]
+    int* nsP = (int*)(red + 32);   // [R]
+    int* nsR = nsP + R;            // [P]
+    const int wstride = conv_wstride(P, R);
+    double* wall = (double*)(((uintptr_t)(nsR + P) + 15) & ~(uintptr_t)15);
+    double* wb = wall + (size_t)warp * wstride;
     __shared__ int s_ticket;
 
+    // line buffers start as zeros: ghost slots that a sweep never writes are
+    // read only by padding lanes, whose results are discarded
+    for (int i = threadIdx.x; i < C3_WARPS * wstride; i += blockDim.x) wall[i] = 0.0;
+
+    const SweepCfg cP = sweep_cfg(P, R - 1), cR = sweep_cfg(R, P);
     const size_t VK = (size_t)V * K;
-    double* lexp = a.scratch + (size_t)blockIdx.x * PR;
-    // face coefficient table: P-line faces [R-1][P] then R-line faces [P][R], 5 planes
-    const int nfP = (R > 1 ? R - 1 : 1) * P;
-    const int nf = nfP + PR;
-    double* coef = PRE ? a.coef + (size_t)blockIdx.x * (5 * (size_t)nf + 2 * (size_t)PR) : nullptr;
-    double* gpl = PRE ? coef + 5 * (size_t)nf : nullptr;     // G of the slice
-    double* spl = PRE ? gpl + PR : nullptr;                  // Sources*dt of the slice
+    double* crP = a.scratch + (size_t)blockIdx.x * conv_scratch_per_cta(P, R);  // [R-1][P]
+    double* crR = crP + (size_t)(R > 1 ? R - 1 : 1) * P;                       // [P][R]
+    double* gpl = crR + PR;    // G of the slice
+    double* lexp = gpl + PR;   // exp(Loss dt)
+    double* spl = lexp + PR;   // Sources dt
     const int nslices = V * K;
-    const int nw = blockDim.x >> 5;
+    const LineArrays laP{lbP, ubP, dxP, dxPu, nsP};
+    const LineArrays laR{lbR, ubR, dxR, dxRu, nsR};
 
     for (;;) {
         if (threadIdx.x == 0) s_ticket = atomicAdd(a.ticket, 1);
@@ -702,17 +785,16 @@ __global__ void __launch_bounds__(CONV_THREADS) convection_kernel(ConvArgs a)
         if (threadIdx.x == 0) a.substeps[off] = (int)num_steps;
         for (int i = threadIdx.x; i < PR; i += blockDim.x) {
             const int iP = i / R, iR = i - iP * R;
-            lexp[i] = exp(a.loss[g(iP, iR)] * dtc);
-            if (PRE) {
-                gpl[i] = a.G[g(iP, iR)];
-                spl[i] = a.S[g(iP, iR)] * dtc;
-            }
+            const size_t gi = g(iP, iR);
+            lexp[i] = exp(a.loss[gi] * dtc);
+            gpl[i] = a.G[gi];
+            spl[i] = a.S[gi] * dtc;
         }
 
         // per-line CFL sub-cycles and face Courant numbers (QUICKEST6.cpp:37-52,
         // 150-160), one warp per line
         if (P >= 3) {
-            for (int iR = warp; iR < R - 1; iR += nw) {
+            for (int iR = warp; iR < R - 1; iR += C3_WARPS) {
                 double m = -INFINITY;
                 for (int iP = lane; iP < P; iP += 32) {
                     const double v = fabs(a.VP[g(iP, iR)]);
@@ -733,17 +815,7 @@ __global__ void __launch_bounds__(CONV_THREADS) convection_kernel(ConvArgs a)
                     const int i0 = ix == 0 ? P - 2 : ix - 1;
                     const double c0 = a.VP[g(i0, iR)] / dx * dtl;
                     const double c1 = a.VP[g(ix, iR)] / dx * dtl;
-                    const double cr = (c0 + c1) / 2;
-                    CFP[iR * P + ix] = cr;
-                    if (PRE) {
-                        const FaceCoef fk = face_coef(cr);
-                        double* co = coef + iR * P + ix;
-                        co[0] = fk.k3;
-                        co[nf] = fk.c6;
-                        co[2 * nf] = fk.k5;
-                        co[3 * nf] = fk.k7;
-                        co[4 * nf] = fk.k9;
-                    }
+                    crP[(size_t)iR * P + ix] = (c0 + c1) / 2;
                 }
                 if (lane == 0) {
                     nsP[iR] = ns;
@@ -756,7 +828,7 @@ __global__ void __launch_bounds__(CONV_THREADS) convection_kernel(ConvArgs a)
             }
         }
         if (R >= 3) {
-            for (int iP = warp; iP < P; iP += nw) {
+            for (int iP = warp; iP < P; iP += C3_WARPS) {
                 double m = -INFINITY;
                 for (int iR = lane; iR < R; iR += 32) {
                     const double v = fabs(a.VR[g(iP, iR)]);
@@ -777,17 +849,7 @@ __global__ void __launch_bounds__(CONV_THREADS) convection_kernel(ConvArgs a)
                     const int i0 = ix == 0 ? R - 2 : ix - 1;
                     const double c0 = a.VR[g(iP, i0)] / dx * dtl;
                     const double c1 = a.VR[g(iP, ix)] / dx * dtl;
-                    const double cr = (c0 + c1) / 2;
-                    CFR[iP * R + ix] = cr;
-                    if (PRE) {
-                        const FaceCoef fk = face_coef(cr);
-                        double* co = coef + nfP + iP * R + ix;
-                        co[0] = fk.k3;
-                        co[nf] = fk.c6;
-                        co[2 * nf] = fk.k5;
-                        co[3 * nf] = fk.k7;
-                        co[4 * nf] = fk.k9;
-                    }
+                    crR[(size_t)iP * R + ix] = (c0 + c1) / 2;
                 }
                 if (lane == 0) {
                     nsR[iP] = ns;
@@ -801,62 +863,33 @@ __global__ void __launch_bounds__(CONV_THREADS) convection_kernel(ConvArgs a)
         }
         __syncthreads();
 
-        SliceIO io;
-        io.G = a.G;
-        io.src = a.S;
-        io.lexp = lexp;
-        io.VK = VK;
-        io.off = off;
-        io.R = R;
-        io.dtc = dtc;
-        io.gpl = gpl;
-        io.spl = spl;
-        const int npairs = (R - 1 + 1) / 2;
         for (int it = 0; it < num_steps; it++) {
             if (P >= 3) {
-                // P-lines iR = 0 .. R-2 in pairs (the last R row is not swept, :104)
-                for (int gp = warp; gp < npairs; gp += nw) {
-                    WLine L[2];
-                    const int nl = (2 * gp + 1 < R - 1) ? 2 : 1;
-                    for (int q = 0; q < nl; q++) {
-                        const int iR = 2 * gp + q;
-                        L[q].base = iR;
-                        L[q].stride = R;
-                        L[q].cf = CFP + iR * P;
-                        L[q].co = PRE ? coef + iR * P : nullptr;
-                        L[q].lbc = lbP[iR];
-                        L[q].ubc = ubP[iR];
-                        L[q].dxl = dxP[iR];
-                        L[q].dxu = dxPu[iR];
-                        L[q].ns = nsP[iR];
-                        L[q].row = 0;
-                    }
-                    warp_lines<false, PRE>(S, wb, L[0], L[1], nl, P, a.Pl_t, a.Pu_t, lane, io, nf);
-                }
+                // P-lines iR = 0 .. R-2 (the last R row is not swept, :104)
+                for (int job = warp; job < cP.njobs; job += C3_WARPS)
+                    sweep_job<false>(S, wb, cP, job, P, R - 1, R, a.Pl_t, a.Pu_t, crP, laP);
                 __syncthreads();
             }
             if (R >= 3) {
-                for (int iP = warp; iP < P; iP += nw) {
-                    WLine L[2];
-                    L[0].base = iP * R;
-                    L[0].stride = 1;
-                    L[0].cf = CFR + iP * R;
-                    L[0].co = PRE ? coef + nfP + iP * R : nullptr;
-                    L[0].lbc = lbR[iP];
-                    L[0].ubc = ubR[iP];
-                    L[0].dxl = dxR[iP];
-                    L[0].dxu = dxRu[iP];
-                    L[0].ns = nsR[iP];
-                    L[0].row = iP;
-                    warp_lines<true, PRE>(S, wb, L[0], L[0], 1, R, a.Rl_t, a.Ru_t, lane, io, nf);
+                for (int i = threadIdx.x; i < PR; i += blockDim.x) S[i] = S[i] * gpl[i];
+                __syncthreads();
+                for (int job = warp; job < cR.njobs; job += C3_WARPS)
+                    sweep_job<true>(S, wb, cR, job, R, P, R, a.Rl_t, a.Ru_t, crR, laR);
+                __syncthreads();
+                for (int i = threadIdx.x; i < PR; i += blockDim.x) {
+                    const int iR = i - (i / R) * R;
+                    double x = S[i] / gpl[i];
+                    x = x * lexp[i];
+                    if (iR >= 1 && iR < R - 1) x = x + spl[i];
+                    S[i] = x;
                 }
                 __syncthreads();
             } else {
                 // no R-sweep: exp(loss dt) and sources only (:147-165)
                 for (int i = threadIdx.x; i < PR; i += blockDim.x) {
-                    const int iP = i / R, iR = i - iP * R;
+                    const int iR = i - (i / R) * R;
                     double x = S[i] * lexp[i];
-                    if (iR >= 1 && iR < R - 1) x = x + a.S[g(iP, iR)] * dtc;
+                    if (iR >= 1 && iR < R - 1) x = x + spl[i];
                     S[i] = x;
                 }
                 __syncthreads();
@@ -921,17 +954,21 @@ __global__ void __launch_bounds__(CONV_THREADS)
 
 size_t conv_smem_bytes(int P, int R)
 {
-    const size_t PR = (size_t)P * R;
-    const size_t lbP = 3 * (size_t)P + 20, lbR = 3 * (size_t)R + 20;
-    const size_t wbuf = 2 * lbP > lbR ? 2 * lbP : lbR;
-    return (PR + (size_t)(R > 1 ? R - 1 : 1) * P + PR + 4 * (size_t)R + 4 * (size_t)P + 32) *
-               sizeof(double) +
-           (size_t)(R + P) * sizeof(int) + 16 + (size_t)(CONV_THREADS / 32) * wbuf * sizeof(double);
+    return ((size_t)P * R + 4 * (size_t)R + 4 * (size_t)P + 32) * sizeof(double) +
+           (size_t)(R + P) * sizeof(int) + 16 + (size_t)C3_WARPS * conv_wstride(P, R) * sizeof(double);
 }
 
-size_t conv_coef_doubles(int P, int R)
+size_t conv_scratch_doubles(int P, int R) { return conv_scratch_per_cta(P, R); }
+
+int conv_check(int P, int R)
 {
-    return 5 * ((size_t)(R > 1 ? R - 1 : 1) * P + (size_t)P * R) + 2 * (size_t)P * R;
+    if ((P >= 3 && sweep_cfg(P, R - 1).lpl == 0) || (R >= 3 && sweep_cfg(R, P).lpl == 0))
+        return VERB_ERR_SIZE;
+    int dev = 0, maxsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (conv_smem_bytes(P, R) > (size_t)maxsm) return VERB_ERR_SIZE;
+    return VERB_OK;
 }
 
 int conv_ctas(int P, int R)
@@ -940,9 +977,8 @@ int conv_ctas(int P, int R)
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const size_t smem = conv_smem_bytes(P, R);
-    cudaFuncSetAttribute(convection_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, convection_kernel<true>, CONV_THREADS, smem);
+    cudaFuncSetAttribute(convection_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, convection_kernel, C3_THREADS, smem);
     if (per < 1) per = 1;
     return sms * per;
 }
@@ -950,15 +986,8 @@ int conv_ctas(int P, int R)
 void launch_convection(const ConvArgs& a, int nctas, cudaStream_t s)
 {
     const size_t smem = conv_smem_bytes(a.d.P, a.d.R);
-    if (a.coef) {
-        cudaFuncSetAttribute(convection_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
-        convection_kernel<true><<<nctas, CONV_THREADS, smem, s>>>(a);
-    } else {
-        cudaFuncSetAttribute(convection_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
-        convection_kernel<false><<<nctas, CONV_THREADS, smem, s>>>(a);
-    }
+    cudaFuncSetAttribute(convection_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    convection_kernel<<<nctas, C3_THREADS, smem, s>>>(a);
 }
 
 void launch_convection_line(double* psd, const double* x, int n, double lbc, double ubc, int lbc_t,

@@ -47,7 +47,6 @@ struct verb_ctx {
     const double* dkv_override = nullptr;  // Dyx for the per-slice entry point
     // convection
     double* conv_scratch = nullptr;
-    double* conv_coef = nullptr;
     int* conv_substeps = nullptr;
     int* ticket = nullptr;
     int conv_nctas = 0;
@@ -364,9 +363,10 @@ int conv_run(verb_ctx* c, double dt)
         int s = need_bc(c, b);
         if (s) return s;
     }
+    if (int s = conv_check(d.P, d.R)) return s;
     if (!c->conv_nctas) c->conv_nctas = conv_ctas(d.P, d.R);
-    CK(alloc((void**)&c->conv_scratch, (size_t)c->conv_nctas * d.P * d.R * sizeof(double)));
-    CK(alloc((void**)&c->conv_coef, (size_t)c->conv_nctas * conv_coef_doubles(d.P, d.R) * sizeof(double)));
+    CK(alloc((void**)&c->conv_scratch,
+             (size_t)c->conv_nctas * conv_scratch_doubles(d.P, d.R) * sizeof(double)));
     CK(alloc((void**)&c->conv_substeps, (size_t)d.V * d.K * sizeof(int)));
     CK(alloc((void**)&c->ticket, sizeof(int)));
     ConvArgs a{};
@@ -389,7 +389,6 @@ int conv_run(verb_ctx* c, double dt)
     a.Ru_t = c->bct[VERB_BCF_RU];
     a.dt = dt;
     a.scratch = c->conv_scratch;
-    a.coef = c->conv_coef;
     a.substeps = c->conv_substeps;
     a.ticket = c->ticket;
     a.status = c->status;
@@ -506,7 +505,7 @@ int verb_destroy(verb_ctx* c)
     }
     for (int i = 0; i < VERB_BCF_COUNT; i++) cudaFree(c->bc[i]);
     for (void* p : {(void*)c->rfa, (void*)c->rfbet, (void*)c->rfgam, (void*)c->Lf, (void*)c->Uf,
-                    (void*)c->lwork, (void*)c->ipiv, (void*)c->conv_scratch, (void*)c->conv_coef,
+                    (void*)c->lwork, (void*)c->ipiv, (void*)c->conv_scratch,
                     (void*)c->conv_substeps, (void*)c->ticket, (void*)c->red, (void*)c->status,
                     (void*)c->Pa, (void*)c->kfwork, (void*)c->obs, (void*)c->kfticket})
         cudaFree(p);

@@ -6,13 +6,15 @@
 // allocating would synchronise the device or is forbidden by policy.  They
 // already hold their input and output arrays on the device.  For them this
 // entry point runs the same convection kernel as verb_convection_2d, with the
-// kernel's scratch (the per-slice exp(Loss*dt) plane, the work ticket, the
-// sub-step count and the status word) placed in a fixed array that the
-// library reserves in device memory when it is loaded.
+// kernel's scratch (the slice's face Courant tables and its G, exp(Loss*dt)
+// and Sources*dt planes, the work ticket, the sub-step count and the status
+// word) placed in a fixed array that the library reserves in device memory
+// when it is loaded.
 //
 // Limits and sharing:
 //  * P_size * R_size must not exceed VERB_NOALLOC_MAX_POINTS (8192 points,
-//    64 KiB of scratch); larger slices are rejected with VERB_ERR_SIZE.
+//    5 doubles each: 320 KiB of scratch); larger slices are rejected with
+//    VERB_ERR_SIZE, and so are lines longer than the kernel's 256 points.
 //  * Every GPU that loads the library holds the array until the process exits.
 //  * All calls share the one array and it keeps the last call's contents; the
 //    entry point clears the ticket and status words on each call.  Calls whose
@@ -30,10 +32,11 @@
 namespace {
 
 constexpr int kMaxPoints = VERB_NOALLOC_MAX_POINTS;
+constexpr int kPlaneDoubles = 5 * kMaxPoints;  // >= conv_scratch_doubles(P, R) for P*R <= kMaxPoints
 constexpr int kWords = 8;  // ticket, sub-step count, status (+ padding)
 
-// The scratch: [kMaxPoints] doubles of exp(Loss*dt), then kWords ints.
-static __device__ __align__(256) double g_noalloc_scratch[kMaxPoints + kWords];
+// The scratch: kPlaneDoubles doubles for one CTA, then kWords ints.
+static __device__ __align__(256) double g_noalloc_scratch[kPlaneDoubles + kWords];
 
 constexpr int kMaxDevices = 64;
 double* g_scratch_addr[kMaxDevices] = {};
@@ -70,12 +73,14 @@ extern "C" int verb_convection_2d_noalloc(double* psd, const double* P, const do
         return VERB_ERR_ARG;
     if ((long)nP * nR > kMaxPoints) return VERB_ERR_SIZE;
     if ((nP >= 3 && nP < 11) || (nR >= 3 && nR < 11)) return VERB_ERR_GRID;
+    if (verb::conv_scratch_doubles(nP, nR) > (size_t)kPlaneDoubles) return VERB_ERR_SIZE;
+    if (int s = verb::conv_check(nP, nR)) return s;
     if ((pl_t == VERB_BC_PERIODIC) != (pu_t == VERB_BC_PERIODIC)) return VERB_ERR_BC;
     if ((rl_t == VERB_BC_PERIODIC) != (ru_t == VERB_BC_PERIODIC)) return VERB_ERR_BC;
     double* scratch = nullptr;
     int s = scratch_for_current_device(&scratch);
     if (s) return s;
-    int* words = reinterpret_cast<int*>(scratch + kMaxPoints);
+    int* words = reinterpret_cast<int*>(scratch + kPlaneDoubles);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     // ticket, sub-step count and status start at zero on every call
     if (cudaMemsetAsync(words, 0, kWords * sizeof(double), st) != cudaSuccess) return VERB_ERR_CUDA;
@@ -98,7 +103,7 @@ extern "C" int verb_convection_2d_noalloc(double* psd, const double* P, const do
     a.Rl_t = rl_t;
     a.Ru_t = ru_t;
     a.dt = dt;
-    a.scratch = scratch;      // one CTA: its exp(Loss*dt) plane is the first P*R doubles
+    a.scratch = scratch;      // one CTA: conv_scratch_doubles(P, R) <= kPlaneDoubles
     a.ticket = words;
     a.substeps = words + 1;
     a.status = words + 2;

@@ -50,15 +50,15 @@ struct ConvArgs {
     const double *Pl, *Pu, *Rl, *Ru;
     int Pl_t, Pu_t, Rl_t, Ru_t;
     double dt;
-    double* scratch;     // per-CTA P*R doubles (exp(loss*dt))
-    double* coef;        // per-CTA face coefficient table (conv_coef_doubles), or nullptr
+    double* scratch;     // per-CTA conv_scratch_doubles(P, R): Courant tables and planes
     int* substeps;       // [V][K] out
     int* ticket;         // work counter (zeroed before launch)
     int* status;
 };
 int conv_ctas(int P, int R);
+int conv_check(int P, int R);  // VERB_ERR_SIZE for slices the kernel cannot hold
 size_t conv_smem_bytes(int P, int R);
-size_t conv_coef_doubles(int P, int R);
+size_t conv_scratch_doubles(int P, int R);
 void launch_convection(const ConvArgs& a, int nctas, cudaStream_t s);
 void launch_convection_line(double* psd, const double* x, int n, double lbc, double ubc, int lbc_t,
                             int ubc_t, const double* ux, double dt, int* status, cudaStream_t s);

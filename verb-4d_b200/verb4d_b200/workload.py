@@ -74,6 +74,10 @@ CONFIGS = {
     # profiling case: the production (MLT, L) slice shape over a coarse (E, alpha)
     # grid that still spans 0.01-10 MeV (small enough for full ncu captures)
     "cfg2s": GridSpec(48, 101, 12, 12),
+    # profiling case: the production (MLT, L, E) grid over 8 pitch angles, so
+    # that the convection kernel sees the production energy mix and more slices
+    # than resident CTAs
+    "cfg2m": GridSpec(48, 101, 101, 8),
 }
 
 
