@@ -437,19 +437,54 @@ __device__ __forceinline__ double face3(const double (&w)[10], double cr)
                            up ? w[8] : w[1], up ? w[9] : w[0], cr, k);
 }
 
+// quickest_limit with the branches turned into selects: the same comparisons
+// and the same fmax/fmin sequence pick the same value; only the division for
+// the reference value stays behind a branch.
+__device__ __forceinline__ double quickest_limit_sel(double f, double cr, double ou, double oc,
+                                                     double od, double UU1, double UU2, double UU3,
+                                                     double UC, double UD1, double UD2, double UD3)
+{
+    const double ca = fabs(cr);
+    const double DEL = od - ou;
+    const double CURV = od - 2 * oc + ou;
+    const double ADEL = fabs(DEL);
+    const double ACURV = fabs(CURV);
+    const double dif1 = UD2 - UD3;
+    const double dif2 = UD1 - UD2;
+    const double dif3 = UC - UD1;
+    const double dif4 = UU1 - UC;
+    const double dif5 = UU2 - UU1;
+    const double dif6 = UU3 - UU2;
+    const bool peak_dw = dif1 > 0 && dif2 > 0 && dif3 < 0 && dif4 < 0 && dif2 < dif1 && dif3 > dif4;
+    const bool peak_c = dif2 > 0 && dif3 > 0 && dif4 < 0 && dif5 < 0 && dif3 < dif2 && dif4 > dif5;
+    const bool peak_u = dif3 > 0 && dif4 > 0 && dif5 < 0 && dif6 < 0 && dif4 < dif3 && dif5 > dif6;
+    const bool mono = !(peak_dw || peak_c || peak_u);
+    const bool flat = ACURV >= ADEL;
+    const bool rise = DEL > 0, fall = DEL < 0;
+    const bool useref = mono && !flat && ca > 1e-31 && (rise || fall);
+    double ref = 0.0;
+    if (useref) ref = ou + (oc - ou) / ca;
+    const double fr = fmin(fmax(f, oc), fmin(ref, od));
+    const double ff = fmax(fmin(f, oc), fmax(ref, od));
+    double res = useref ? (rise ? fr : ff) : f;
+    if (mono && flat) res = oc;
+    return res;
+}
+
 // Limited face value of face x from u[k] = UE[x-4+k] and ev[k] = E[x-2+k].
 template <int DIR>
 __device__ __forceinline__ double limit3(double f, double cr, const double (&u)[8],
                                          const double (&ev)[4])
 {
     if (DIR == DIR_POS)
-        return quickest_limit(f, cr, ev[0], ev[1], ev[2], u[2], u[1], u[0], u[3], u[4], u[5], u[6]);
+        return quickest_limit_sel(f, cr, ev[0], ev[1], ev[2], u[2], u[1], u[0], u[3], u[4], u[5], u[6]);
     if (DIR == DIR_NEG)
-        return quickest_limit(f, cr, ev[3], ev[2], ev[1], u[5], u[6], u[7], u[4], u[3], u[2], u[1]);
+        return quickest_limit_sel(f, cr, ev[3], ev[2], ev[1], u[5], u[6], u[7], u[4], u[3], u[2], u[1]);
     const bool up = cr >= 0;
-    return quickest_limit(f, cr, up ? ev[0] : ev[3], up ? ev[1] : ev[2], up ? ev[2] : ev[1],
-                          up ? u[2] : u[5], up ? u[1] : u[6], up ? u[0] : u[7], up ? u[3] : u[4],
-                          up ? u[4] : u[3], up ? u[5] : u[2], up ? u[6] : u[1]);
+    return quickest_limit_sel(f, cr, up ? ev[0] : ev[3], up ? ev[1] : ev[2], up ? ev[2] : ev[1],
+                              up ? u[2] : u[5], up ? u[1] : u[6], up ? u[0] : u[7],
+                              up ? u[3] : u[4], up ? u[4] : u[3], up ? u[5] : u[2],
+                              up ? u[6] : u[1]);
 }
 
 // Work split of one sweep: nlines lines of n points, lpl lanes per line.
@@ -504,53 +539,6 @@ struct LineJob {
     double lbc, ubc, dxl, dxu;
 };
 
-// Stores cell x of the E buffer together with the ghost cells it determines:
-// periodic mirrors (QUICKEST6.cpp:96-100, 123-127) and the constant-derivative
-// extrapolation from the end cells (:108-115, 134-140).
-__device__ __forceinline__ void store_e(const LineJob& J, int x, double v)
-{
-    double* X = J.E;
-    X[x + 5] = v;
-    if (J.lt == VERB_BC_PERIODIC) {
-        if (x >= J.n - 6 && x <= J.n - 2) X[x - (J.n - 1) + 5] = v;
-        if (x >= 1 && x <= 5) X[x + (J.n - 1) + 5] = v;
-    } else if (x == 0 && J.lt == VERB_BC_CONSTANT_DERIVATIVE) {
-        double g = v - J.lbc * J.dxl;
-        X[4] = g;
-        for (int ig = 2; ig <= 5; ig++) {
-            g = g - J.lbc * J.dxl;
-            X[5 - ig] = g;
-        }
-    }
-    if (x == J.n - 1 && J.ut == VERB_BC_CONSTANT_DERIVATIVE) {
-        double g = v + J.ubc * J.dxu;
-        X[J.n + 5] = g;
-        for (int ig = 2; ig <= 5; ig++) {
-            g = g + J.ubc * J.dxu;
-            X[J.n + 4 + ig] = g;
-        }
-    }
-}
-
-// Stores cell x of the UE buffer: high ghosts from UE (periodic mirror or
-// constant-derivative extrapolation, :307-326); the low ghosts are the
-// pre-step ones of E (:281-304) and are copied separately.
-__device__ __forceinline__ void store_ue(const LineJob& J, int x, double v)
-{
-    double* X = J.UE;
-    X[x + 5] = v;
-    if (J.ut == VERB_BC_PERIODIC) {
-        if (x >= 1 && x <= 5) X[x + (J.n - 1) + 5] = v;
-    } else if (x == J.n - 1 && J.ut == VERB_BC_CONSTANT_DERIVATIVE) {
-        double g = v + J.ubc * J.dxu;
-        X[J.n + 5] = g;
-        for (int ig = 2; ig <= 5; ig++) {
-            g = g + J.ubc * J.dxu;
-            X[J.n + 4 + ig] = g;
-        }
-    }
-}
-
 // Flux update of cell k, E[k] - (cr[k+1]*F[k+1] - cr[k]*F[k]) (:245-249,
 // 448-452).  A non-periodic line's cell 0 is always rewritten, so its left
 // flux (zero in the reference) is never used.
@@ -559,18 +547,41 @@ __device__ __forceinline__ double cell_raw3(const LineJob& J, int k)
     return J.E[k + 5] - (J.CR[k + 1] * J.F[k + 1] - J.CR[k] * J.F[k]);
 }
 
-// Cell x after the boundary rewrite (:257-272 / 457-477).
-__device__ __forceinline__ double cell_final3(const LineJob& J, int x)
+// Boundary rewrites of the end cells (:257-272 / 457-477); cells 1..n-2 keep
+// their flux update.
+__device__ __forceinline__ double cell_first3(const LineJob& J)
 {
-    if (x == J.n - 1) {
-        if (J.ut == VERB_BC_CONSTANT_VALUE) return J.ubc;
-        return cell_raw3(J, J.ut == VERB_BC_CONSTANT_DERIVATIVE ? J.n - 2 : 0);
+    if (J.lt == VERB_BC_CONSTANT_VALUE) return J.lbc;
+    return cell_raw3(J, J.lt == VERB_BC_CONSTANT_DERIVATIVE ? 1 : 0);
+}
+
+__device__ __forceinline__ double cell_last3(const LineJob& J)
+{
+    if (J.ut == VERB_BC_CONSTANT_VALUE) return J.ubc;
+    return cell_raw3(J, J.ut == VERB_BC_CONSTANT_DERIVATIVE ? J.n - 2 : 0);
+}
+
+// Constant-derivative ghost cells from an end value (:108-115, 134-140 and
+// :295-300, 319-324): low ghosts X[4..0] from cell 0, high X[n+5..n+9] from
+// cell n-1, each the previous one -/+ bc*dx.
+__device__ __forceinline__ void cd_low(double* X, double v0, double bc, double dx)
+{
+    double g = v0 - bc * dx;
+    X[4] = g;
+    for (int ig = 2; ig <= 5; ig++) {
+        g = g - bc * dx;
+        X[5 - ig] = g;
     }
-    if (x == 0) {
-        if (J.lt == VERB_BC_CONSTANT_VALUE) return J.lbc;
-        if (J.lt == VERB_BC_CONSTANT_DERIVATIVE) return cell_raw3(J, 1);
+}
+
+__device__ __forceinline__ void cd_high(double* X, int n, double vn, double bc, double dx)
+{
+    double g = vn + bc * dx;
+    X[n + 5] = g;
+    for (int ig = 2; ig <= 5; ig++) {
+        g = g + bc * dx;
+        X[n + 4 + ig] = g;
     }
-    return cell_raw3(J, x);
 }
 
 __device__ __forceinline__ void store_plane(double* S, const LineJob& J, bool RS, int x, double v)
@@ -582,29 +593,49 @@ __device__ __forceinline__ void store_plane(double* S, const LineJob& J, bool RS
 // All sub-steps of one job (QUICKEST6.cpp:37-52 sub-cycle, one pass per
 // sub-step).  The loops over a lane's cells stay rolled (one copy of the face
 // code per phase keeps the kernel small enough for the instruction caches);
-// the per-cell state between phases lives in the line buffers.
+// the per-cell state between phases lives in the line buffers.  The cell
+// loops store every cell's flux update (periodic ghost mirrors with it); the
+// lanes that own a line's end cells then apply the boundary rewrite and the
+// ghosts that follow from it.
 template <bool RS, int DIR>
 __device__ __forceinline__ void job_substeps(double* S, const LineJob& J)
 {
+    const int np = J.lpl * J.T;
+    const bool per = J.lt == VERB_BC_PERIODIC;
+    const bool own0 = J.lv && J.j == 0;
+    const bool ownl = J.lv && J.j == (J.n - 1) % J.lpl;
+    const int nc = J.lv ? J.n : 0;  // cells this lane's line stores
     for (int sub = 0; sub < J.nsmax; sub++) {
         // A: unlimited faces
 #pragma unroll 1
-        for (int x = J.j; x < J.lpl * J.T; x += J.lpl) {
+        for (int x = J.j; x < np; x += J.lpl) {
             double w[10];
 #pragma unroll
             for (int k = 0; k < 10; k++) w[k] = J.E[x + k];
             J.F[x] = face3<DIR>(w, J.CR[x]);
         }
         __syncwarp();
-        // B: unlimited cells into UE
+        // B: unlimited cells into UE; high ghosts follow UE (:307-326), low
+        // ghosts are the pre-step ones of E (:281-304)
 #pragma unroll 1
-        for (int x = J.j; x < J.lpl * J.T; x += J.lpl)
-            if (J.lv && x < J.n) store_ue(J, x, cell_final3(J, x));
-        if (J.lv && J.j < 5) J.UE[J.j] = J.E[J.j];
+        for (int x = J.j; x < nc; x += J.lpl) {
+            const double v = cell_raw3(J, x);
+            J.UE[x + 5] = v;
+            if (per && x >= 1 && x <= 5) J.UE[x + J.n + 4] = v;
+        }
+        if (own0) {
+            for (int k = 0; k < 5; k++) J.UE[k] = J.E[k];
+            J.UE[5] = cell_first3(J);
+        }
+        if (ownl) {
+            const double v = cell_last3(J);
+            J.UE[J.n + 4] = v;
+            if (J.ut == VERB_BC_CONSTANT_DERIVATIVE) cd_high(J.UE, J.n, v, J.ubc, J.dxu);
+        }
         __syncwarp();
         // C: limited faces, in place (each lane reads only its own faces)
 #pragma unroll 1
-        for (int x = J.j; x < J.lpl * J.T; x += J.lpl) {
+        for (int x = J.j; x < np; x += J.lpl) {
             double u[8], ev[4];
 #pragma unroll
             for (int k = 0; k < 8; k++) u[k] = J.UE[x + 1 + k];
@@ -613,25 +644,39 @@ __device__ __forceinline__ void job_substeps(double* S, const LineJob& J)
             J.F[x] = limit3<DIR>(J.F[x], J.CR[x], u, ev);
         }
         __syncwarp();
-        // D: final cells; lines that go on stage the new values in UE (free
-        // after phase C) and copy them into E once every lane is done with E
+        // D: final cells.  On a line's last sub-step they go to the plane;
+        // otherwise they are staged in UE (free after phase C) and copied into
+        // E once every lane is done reading E.
         const bool last = sub == J.ns - 1;
+        if (last) {
 #pragma unroll 1
-        for (int x = J.j; x < J.lpl * J.T; x += J.lpl) {
-            if (J.lv && x < J.n) {
-                const double v = cell_final3(J, x);
-                if (last) store_plane(S, J, RS, x, v);
-                else J.UE[x + 5] = v;
-            }
+            for (int x = J.j; x < nc; x += J.lpl) store_plane(S, J, RS, x, cell_raw3(J, x));
+            if (own0) store_plane(S, J, RS, 0, cell_first3(J));
+            if (ownl) store_plane(S, J, RS, J.n - 1, cell_last3(J));
+        } else {
+#pragma unroll 1
+            for (int x = J.j; x < nc; x += J.lpl) J.UE[x + 5] = cell_raw3(J, x);
+            if (own0) J.UE[5] = cell_first3(J);
+            if (ownl) J.UE[J.n + 4] = cell_last3(J);
         }
         if (sub + 1 < J.nsmax) {
             __syncwarp();
 #pragma unroll 1
-            for (int x = J.j; x < J.lpl * J.T; x += J.lpl)
-                if (J.lv && x < J.n) store_e(J, x, J.UE[x + 5]);
+            for (int x = J.j; x < nc; x += J.lpl) {
+                const double v = J.UE[x + 5];
+                J.E[x + 5] = v;
+                if (per) {
+                    if (x >= J.n - 6 && x <= J.n - 2) J.E[x - J.n + 6] = v;
+                    if (x >= 1 && x <= 5) J.E[x + J.n + 4] = v;
+                }
+            }
+            if (own0 && J.lt == VERB_BC_CONSTANT_DERIVATIVE) cd_low(J.E, J.UE[5], J.lbc, J.dxl);
+            if (ownl && J.ut == VERB_BC_CONSTANT_DERIVATIVE)
+                cd_high(J.E, J.n, J.UE[J.n + 4], J.ubc, J.dxu);
             __syncwarp();
         }
     }
+    __syncwarp();  // the warp's next job overwrites the buffers read in phase D
 }
 
 struct LineArrays {
@@ -670,11 +715,21 @@ __device__ __forceinline__ void sweep_job(double* S, double* wb, const SweepCfg&
     J.nsmax = __reduce_max_sync(0xffffffffu, J.ns);
     const int ix0 = (lt == VERB_BC_PERIODIC) ? 0 : 1;
     bool pos = true, neg = true;
+    // E with its ghost cells (QUICKEST6.cpp:89-143): periodic mirrors by the
+    // owners of the mirrored cells, constant values and constant-derivative
+    // extrapolations by the owners of the end cells
     for (int x = J.j; x <= J.lpl * J.T; x += J.lpl) {
         double cr = 0.0;
         if (J.lv && x < n) {
             cr = crtab[(size_t)J.li * n + x];
-            store_e(J, x, RS ? S[J.li * R + x] : S[x * R + J.li]);
+            const double v = RS ? S[J.li * R + x] : S[x * R + J.li];
+            J.E[x + 5] = v;
+            if (lt == VERB_BC_PERIODIC) {
+                if (x >= n - 6 && x <= n - 2) J.E[x - n + 6] = v;
+                if (x >= 1 && x <= 5) J.E[x + n + 4] = v;
+            }
+            if (x == 0 && lt == VERB_BC_CONSTANT_DERIVATIVE) cd_low(J.E, v, J.lbc, J.dxl);
+            if (x == n - 1 && ut == VERB_BC_CONSTANT_DERIVATIVE) cd_high(J.E, n, v, J.ubc, J.dxu);
             if (x >= ix0) {
                 pos = pos && cr >= 0;
                 neg = neg && cr < 0;
@@ -692,6 +747,15 @@ __device__ __forceinline__ void sweep_job(double* S, double* wb, const SweepCfg&
     if (pos) job_substeps<RS, DIR_POS>(S, J);
     else if (neg) job_substeps<RS, DIR_NEG>(S, J);
     else job_substeps<RS, DIR_MIX>(S, J);
+}
+
+// offset (doubles) of the warp buffers in the dynamic shared memory: plane,
+// per-line arrays, reduction slots and the int sub-step counts, rounded up to
+// 16 bytes
+__host__ __device__ inline int conv_wall_offset(int P, int R)
+{
+    const int o = P * R + 4 * R + 4 * P + 32 + (R + P + 1) / 2;
+    return (o + 1) & ~1;
 }
 
 __host__ __device__ inline size_t conv_scratch_per_cta(int P, int R)
@@ -719,7 +783,7 @@ __global__ void __launch_bounds__(C3_THREADS, 2) convection_kernel(ConvArgs a)
     int* nsP = (int*)(red + 32);   // [R]
     int* nsR = nsP + R;            // [P]
     const int wstride = conv_wstride(P, R);
-    double* wall = (double*)(((uintptr_t)(nsR + P) + 15) & ~(uintptr_t)15);
+    double* wall = sm + conv_wall_offset(P, R);  // pointer arithmetic on sm keeps LDS/STS
     double* wb = wall + (size_t)warp * wstride;
     __shared__ int s_ticket;
 
@@ -954,8 +1018,7 @@ __global__ void __launch_bounds__(CONV_THREADS)
 
 size_t conv_smem_bytes(int P, int R)
 {
-    return ((size_t)P * R + 4 * (size_t)R + 4 * (size_t)P + 32) * sizeof(double) +
-           (size_t)(R + P) * sizeof(int) + 16 + (size_t)C3_WARPS * conv_wstride(P, R) * sizeof(double);
+    return ((size_t)conv_wall_offset(P, R) + (size_t)C3_WARPS * conv_wstride(P, R)) * sizeof(double);
 }
 
 size_t conv_scratch_doubles(int P, int R) { return conv_scratch_per_cta(P, R); }
