@@ -487,6 +487,15 @@ __device__ __forceinline__ double limit3(double f, double cr, const double (&u)[
                               up ? u[6] : u[1]);
 }
 
+// 8-byte asynchronous global->shared copy (cp.async, sm_80+).
+__device__ __forceinline__ void cp_async8(double* dst, const double* src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Work split of one sweep: nlines lines of n points, lpl lanes per line.
 struct SweepCfg {
     int lpl, T, nlw, njobs, nb;  // nb: doubles per line buffer (E, UE, F and CR each)
@@ -561,29 +570,6 @@ __device__ __forceinline__ double cell_last3(const LineJob& J)
     return cell_raw3(J, J.ut == VERB_BC_CONSTANT_DERIVATIVE ? J.n - 2 : 0);
 }
 
-// Constant-derivative ghost cells from an end value (:108-115, 134-140 and
-// :295-300, 319-324): low ghosts X[4..0] from cell 0, high X[n+5..n+9] from
-// cell n-1, each the previous one -/+ bc*dx.
-__device__ __forceinline__ void cd_low(double* X, double v0, double bc, double dx)
-{
-    double g = v0 - bc * dx;
-    X[4] = g;
-    for (int ig = 2; ig <= 5; ig++) {
-        g = g - bc * dx;
-        X[5 - ig] = g;
-    }
-}
-
-__device__ __forceinline__ void cd_high(double* X, int n, double vn, double bc, double dx)
-{
-    double g = vn + bc * dx;
-    X[n + 5] = g;
-    for (int ig = 2; ig <= 5; ig++) {
-        g = g + bc * dx;
-        X[n + 4 + ig] = g;
-    }
-}
-
 __device__ __forceinline__ void store_plane(double* S, const LineJob& J, bool RS, int x, double v)
 {
     if (RS) S[J.li * J.R + x] = v;
@@ -597,82 +583,147 @@ __device__ __forceinline__ void store_plane(double* S, const LineJob& J, bool RS
 // loops store every cell's flux update (periodic ghost mirrors with it); the
 // lanes that own a line's end cells then apply the boundary rewrite and the
 // ghosts that follow from it.
+// Ghost cells of the extended line X from its interior (QUICKEST6.cpp:94-140
+// for E; :281-326 for UE with lowsrc = E): lanes 0-4 of a line fill low ghost
+// j+1, lanes 5-9 high ghost j-4.  lowsrc supplies the low ghosts' periodic
+// and constant-derivative values; constant-value ghosts are written only when
+// cv is set (they never change within a job).
+__device__ __forceinline__ void fill_ghosts3(double* X, const double* lowsrc, const LineJob& J,
+                                             bool low, bool cv)
+{
+    const int n = J.n;
+    if (low && J.j < 5) {
+        const int ig = J.j + 1;
+        if (J.lt == VERB_BC_PERIODIC) {
+            X[5 - ig] = lowsrc[5 + (n - 1) - ig];
+        } else if (J.lt == VERB_BC_CONSTANT_VALUE) {
+            if (cv) X[5 - ig] = J.lbc;
+        } else {
+            double g = lowsrc[5] - J.lbc * J.dxl;
+            for (int i = 2; i <= ig; i++) g = g - J.lbc * J.dxl;
+            X[5 - ig] = g;
+        }
+    } else if (J.j >= 5 && J.j < 10) {
+        const int ig = J.j - 4;
+        if (J.ut == VERB_BC_PERIODIC) {
+            X[5 + (n - 1) + ig] = X[5 + ig];
+        } else if (J.ut == VERB_BC_CONSTANT_VALUE) {
+            if (cv) X[5 + (n - 1) + ig] = J.ubc;
+        } else {
+            double g = X[5 + n - 1] + J.ubc * J.dxu;
+            for (int i = 2; i <= ig; i++) g = g + J.ubc * J.dxu;
+            X[5 + (n - 1) + ig] = g;
+        }
+    }
+}
+
+// All sub-steps of one job (QUICKEST6.cpp:37-52 sub-cycle, one pass per
+// sub-step).  The loops over a lane's cells stay rolled (one copy of the face
+// code per phase keeps the kernel small enough for the instruction caches);
+// the per-cell state between phases lives in the line buffers.  Cell loops
+// cover cells 0..n-2 (lane 0 rewrites cell 0); lane 1 of a line writes cell
+// n-1 with its boundary rewrite; lanes 0-9 then fill the ghost cells.
 template <bool RS, int DIR>
 __device__ __forceinline__ void job_substeps(double* S, const LineJob& J)
 {
-    const int np = J.lpl * J.T;
-    const bool per = J.lt == VERB_BC_PERIODIC;
-    const bool own0 = J.lv && J.j == 0;
-    const bool ownl = J.lv && J.j == (J.n - 1) % J.lpl;
-    const int nc = J.lv ? J.n : 0;  // cells this lane's line stores
+    const int L = J.lpl;
+    const bool lane0 = J.lv && J.j == 0;
+    const bool lane1 = J.lv && J.j == 1;
+    const int nc = J.lv ? J.n - 1 : 0;
+    // the lane's first cell in every buffer; loops advance them by L cells
+    const double* const E0 = J.E + J.j;
+    double* const UE0 = J.UE + J.j;
+    double* const F0 = J.F + J.j;
+    const double* const CR0 = J.CR + J.j;
+    double* const SP0 = RS ? S + J.li * J.R + J.j : S + J.j * J.R + J.li;
+    const int sstep = RS ? L : L * J.R;
     for (int sub = 0; sub < J.nsmax; sub++) {
         // A: unlimited faces
+        {
+            const double* e = E0;
+            const double* c = CR0;
+            double* f = F0;
 #pragma unroll 1
-        for (int x = J.j; x < np; x += J.lpl) {
-            double w[10];
+            for (int t = 0; t < J.T; t++, e += L, c += L, f += L) {
+                double w[10];
 #pragma unroll
-            for (int k = 0; k < 10; k++) w[k] = J.E[x + k];
-            J.F[x] = face3<DIR>(w, J.CR[x]);
+                for (int k = 0; k < 10; k++) w[k] = e[k];
+                *f = face3<DIR>(w, *c);
+            }
         }
         __syncwarp();
-        // B: unlimited cells into UE; high ghosts follow UE (:307-326), low
-        // ghosts are the pre-step ones of E (:281-304)
-#pragma unroll 1
-        for (int x = J.j; x < nc; x += J.lpl) {
-            const double v = cell_raw3(J, x);
-            J.UE[x + 5] = v;
-            if (per && x >= 1 && x <= 5) J.UE[x + J.n + 4] = v;
+        // B: unlimited cells into UE
+        {
+            const double* e = E0;
+            const double* c = CR0;
+            const double* f = F0;
+            double* u = UE0;
+#pragma unroll 2
+            for (int x = J.j; x < nc; x += L, e += L, c += L, f += L, u += L)
+                u[5] = e[5] - (c[1] * f[1] - c[0] * f[0]);
         }
-        if (own0) {
-            for (int k = 0; k < 5; k++) J.UE[k] = J.E[k];
-            J.UE[5] = cell_first3(J);
-        }
-        if (ownl) {
-            const double v = cell_last3(J);
-            J.UE[J.n + 4] = v;
-            if (J.ut == VERB_BC_CONSTANT_DERIVATIVE) cd_high(J.UE, J.n, v, J.ubc, J.dxu);
+        if (lane0) J.UE[5] = cell_first3(J);
+        else if (lane1) J.UE[J.n + 4] = cell_last3(J);
+        __syncwarp();
+        if (J.lv) {
+            if (J.j < 5) J.UE[J.j] = J.E[J.j];  // low ghosts: the pre-step ones of E
+            fill_ghosts3(J.UE, J.E, J, false, false);
         }
         __syncwarp();
         // C: limited faces, in place (each lane reads only its own faces)
+        {
+            const double* e = E0;
+            const double* c = CR0;
+            double* f = F0;
+            const double* u = UE0;
 #pragma unroll 1
-        for (int x = J.j; x < np; x += J.lpl) {
-            double u[8], ev[4];
+            for (int t = 0; t < J.T; t++, e += L, c += L, f += L, u += L) {
+                double uu[8], ev[4];
 #pragma unroll
-            for (int k = 0; k < 8; k++) u[k] = J.UE[x + 1 + k];
+                for (int k = 0; k < 8; k++) uu[k] = u[1 + k];
 #pragma unroll
-            for (int k = 0; k < 4; k++) ev[k] = J.E[x + 3 + k];
-            J.F[x] = limit3<DIR>(J.F[x], J.CR[x], u, ev);
+                for (int k = 0; k < 4; k++) ev[k] = e[3 + k];
+                *f = limit3<DIR>(*f, *c, uu, ev);
+            }
         }
         __syncwarp();
         // D: final cells.  On a line's last sub-step they go to the plane;
         // otherwise they are staged in UE (free after phase C) and copied into
         // E once every lane is done reading E.
         const bool last = sub == J.ns - 1;
-        if (last) {
-#pragma unroll 1
-            for (int x = J.j; x < nc; x += J.lpl) store_plane(S, J, RS, x, cell_raw3(J, x));
-            if (own0) store_plane(S, J, RS, 0, cell_first3(J));
-            if (ownl) store_plane(S, J, RS, J.n - 1, cell_last3(J));
-        } else {
-#pragma unroll 1
-            for (int x = J.j; x < nc; x += J.lpl) J.UE[x + 5] = cell_raw3(J, x);
-            if (own0) J.UE[5] = cell_first3(J);
-            if (ownl) J.UE[J.n + 4] = cell_last3(J);
+        {
+            const double* e = E0;
+            const double* c = CR0;
+            const double* f = F0;
+            double* u = UE0;
+            double* sp = SP0;
+#pragma unroll 2
+            for (int x = J.j; x < nc; x += L, e += L, c += L, f += L, u += L, sp += sstep) {
+                const double v = e[5] - (c[1] * f[1] - c[0] * f[0]);
+                if (last) *sp = v;
+                else u[5] = v;
+            }
+        }
+        if (lane0) {
+            const double v = cell_first3(J);
+            if (last) store_plane(S, J, RS, 0, v);
+            else J.UE[5] = v;
+        } else if (lane1) {
+            const double v = cell_last3(J);
+            if (last) store_plane(S, J, RS, J.n - 1, v);
+            else J.UE[J.n + 4] = v;
         }
         if (sub + 1 < J.nsmax) {
             __syncwarp();
-#pragma unroll 1
-            for (int x = J.j; x < nc; x += J.lpl) {
-                const double v = J.UE[x + 5];
-                J.E[x + 5] = v;
-                if (per) {
-                    if (x >= J.n - 6 && x <= J.n - 2) J.E[x - J.n + 6] = v;
-                    if (x >= 1 && x <= 5) J.E[x + J.n + 4] = v;
-                }
+            {
+                const double* u = UE0;
+                double* e = J.E + J.j;
+                const int ncf = J.lv ? J.n : 0;
+#pragma unroll 2
+                for (int x = J.j; x < ncf; x += L, u += L, e += L) e[5] = u[5];
             }
-            if (own0 && J.lt == VERB_BC_CONSTANT_DERIVATIVE) cd_low(J.E, J.UE[5], J.lbc, J.dxl);
-            if (ownl && J.ut == VERB_BC_CONSTANT_DERIVATIVE)
-                cd_high(J.E, J.n, J.UE[J.n + 4], J.ubc, J.dxu);
+            __syncwarp();
+            if (J.lv) fill_ghosts3(J.E, J.E, J, true, false);
             __syncwarp();
         }
     }
@@ -681,7 +732,7 @@ __device__ __forceinline__ void job_substeps(double* S, const LineJob& J)
 
 struct LineArrays {
     const double *lb, *ub, *dxl, *dxu;
-    const int* ns;
+    const int *ns, *dir;
 };
 
 // One job of a sweep: load the lines into the warp's buffers, pick the
@@ -707,46 +758,44 @@ __device__ __forceinline__ void sweep_job(double* S, double* wb, const SweepCfg&
     J.UE = J.E + c.nb;
     J.F = J.UE + c.nb;
     J.CR = J.F + c.nb;
+    const int L = c.lpl;
+    // the lines' face Courant numbers: asynchronous copies from the per-CTA
+    // table (L2), in flight while the lines are copied out of the plane
+    {
+        const double* src = crtab + (size_t)J.li * n + J.j;
+        double* dst = J.CR + J.j;
+        const int nv = J.lv ? n : 0;
+        int x = J.j;
+        for (; x < nv; x += L, src += L, dst += L) cp_async8(dst, src);
+        for (; x <= L * c.T; x += L, dst += L) *dst = 0.0;
+        cp_async_commit();
+    }
     J.lbc = J.lv ? la.lb[J.li] : 0.0;
     J.ubc = J.lv ? la.ub[J.li] : 0.0;
     J.dxl = J.lv ? la.dxl[J.li] : 0.0;
     J.dxu = J.lv ? la.dxu[J.li] : 0.0;
     J.ns = J.lv ? la.ns[J.li] : 0;
     J.nsmax = __reduce_max_sync(0xffffffffu, J.ns);
-    const int ix0 = (lt == VERB_BC_PERIODIC) ? 0 : 1;
-    bool pos = true, neg = true;
-    // E with its ghost cells (QUICKEST6.cpp:89-143): periodic mirrors by the
-    // owners of the mirrored cells, constant values and constant-derivative
-    // extrapolations by the owners of the end cells
-    for (int x = J.j; x <= J.lpl * J.T; x += J.lpl) {
-        double cr = 0.0;
-        if (J.lv && x < n) {
-            cr = crtab[(size_t)J.li * n + x];
-            const double v = RS ? S[J.li * R + x] : S[x * R + J.li];
-            J.E[x + 5] = v;
-            if (lt == VERB_BC_PERIODIC) {
-                if (x >= n - 6 && x <= n - 2) J.E[x - n + 6] = v;
-                if (x >= 1 && x <= 5) J.E[x + n + 4] = v;
-            }
-            if (x == 0 && lt == VERB_BC_CONSTANT_DERIVATIVE) cd_low(J.E, v, J.lbc, J.dxl);
-            if (x == n - 1 && ut == VERB_BC_CONSTANT_DERIVATIVE) cd_high(J.E, n, v, J.ubc, J.dxu);
-            if (x >= ix0) {
-                pos = pos && cr >= 0;
-                neg = neg && cr < 0;
-            }
-        }
-        J.CR[x] = cr;
+    const unsigned dir = __reduce_or_sync(0xffffffffu, J.lv ? (unsigned)la.dir[J.li] : 0u);
+    // E (QUICKEST6.cpp:89-91), then its ghost cells
+    {
+        const double* sp = RS ? S + J.li * R + J.j : S + J.j * R + J.li;
+        const int sstep = RS ? L : L * R;
+        double* e = J.E + 5 + J.j;
+        const int nv = J.lv ? n : 0;
+#pragma unroll 2
+        for (int x = J.j; x < nv; x += L, sp += sstep, e += L) *e = *sp;
     }
-    if (J.lv && J.j == 0 && lt == VERB_BC_CONSTANT_VALUE)
-        for (int k = 0; k < 5; k++) J.E[k] = J.lbc;
-    if (J.lv && J.j == (n - 1) % J.lpl && ut == VERB_BC_CONSTANT_VALUE)
-        for (int k = 0; k < 5; k++) J.E[n + 5 + k] = J.UE[n + 5 + k] = J.ubc;
-    pos = __all_sync(0xffffffffu, pos);
-    neg = __all_sync(0xffffffffu, neg);
     __syncwarp();
-    if (pos) job_substeps<RS, DIR_POS>(S, J);
-    else if (neg) job_substeps<RS, DIR_NEG>(S, J);
-    else job_substeps<RS, DIR_MIX>(S, J);
+    if (J.lv) {
+        fill_ghosts3(J.E, J.E, J, true, true);
+        if (ut == VERB_BC_CONSTANT_VALUE && J.j >= 5 && J.j < 10) J.UE[n + J.j] = J.ubc;
+    }
+    cp_async_wait_all();
+    __syncwarp();
+    if (dir == 2u) job_substeps<RS, DIR_NEG>(S, J);
+    else if (dir == 3u) job_substeps<RS, DIR_MIX>(S, J);
+    else job_substeps<RS, DIR_POS>(S, J);
 }
 
 // offset (doubles) of the warp buffers in the dynamic shared memory: plane,
@@ -754,7 +803,7 @@ __device__ __forceinline__ void sweep_job(double* S, double* wb, const SweepCfg&
 // 16 bytes
 __host__ __device__ inline int conv_wall_offset(int P, int R)
 {
-    const int o = P * R + 4 * R + 4 * P + 32 + (R + P + 1) / 2;
+    const int o = P * R + 4 * R + 4 * P + 32 + (R + P);
     return (o + 1) & ~1;
 }
 
@@ -780,8 +829,10 @@ __global__ void __launch_bounds__(C3_THREADS, 2) convection_kernel(ConvArgs a)
     double* dxR = ubR + P;
     double* dxRu = dxR + P;
     double* red = dxRu + P;        // [32]
-    int* nsP = (int*)(red + 32);   // [R]
+    int* nsP = (int*)(red + 32);   // [R] per-line sub-steps
     int* nsR = nsP + R;            // [P]
+    int* dirP = nsR + P;           // [R] per-line face directions: bit 0 some Courant >= 0,
+    int* dirR = dirP + R;          // [P]                           bit 1 some Courant < 0
     const int wstride = conv_wstride(P, R);
     double* wall = sm + conv_wall_offset(P, R);  // pointer arithmetic on sm keeps LDS/STS
     double* wb = wall + (size_t)warp * wstride;
@@ -799,8 +850,13 @@ __global__ void __launch_bounds__(C3_THREADS, 2) convection_kernel(ConvArgs a)
     double* lexp = gpl + PR;   // exp(Loss dt)
     double* spl = lexp + PR;   // Sources dt
     const int nslices = V * K;
-    const LineArrays laP{lbP, ubP, dxP, dxPu, nsP};
-    const LineArrays laR{lbR, ubR, dxR, dxRu, nsR};
+    const LineArrays laP{lbP, ubP, dxP, dxPu, nsP, dirP};
+    const LineArrays laR{lbR, ubR, dxR, dxRu, nsR, dirR};
+    // first face of a line that the reference sweeps (face 0 only when periodic)
+    const int ixP0 = a.Pl_t == VERB_BC_PERIODIC ? 0 : 1;
+    const int ixR0 = a.Rl_t == VERB_BC_PERIODIC ? 0 : 1;
+    // the thread's first L index and its advance per C3_THREADS cells
+    const int iR0 = threadIdx.x % R, iRstep = C3_THREADS % R;
 
     for (;;) {
         if (threadIdx.x == 0) s_ticket = atomicAdd(a.ticket, 1);
@@ -875,13 +931,18 @@ __global__ void __launch_bounds__(C3_THREADS, 2) convection_kernel(ConvArgs a)
                 else if (sd > 1) ns = (int)ceil(sd);
                 const double dtl = dtc / ns;
                 if (fabs(m / dx * dtl) > 1) set_error(a.status, VERB_ERR_CFL);
+                unsigned dir = 0;
                 for (int ix = lane; ix < P; ix += 32) {
                     const int i0 = ix == 0 ? P - 2 : ix - 1;
                     const double c0 = a.VP[g(i0, iR)] / dx * dtl;
                     const double c1 = a.VP[g(ix, iR)] / dx * dtl;
-                    crP[(size_t)iR * P + ix] = (c0 + c1) / 2;
+                    const double cr = (c0 + c1) / 2;
+                    crP[(size_t)iR * P + ix] = cr;
+                    if (ix >= ixP0) dir |= cr >= 0 ? 1u : (cr < 0 ? 2u : 0u);
                 }
+                dir = __reduce_or_sync(0xffffffffu, dir);
                 if (lane == 0) {
+                    dirP[iR] = (int)dir;
                     nsP[iR] = ns;
                     dxP[iR] = dx;
                     dxPu[iR] = a.Pg[g(P - 1, iR)] - a.Pg[g(P - 2, iR)];
@@ -909,13 +970,18 @@ __global__ void __launch_bounds__(C3_THREADS, 2) convection_kernel(ConvArgs a)
                 else if (sd > 1) ns = (int)ceil(sd);
                 const double dtl = dtc / ns;
                 if (fabs(m / dx * dtl) > 1) set_error(a.status, VERB_ERR_CFL);
+                unsigned dir = 0;
                 for (int ix = lane; ix < R; ix += 32) {
                     const int i0 = ix == 0 ? R - 2 : ix - 1;
                     const double c0 = a.VR[g(iP, i0)] / dx * dtl;
                     const double c1 = a.VR[g(iP, ix)] / dx * dtl;
-                    crR[(size_t)iP * R + ix] = (c0 + c1) / 2;
+                    const double cr = (c0 + c1) / 2;
+                    crR[(size_t)iP * R + ix] = cr;
+                    if (ix >= ixR0) dir |= cr >= 0 ? 1u : (cr < 0 ? 2u : 0u);
                 }
+                dir = __reduce_or_sync(0xffffffffu, dir);
                 if (lane == 0) {
+                    dirR[iP] = (int)dir;
                     nsR[iP] = ns;
                     dxR[iP] = dx;
                     dxRu[iP] = a.Rg[g(iP, R - 1)] - a.Rg[g(iP, R - 2)];
@@ -935,26 +1001,32 @@ __global__ void __launch_bounds__(C3_THREADS, 2) convection_kernel(ConvArgs a)
                 __syncthreads();
             }
             if (R >= 3) {
-                for (int i = threadIdx.x; i < PR; i += blockDim.x) S[i] = S[i] * gpl[i];
+#pragma unroll 4
+                for (int i = threadIdx.x; i < PR; i += C3_THREADS) S[i] = S[i] * gpl[i];
                 __syncthreads();
                 for (int job = warp; job < cR.njobs; job += C3_WARPS)
                     sweep_job<true>(S, wb, cR, job, R, P, R, a.Rl_t, a.Ru_t, crR, laR);
                 __syncthreads();
-                for (int i = threadIdx.x; i < PR; i += blockDim.x) {
-                    const int iR = i - (i / R) * R;
+                int iR = iR0;
+#pragma unroll 4
+                for (int i = threadIdx.x; i < PR; i += C3_THREADS) {
                     double x = S[i] / gpl[i];
                     x = x * lexp[i];
                     if (iR >= 1 && iR < R - 1) x = x + spl[i];
                     S[i] = x;
+                    iR += iRstep;
+                    if (iR >= R) iR -= R;
                 }
                 __syncthreads();
             } else {
                 // no R-sweep: exp(loss dt) and sources only (:147-165)
-                for (int i = threadIdx.x; i < PR; i += blockDim.x) {
-                    const int iR = i - (i / R) * R;
+                int iR = iR0;
+                for (int i = threadIdx.x; i < PR; i += C3_THREADS) {
                     double x = S[i] * lexp[i];
                     if (iR >= 1 && iR < R - 1) x = x + spl[i];
                     S[i] = x;
+                    iR += iRstep;
+                    if (iR >= R) iR -= R;
                 }
                 __syncthreads();
             }
