@@ -380,7 +380,7 @@ __device__ __forceinline__ double block_max(double v, double* red)
 
 constexpr int C3_WARPS = 8;
 constexpr int C3_THREADS = C3_WARPS * 32;
-constexpr int TMAX = 8;  // cells per lane: lines of up to 32*TMAX points
+constexpr int TMAX = 16;  // cells per lane: lines of up to 32*TMAX points
 
 // a / b rounded to nearest, for the constants b = 6, 120, 5040 and 362880 with
 // y = RN(1/b) (Markstein's correction step: P. Markstein, IBM J. Res. Dev.
@@ -496,7 +496,11 @@ __device__ __forceinline__ void cp_async8(double* dst, const double* src)
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// Work split of one sweep: nlines lines of n points, lpl lanes per line.
+// Work split of one sweep: nlines lines of n points, lpl lanes per line, T
+// cells per lane.  The choice models a job's cost as a fixed part (line
+// set-up, boundary cells, ghost cells, barriers: about 400 warp instructions)
+// plus about 330 per cell step, and counts half of the idle warp slots of the
+// last round (the other CTA on the SM fills the rest).
 struct SweepCfg {
     int lpl, T, nlw, njobs, nb;  // nb: doubles per line buffer (E, UE, F and CR each)
 };
@@ -504,16 +508,17 @@ struct SweepCfg {
 __host__ __device__ inline SweepCfg sweep_cfg(int n, int nlines)
 {
     SweepCfg best{0, 0, 0, 0, 0};
-    double be = -1.0;
+    double bc = 0.0;
     for (int lpl = 32; lpl >= 8; lpl >>= 1) {
         const int T = (n + lpl - 1) / lpl;
         if (T > TMAX) continue;
         const int nlw = 32 / lpl;
         const int jobs = (nlines + nlw - 1) / nlw;
         const int rounds = (jobs + C3_WARPS - 1) / C3_WARPS;
-        const double eff = (double)nlines * n / ((double)(rounds > 0 ? rounds : 1) * C3_WARPS * 32 * T);
-        if (eff > be + 1e-12) {
-            be = eff;
+        const double job = 400.0 + 330.0 * T;
+        const double cost = job * (jobs + 0.5 * (rounds * C3_WARPS - jobs));
+        if (best.lpl == 0 || cost < bc - 1e-9) {
+            bc = cost;
             best = SweepCfg{lpl, T, nlw, jobs, lpl * T + 10};
         }
     }
@@ -556,18 +561,16 @@ __device__ __forceinline__ double cell_raw3(const LineJob& J, int k)
     return J.E[k + 5] - (J.CR[k + 1] * J.F[k + 1] - J.CR[k] * J.F[k]);
 }
 
-// Boundary rewrites of the end cells (:257-272 / 457-477); cells 1..n-2 keep
-// their flux update.
-__device__ __forceinline__ double cell_first3(const LineJob& J)
+// End cell of a line after the boundary rewrite (:257-272 / 457-477): lane 0
+// of a line computes cell 0 and lane 1 cell n-1, with the same code; cells
+// 1..n-2 keep their flux update.
+__device__ __forceinline__ double edge_cell3(const LineJob& J)
 {
-    if (J.lt == VERB_BC_CONSTANT_VALUE) return J.lbc;
-    return cell_raw3(J, J.lt == VERB_BC_CONSTANT_DERIVATIVE ? 1 : 0);
-}
-
-__device__ __forceinline__ double cell_last3(const LineJob& J)
-{
-    if (J.ut == VERB_BC_CONSTANT_VALUE) return J.ubc;
-    return cell_raw3(J, J.ut == VERB_BC_CONSTANT_DERIVATIVE ? J.n - 2 : 0);
+    const bool hi = J.j == 1;
+    const int type = hi ? J.ut : J.lt;
+    const int k = type == VERB_BC_CONSTANT_DERIVATIVE ? (hi ? J.n - 2 : 1) : 0;
+    const double raw = cell_raw3(J, k);
+    return type == VERB_BC_CONSTANT_VALUE ? (hi ? J.ubc : J.lbc) : raw;
 }
 
 __device__ __forceinline__ void store_plane(double* S, const LineJob& J, bool RS, int x, double v)
@@ -576,44 +579,32 @@ __device__ __forceinline__ void store_plane(double* S, const LineJob& J, bool RS
     else S[x * J.R + J.li] = v;
 }
 
-// All sub-steps of one job (QUICKEST6.cpp:37-52 sub-cycle, one pass per
-// sub-step).  The loops over a lane's cells stay rolled (one copy of the face
-// code per phase keeps the kernel small enough for the instruction caches);
-// the per-cell state between phases lives in the line buffers.  The cell
-// loops store every cell's flux update (periodic ghost mirrors with it); the
-// lanes that own a line's end cells then apply the boundary rewrite and the
-// ghosts that follow from it.
 // Ghost cells of the extended line X from its interior (QUICKEST6.cpp:94-140
-// for E; :281-326 for UE with lowsrc = E): lanes 0-4 of a line fill low ghost
-// j+1, lanes 5-9 high ghost j-4.  lowsrc supplies the low ghosts' periodic
-// and constant-derivative values; constant-value ghosts are written only when
-// cv is set (they never change within a job).
-__device__ __forceinline__ void fill_ghosts3(double* X, const double* lowsrc, const LineJob& J,
-                                             bool low, bool cv)
+// for E; :281-326 for UE).  Ghost gi < 5 is low ghost gi+1, gi >= 5 high
+// ghost gi-4; the lanes of a line take the ten of them in turn, with the same
+// code at both ends.  With low unset only the high ghosts are filled (UE's low
+// ghosts are copies of E's); constant-value ghosts are written only when cv is
+// set (they do not change within a job).
+__device__ __forceinline__ void fill_ghosts3(double* X, const LineJob& J, bool low, bool cv)
 {
     const int n = J.n;
-    if (low && J.j < 5) {
-        const int ig = J.j + 1;
-        if (J.lt == VERB_BC_PERIODIC) {
-            X[5 - ig] = lowsrc[5 + (n - 1) - ig];
-        } else if (J.lt == VERB_BC_CONSTANT_VALUE) {
-            if (cv) X[5 - ig] = J.lbc;
+    for (int gi = J.j; gi < 10; gi += J.lpl) {
+        if (!low && gi < 5) continue;
+        const bool hi = gi >= 5;
+        const int ig = hi ? gi - 4 : gi + 1;
+        const int type = hi ? J.ut : J.lt;
+        double g;
+        if (type == VERB_BC_PERIODIC) {
+            g = X[hi ? 5 + ig : 5 + (n - 1) - ig];
+        } else if (type == VERB_BC_CONSTANT_VALUE) {
+            if (!cv) continue;
+            g = hi ? J.ubc : J.lbc;
         } else {
-            double g = lowsrc[5] - J.lbc * J.dxl;
-            for (int i = 2; i <= ig; i++) g = g - J.lbc * J.dxl;
-            X[5 - ig] = g;
+            const double c = hi ? J.ubc * J.dxu : J.lbc * J.dxl;
+            g = hi ? X[5 + n - 1] + c : X[5] - c;
+            for (int i = 2; i <= ig; i++) g = hi ? g + c : g - c;
         }
-    } else if (J.j >= 5 && J.j < 10) {
-        const int ig = J.j - 4;
-        if (J.ut == VERB_BC_PERIODIC) {
-            X[5 + (n - 1) + ig] = X[5 + ig];
-        } else if (J.ut == VERB_BC_CONSTANT_VALUE) {
-            if (cv) X[5 + (n - 1) + ig] = J.ubc;
-        } else {
-            double g = X[5 + n - 1] + J.ubc * J.dxu;
-            for (int i = 2; i <= ig; i++) g = g + J.ubc * J.dxu;
-            X[5 + (n - 1) + ig] = g;
-        }
+        X[hi ? 5 + (n - 1) + ig : 5 - ig] = g;
     }
 }
 
@@ -627,8 +618,8 @@ template <bool RS, int DIR>
 __device__ __forceinline__ void job_substeps(double* S, const LineJob& J)
 {
     const int L = J.lpl;
-    const bool lane0 = J.lv && J.j == 0;
-    const bool lane1 = J.lv && J.j == 1;
+    const bool edge = J.lv && J.j < 2;      // lanes 0 and 1: cells 0 and n-1
+    const int ecell = J.j == 1 ? J.n - 1 : 0;
     const int nc = J.lv ? J.n - 1 : 0;
     // the lane's first cell in every buffer; loops advance them by L cells
     const double* const E0 = J.E + J.j;
@@ -662,12 +653,11 @@ __device__ __forceinline__ void job_substeps(double* S, const LineJob& J)
             for (int x = J.j; x < nc; x += L, e += L, c += L, f += L, u += L)
                 u[5] = e[5] - (c[1] * f[1] - c[0] * f[0]);
         }
-        if (lane0) J.UE[5] = cell_first3(J);
-        else if (lane1) J.UE[J.n + 4] = cell_last3(J);
+        if (edge) J.UE[ecell + 5] = edge_cell3(J);
         __syncwarp();
         if (J.lv) {
             if (J.j < 5) J.UE[J.j] = J.E[J.j];  // low ghosts: the pre-step ones of E
-            fill_ghosts3(J.UE, J.E, J, false, false);
+            fill_ghosts3(J.UE, J, false, false);
         }
         __syncwarp();
         // C: limited faces, in place (each lane reads only its own faces)
@@ -704,14 +694,10 @@ __device__ __forceinline__ void job_substeps(double* S, const LineJob& J)
                 else u[5] = v;
             }
         }
-        if (lane0) {
-            const double v = cell_first3(J);
-            if (last) store_plane(S, J, RS, 0, v);
-            else J.UE[5] = v;
-        } else if (lane1) {
-            const double v = cell_last3(J);
-            if (last) store_plane(S, J, RS, J.n - 1, v);
-            else J.UE[J.n + 4] = v;
+        if (edge) {
+            const double v = edge_cell3(J);
+            if (last) store_plane(S, J, RS, ecell, v);
+            else J.UE[ecell + 5] = v;
         }
         if (sub + 1 < J.nsmax) {
             __syncwarp();
@@ -723,7 +709,7 @@ __device__ __forceinline__ void job_substeps(double* S, const LineJob& J)
                 for (int x = J.j; x < ncf; x += L, u += L, e += L) e[5] = u[5];
             }
             __syncwarp();
-            if (J.lv) fill_ghosts3(J.E, J.E, J, true, false);
+            if (J.lv) fill_ghosts3(J.E, J, true, false);
             __syncwarp();
         }
     }
@@ -788,8 +774,10 @@ __device__ __forceinline__ void sweep_job(double* S, double* wb, const SweepCfg&
     }
     __syncwarp();
     if (J.lv) {
-        fill_ghosts3(J.E, J.E, J, true, true);
-        if (ut == VERB_BC_CONSTANT_VALUE && J.j >= 5 && J.j < 10) J.UE[n + J.j] = J.ubc;
+        fill_ghosts3(J.E, J, true, true);
+        if (ut == VERB_BC_CONSTANT_VALUE)
+            for (int gi = J.j; gi < 10; gi += L)
+                if (gi >= 5) J.UE[n + gi] = J.ubc;
     }
     cp_async_wait_all();
     __syncwarp();

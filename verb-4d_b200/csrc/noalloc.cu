@@ -14,7 +14,7 @@
 // Limits and sharing:
 //  * P_size * R_size must not exceed VERB_NOALLOC_MAX_POINTS (8192 points,
 //    5 doubles each: 320 KiB of scratch); larger slices are rejected with
-//    VERB_ERR_SIZE, and so are lines longer than the kernel's 256 points.
+//    VERB_ERR_SIZE, and so are lines longer than the kernel's 512 points.
 //  * Every GPU that loads the library holds the array until the process exits.
 //  * All calls share the one array and it keeps the last call's contents; the
 //    entry point clears the ticket and status words on each call.  Calls whose
