@@ -92,6 +92,18 @@ class ClockSampler:
                 "samples": len(rows), "reasons": reasons}
 
 
+FP64_OPS_PER_FACE = 179
+
+
+def fp64_peak_tops():
+    try:
+        with open(MEASURED) as f:
+            mhz = float(json.load(f)["sm_max_mhz"])
+    except (OSError, KeyError, ValueError):
+        mhz = 1965.0
+    return round(148 * 64 * mhz * 1e6 / 1e12, 2)
+
+
 def measured_peaks():
     try:
         with open(MEASURED) as f:
@@ -174,6 +186,7 @@ def run_ours(args):
     tm = ctx.timing()
     neg = ctx.negative_count()
     dev_bytes = ctx.device_bytes()
+    conv_substeps = int(ctx.convection_substeps().astype(np.int64).sum())
     ctx.close()
     del solver, ctx
     if world > 1:
@@ -234,6 +247,16 @@ def run_ours(args):
     hbm_peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (solve_ms / 1e3) / 1e9
     conv_ms = tm["convection_ms"] / args.steps
+    # FP64 roofline of convection: the reference's arithmetic per face update
+    # (9th-order face 136 ops, limiter 35 incl. comparisons, two cell updates
+    # 8) over the faces one outer sub-step sweeps, times the slice sub-steps of
+    # the last timed step; peak = FP64 issue rate (64 lanes/SM/clock) at the
+    # maximum SM clock
+    p_faces = (R - 1) * (P if wl.bc_types["Pl"] == W.BC_PERIODIC else P - 1)
+    r_faces = P * (R if wl.bc_types["Rl"] == W.BC_PERIODIC else R - 1)
+    conv_ops = FP64_OPS_PER_FACE * (p_faces + r_faces) * conv_substeps
+    fp64_peak = fp64_peak_tops()
+    conv_tops = conv_ops / (conv_ms / 1e3) / 1e12
     out = {
         "metric": METRIC if args.config == "cfg2" else "sim-hours/s at 25x31x31x24",
         "value": round(value, 5), "unit": "sim-hours/s", "n_gpus": world, "steps": args.steps,
@@ -259,6 +282,13 @@ def run_ours(args):
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                      "algorithmic_bytes_per_launch": int(alg_bytes),
                      "traffic": args.traffic},
+        "roofline_fp64": {"kernel": "convection_kernel (ULTIMATE-QUICKEST sweeps, FP64 vector)",
+                          "bound": "fp64", "achieved": round(conv_tops, 3), "peak": fp64_peak,
+                          "unit": "TOP/s", "frac": round(conv_tops / fp64_peak, 4),
+                          "peak_source": "nominal FP64 issue rate, 148 SMs x 64 lanes at "
+                                         "MEASURED_PEAKS.json sm_max_mhz",
+                          "fp64_ops_per_face": FP64_OPS_PER_FACE,
+                          "face_updates_per_step": int((p_faces + r_faces) * conv_substeps)},
         "clocks": clk.summary(),
         "gpu_launches": int(tm["kernel_launches"]),
         "negative_points_end": int(neg),
