@@ -399,6 +399,14 @@ __device__ __forceinline__ double div_const(double a, double b, double y)
     return r == 0.0 ? q : __fma_rn(r, y, q);
 }
 
+// The same for a dividend that is never -0 (then a zero residual needs no
+// special case: q + 0*y = q for every q but -0).
+__device__ __forceinline__ double div_const_nz(double a, double b, double y)
+{
+    const double q = __dmul_rn(a, y);
+    return __fma_rn(__fma_rn(-q, b, a), y, q);
+}
+
 // Courant factors of the face polynomial (QUICKEST6.cpp:209-238), the same
 // expressions as face_coef().
 __device__ __forceinline__ FaceCoef face_coef_exact(double cr)
@@ -409,11 +417,13 @@ __device__ __forceinline__ FaceCoef face_coef_exact(double cr)
     const double p2 = t1 * (cs - 4);
     const double p3 = p2 * (cs - 9);
     const double p4 = p3 * (cs - 16);
+    // t1 = cs - 1 and ca = |cr| are never -0, nor is p3 = p2*(cs-9) (p2 = -0
+    // only when cs = 1, and then p3 = +0); p2 and p4 are -0 when |cr| = 1
     FaceCoef k;
-    k.k3 = div_const(t1, 6.0, 1.0 / 6.0);
-    k.c6 = div_const(ca, 6.0, 1.0 / 6.0);
+    k.k3 = div_const_nz(t1, 6.0, 1.0 / 6.0);
+    k.c6 = div_const_nz(ca, 6.0, 1.0 / 6.0);
     k.k5 = div_const(p2, 120.0, 1.0 / 120.0);
-    k.k7 = div_const(p3, 5040.0, 1.0 / 5040.0);
+    k.k7 = div_const_nz(p3, 5040.0, 1.0 / 5040.0);
     k.k9 = div_const(p4, 362880.0, 1.0 / 362880.0);
     return k;
 }
