@@ -143,26 +143,35 @@ def run_ours(args):
                for h, (vp, vr) in vel_host.items()}
     torch.cuda.synchronize(dev)
 
-    solver = Solver(wl, stream=stream.cuda_stream, velocity_provider=None)
+    def make_solver(form):
+        sv = Solver(wl, stream=stream.cuda_stream, velocity_provider=None)
+        sv.load()
+        sv.ctx.set_local_precision(form, args.refine if form == "mixed" else 0)
+        return sv
+
+    solver = make_solver(args.form)
     ctx = solver.ctx
-    solver.load()
     lib = ctx.lib
 
-    def update_dev(it):
+    def update_dev(it, sv=None):
+        sv = sv or solver
         h = min(int(np.floor(it * wl.dt * 24 + 1e-9)), len(kp) - 1)
-        if h != solver.hour:
-            solver.hour = h
-            ctx.set_scale("DLL", wl.dll_scale(h))
+        if h != sv.hour:
+            sv.hour = h
+            sv.ctx.set_scale("DLL", wl.dll_scale(h))
             vp, vr = vel_dev[h]
-            lib.verb_upload_field_device(ctx.h, 10, vp.data_ptr())
-            lib.verb_upload_field_device(ctx.h, 11, vr.data_ptr())
+            lib.verb_upload_field_device(sv.ctx.h, 10, vp.data_ptr())
+            lib.verb_upload_field_device(sv.ctx.h, 11, vr.data_ptr())
 
     fl = wl.flags
     t_w0 = time.perf_counter()
     ctx.set_timing(True)
+    psd_step1 = None
     for it in range(1, args.warmup + 1):
         update_dev(it)
         ctx.step(wl.dt, wl.sub_dt, fl["run_convection"], fl["run_radial"], fl["run_local"])
+        if it == 1 and args.form == "mixed":
+            psd_step1 = ctx.download()  # one step from the initial state (untimed)
     ctx.sync()
     warm = ctx.timing()
     warm_s = time.perf_counter() - t_w0
@@ -187,8 +196,59 @@ def run_ours(args):
     neg = ctx.negative_count()
     dev_bytes = ctx.device_bytes()
     conv_substeps = int(ctx.convection_substeps().astype(np.int64).sum())
-    ctx.close()
-    del solver, ctx
+    form_info = None
+    if args.form == "mixed":
+        # the same steps in the FP64 form, for the error of the mixed form and
+        # the FP64 time on the same box
+        psd_mixed = ctx.download()
+        corr = ctx.local_refinement()
+        ctx.close()
+        del solver, ctx
+        sv = make_solver("fp64")
+        for it in range(1, args.warmup + 1):
+            update_dev(it, sv)
+            sv.ctx.step(wl.dt, wl.sub_dt, fl["run_convection"], fl["run_radial"], fl["run_local"])
+            if it == 1:
+                p64 = sv.ctx.download()
+                err1 = float(np.abs(psd_step1 - p64).max() / np.abs(p64).max())
+        sv.ctx.sync()
+        sv.ctx.set_timing(True)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for it in range(args.warmup + 1, args.warmup + args.steps + 1):
+            update_dev(it, sv)
+            sv.ctx.step(wl.dt, wl.sub_dt, fl["run_convection"], fl["run_radial"], fl["run_local"])
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        tm64 = sv.ctx.timing()
+        psd64 = sv.ctx.download()
+        sv.ctx.close()
+        del sv
+        # one step with FP64 factors and 3 FP64 refinement steps: the FP64 path
+        # itself is only accurate to ~kappa*eps64 on these stiff systems
+        sv = Solver(wl, stream=stream.cuda_stream, velocity_provider=None)
+        sv.load()
+        sv.ctx.set_local_precision("fp64", 3)
+        update_dev(1, sv)
+        sv.ctx.step(wl.dt, wl.sub_dt, fl["run_convection"], fl["run_radial"], fl["run_local"])
+        p64r = sv.ctx.download()
+        sv.ctx.close()
+        del sv
+        rel = lambda a, b: float(np.abs(a - b).max() / np.abs(b).max())  # noqa: E731
+        err = float(np.abs(psd_mixed - psd64).max() / np.abs(psd64).max())
+        form_info = {"form": "mixed", "refinements": args.refine,
+                     "max_rel_err_one_step": err1, "tolerance": 1e-8,
+                     "max_rel_err_one_step_vs_fp64_refined": rel(psd_step1, p64r),
+                     "fp64_vs_fp64_refined_one_step": rel(p64, p64r),
+                     "max_rel_err_after_run": err,
+                     "last_relative_correction": corr,
+                     "fp64_ms_per_step": round(e0.elapsed_time(e1) / args.steps, 3),
+                     "fp64_local_solve_ms_per_step": round(tm64["local_solve_ms"] / args.steps, 3),
+                     "err_measured_after_steps": args.warmup + args.steps}
+    else:
+        ctx.close()
+        del solver, ctx
     if world > 1:
         t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -213,6 +273,7 @@ def run_ours(args):
         t0 = time.perf_counter()
         s2 = Solver(wl, stream=stream.cuda_stream, velocity_provider=host_provider)
         s2.load()
+        s2.ctx.set_local_precision(args.form, args.refine if args.form == "mixed" else 0)
         h2d = sum(np.asarray(v).nbytes for k, v in wl.fields.items() if k != "DLL")
         d2h = 0
         for it in range(1, args.steps + 1):
@@ -242,7 +303,8 @@ def run_ours(args):
     n = V * K
     kl, kv = V + 1, 2 * (V + 1)
     nsys = P * R
-    alg_bytes = nsys * (n * (kl + kv + 1) * 8 + n * 4 + 2 * n * 8)  # LAPACK band factors + pivots + rhs/x
+    fbytes = 4 if args.form == "mixed" else 8  # factor storage
+    alg_bytes = nsys * (n * (kl + kv + 1) * fbytes + n * 4 + 2 * n * 8)  # band factors + pivots + rhs/x
     solve_ms = tm["local_solve_ms"] / max(tm["local_solve_launches"], 1)
     hbm_peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (solve_ms / 1e3) / 1e9
@@ -261,7 +323,9 @@ def run_ours(args):
         "metric": METRIC if args.config == "cfg2" else "sim-hours/s at 25x31x31x24",
         "value": round(value, 5), "unit": "sim-hours/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.form == "fp64" else "f64 (local LU factors stored f32)",
+        "data": "synthetic (seeded)",
         "config": {"workload": f"VERB-4D operator-split step {args.config} "
                                f"(P,R,V,K)={spec.shape}, dt=5 min, hourly Kp in [1,6]",
                    "P_mlt": P, "R_L": R, "V_energy": V, "K_alpha": K, "dt_min": 5,
@@ -296,6 +360,8 @@ def run_ours(args):
     }
     if e2e:
         out["e2e"] = e2e
+    if form_info:
+        out["form"] = form_info
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         cb = reference_estimate(wl, budget_s=args.cpu_budget)
         out["cpu_baseline"] = {"value": round(cb["value"], 8), "unit": "sim-hours/s",
@@ -460,6 +526,9 @@ def main():
     ap.add_argument("--config", default="cfg2", choices=["cfg2", "cfg1", "cfg2s", "cfg2m"])
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"],
+                    help="local solve: FP64 factors, or FP32 factors with FP64 refinement")
+    ap.add_argument("--refine", type=int, default=2, help="refinement steps of the mixed form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--traffic", type=float, default=None,

@@ -110,6 +110,23 @@ int verb_set_options(verb_ctx* ctx, int radial_sources, int local_sources, int i
                      int positive_psd);
 /* Force the local LU factors to be recomputed at the next verb_local(). */
 int verb_invalidate_lu(verb_ctx* ctx);
+/* Precision of the local (V,K) solve.  VERB_PREC_FP64 (default): the LU
+ * factors are kept in FP64, as LAPACK's dgbtrf leaves them
+ * (src/MatrixSolver.cpp:223-340, cached as in src/VERB4D_Solver.cpp:340-365).
+ * VERB_PREC_MIXED: the same factorisation (FP64 arithmetic, the same pivots)
+ * is stored in FP32, which halves the factor cache and the bytes every solve
+ * streams.  With refinements > 0 (either form) each solve is followed by that
+ * many steps of FP64 iterative refinement: r = b - A x with A assembled in
+ * FP64, A d = r with the cached factors, x += d.  FP64 with 0 refinements is
+ * the reference's arithmetic; every other setting has no counterpart in the
+ * reference.  Changing the form frees the other form's factors and refactors
+ * at the next verb_local(). */
+#define VERB_PREC_FP64 0
+#define VERB_PREC_MIXED 1
+int verb_set_local_precision(verb_ctx* ctx, int mode, int refinements);
+/* max |d| / max |x| of the last refinement step of the last verb_local()
+ * (0 without refinement). */
+int verb_local_refinement(verb_ctx* ctx, double* rel_correction);
 int verb_download_psd(verb_ctx* ctx, double* host);
 int verb_download_field(verb_ctx* ctx, int field, double* host);
 /* Device pointer of a field (for zero-copy use from the caller's CUDA code). */
@@ -145,6 +162,7 @@ int verb_convection_substeps(verb_ctx* ctx, int* host_vk);
  * them) for parity checks and LU-cache hand-off. */
 int verb_local_pivots(verb_ctx* ctx, int32_t* host);
 int verb_local_factor_lapack(verb_ctx* ctx, int p, int r, double* ab_host, long* ipiv1_host);
+/* (FP64 form only: VERB_ERR_ARG when the factors are held in FP32.) */
 
 /* ---- radial Kalman filter ------------------------------------------------ */
 /* One assimilation update of every (P,V,K) radial column (the reference

@@ -42,6 +42,12 @@ struct verb_ctx {
     double *Lf = nullptr, *Uf = nullptr, *lwork = nullptr;
     int32_t* ipiv = nullptr;
     int kl = 0, kv = 0, klp = 0, kvp = 0;
+    // mixed-precision form: FP32 factors, FP64 refinement (rhs copy, residual)
+    int local_prec = VERB_PREC_FP64, refine_iters = 0;
+    float *Lf32 = nullptr, *Uf32 = nullptr;
+    int klp32 = 0, kvp32 = 0;
+    double *lrhs = nullptr, *lres = nullptr;
+    unsigned long long* refine_red = nullptr;  // max |last correction|, max |x|
     bool local_dirty = true;
     double local_dt = -1;
     const double* dkv_override = nullptr;  // Dyx for the per-slice entry point
@@ -264,9 +270,21 @@ int local_prepare(verb_ctx* c, LocalArgs& a, double dts)
     c->kv = 2 * c->kl;
     c->klp = (c->kl + 1) & ~1;
     c->kvp = (c->kv + 2) & ~1;
+    c->klp32 = (c->kl + 3) & ~3;  // 16-byte columns for cp.async
+    c->kvp32 = (c->kv + 4) & ~3;
     const size_t nsys = (size_t)d.P * d.R, n = (size_t)d.V * d.K;
-    CK(alloc((void**)&c->Lf, nsys * n * c->klp * sizeof(double)));
-    CK(alloc((void**)&c->Uf, nsys * n * c->kvp * sizeof(double)));
+    if (c->refine_iters > 0) {
+        CK(alloc((void**)&c->lrhs, nsys * n * sizeof(double)));
+        CK(alloc((void**)&c->lres, nsys * n * sizeof(double)));
+        CK(alloc((void**)&c->refine_red, 2 * sizeof(unsigned long long)));
+    }
+    if (c->local_prec == VERB_PREC_MIXED) {
+        CK(alloc((void**)&c->Lf32, nsys * n * c->klp32 * sizeof(float)));
+        CK(alloc((void**)&c->Uf32, nsys * n * c->kvp32 * sizeof(float)));
+    } else {
+        CK(alloc((void**)&c->Lf, nsys * n * c->klp * sizeof(double)));
+        CK(alloc((void**)&c->Uf, nsys * n * c->kvp * sizeof(double)));
+    }
     CK(alloc((void**)&c->ipiv, nsys * n * sizeof(int32_t)));
     CK(alloc((void**)&c->lwork, nsys * n * sizeof(double)));
     a.d = d;
@@ -297,6 +315,11 @@ int local_prepare(verb_ctx* c, LocalArgs& a, double dts)
     a.kvp = c->kvp;
     a.Lf = c->Lf;
     a.Uf = c->Uf;
+    a.factors32 = c->local_prec == VERB_PREC_MIXED;
+    a.klp32 = c->klp32;
+    a.kvp32 = c->kvp32;
+    a.Lf32 = c->Lf32;
+    a.Uf32 = c->Uf32;
     a.ipiv = c->ipiv;
     a.work = c->lwork;
     a.status = c->status;
@@ -307,7 +330,10 @@ int local_factor(verb_ctx* c, LocalArgs& a)
 {
     PhaseTimer t(c, PH_LOCF);
     const size_t nsys = (size_t)c->d.P * c->d.R, n = (size_t)c->d.V * c->d.K;
-    CK(cudaMemsetAsync(c->Uf, 0, nsys * n * c->kvp * sizeof(double), c->stream));
+    if (a.factors32)
+        CK(cudaMemsetAsync(c->Uf32, 0, nsys * n * c->kvp32 * sizeof(float), c->stream));
+    else
+        CK(cudaMemsetAsync(c->Uf, 0, nsys * n * c->kvp * sizeof(double), c->stream));
     launch_local_factor(a, c->stream);
     c->acc.kernel_launches++;
     c->local_dirty = false;
@@ -331,15 +357,37 @@ int local_run(verb_ctx* c, double dt, double sub_dt)
         s = local_factor(c, a);
         if (s) return s;
     }
+    const bool refine = c->refine_iters > 0;
+    const size_t nall = (size_t)d.P * d.R * d.V * d.K;
     for (int k = 0; k < nsub; k++) {
         launch_local_rhs(a, k > 0, c->stream);
         c->acc.kernel_launches++;
+        if (refine) CK(cudaMemcpyAsync(c->lrhs, c->lwork, nall * sizeof(double),
+                                       cudaMemcpyDeviceToDevice, c->stream));
         {
             PhaseTimer ts(c, PH_LOCS);
             launch_local_solve(a, c->stream);
             c->acc.kernel_launches++;
         }
         c->acc.local_solve_launches++;
+        if (refine) {
+            // iterative refinement in FP64: r = b - A x, A d = r with the
+            // cached factors (FP32 in the mixed form), x += d
+            LocalArgs ar = a;
+            ar.work = c->lres;
+            for (int it = 0; it < c->refine_iters; it++) {
+                launch_local_residual(a, c->lrhs, c->lwork, c->lres, c->stream);
+                {
+                    PhaseTimer ts(c, PH_LOCS);
+                    launch_local_solve(ar, c->stream);
+                }
+                if (it == c->refine_iters - 1)
+                    CK(cudaMemsetAsync(c->refine_red, 0, 2 * sizeof(unsigned long long), c->stream));
+                launch_local_update(a, c->lwork, c->lres, c->refine_red, c->stream);
+                c->acc.kernel_launches += 3;
+                c->acc.local_solve_launches++;
+            }
+        }
     }
     launch_local_store(a, c->stream);
     c->acc.kernel_launches++;
@@ -504,6 +552,9 @@ int verb_destroy(verb_ctx* c)
         cudaFree(c->fbase[i]);
     }
     for (int i = 0; i < VERB_BCF_COUNT; i++) cudaFree(c->bc[i]);
+    for (void* p : {(void*)c->Lf32, (void*)c->Uf32, (void*)c->lrhs, (void*)c->lres,
+                    (void*)c->refine_red})
+        cudaFree(p);
     for (void* p : {(void*)c->rfa, (void*)c->rfbet, (void*)c->rfgam, (void*)c->Lf, (void*)c->Uf,
                     (void*)c->lwork, (void*)c->ipiv, (void*)c->conv_scratch,
                     (void*)c->conv_substeps, (void*)c->ticket, (void*)c->red, (void*)c->status,
@@ -529,10 +580,11 @@ int verb_device_bytes(const verb_ctx* c, size_t* bytes)
     for (int i = 0; i < VERB_BCF_COUNT; i++)
         if (c->bc[i]) b += bc_elems(c, i) * sizeof(double);
     if (c->rfa) b += 3 * F;
-    if (c->Lf) {
-        const size_t ns = (size_t)c->d.P * c->d.R * c->d.V * c->d.K;
-        b += ns * (c->klp + c->kvp + 1) * sizeof(double) + ns * sizeof(int32_t);
-    }
+    const size_t ns = (size_t)c->d.P * c->d.R * c->d.V * c->d.K;
+    if (c->Lf) b += ns * (c->klp + c->kvp) * sizeof(double);
+    if (c->Lf32) b += ns * (c->klp32 + c->kvp32) * sizeof(float);
+    if (c->ipiv) b += ns * (sizeof(double) + sizeof(int32_t));  // work vector and pivots
+    if (c->lrhs) b += 2 * ns * sizeof(double);
     *bytes = b;
     return VERB_OK;
 }
@@ -626,6 +678,46 @@ int verb_set_options(verb_ctx* c, int radial_sources, int local_sources, int inc
     if ((include_boundary != 0) != (c->include_boundary != 0)) c->local_dirty = true;
     c->include_boundary = include_boundary;
     c->positive_psd = positive_psd;
+    return VERB_OK;
+}
+
+int verb_set_local_precision(verb_ctx* c, int mode, int refinements)
+{
+    if (!c || (mode != VERB_PREC_FP64 && mode != VERB_PREC_MIXED) || refinements < 0 ||
+        refinements > 16)
+        return VERB_ERR_ARG;
+    if (mode != c->local_prec) {
+        // release the other form's factors before the next factorisation
+        // allocates this one's
+        CK(cudaStreamSynchronize(c->stream));
+        if (mode == VERB_PREC_MIXED) {
+            cudaFree(c->Lf);
+            cudaFree(c->Uf);
+            c->Lf = c->Uf = nullptr;
+        } else {
+            cudaFree(c->Lf32);
+            cudaFree(c->Uf32);
+            c->Lf32 = c->Uf32 = nullptr;
+        }
+        c->local_prec = mode;
+        c->local_dirty = true;
+    }
+    c->refine_iters = refinements;
+    return VERB_OK;
+}
+
+int verb_local_refinement(verb_ctx* c, double* rel_correction)
+{
+    if (!c || !rel_correction) return VERB_ERR_ARG;
+    if (!c->refine_red || c->refine_iters == 0) {
+        *rel_correction = 0.0;
+        return VERB_OK;
+    }
+    unsigned long long k[2];
+    CK(cudaMemcpyAsync(k, c->refine_red, sizeof(k), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const double md = dkey_inv(k[0]), mx = dkey_inv(k[1]);
+    *rel_correction = mx > 0 ? md / mx : md;
     return VERB_OK;
 }
 

@@ -163,6 +163,10 @@ __device__ __forceinline__ bool skip_system(const LocalArgs& a, int sys)
 constexpr int FACT_THREADS = 512;
 constexpr int STAGE_ROWS = 128;
 
+// The factorisation always runs in FP64 (pivots and multipliers as LAPACK's);
+// T is the storage type of the factors: double, or float for the
+// mixed-precision form, whose solves are refined in FP64.
+template <typename T>
 __global__ void __launch_bounds__(FACT_THREADS) local_factor_kernel(LocalArgs a)
 {
     extern __shared__ double sm[];
@@ -181,8 +185,10 @@ __global__ void __launch_bounds__(FACT_THREADS) local_factor_kernel(LocalArgs a)
     __shared__ double s_piv;
     const SysView v = sys_view(a, sys);
     int types[4] = {a.Vl_t, a.Vu_t, a.Kl_t, a.Ku_t};
-    double* Lf = a.Lf + (size_t)sys * n * a.klp;
-    double* Uf = a.Uf + (size_t)sys * n * a.kvp;
+    const bool f32 = sizeof(T) == sizeof(float);
+    const int klp = f32 ? a.klp32 : a.klp, kvp = f32 ? a.kvp32 : a.kvp;
+    T* Lf = (f32 ? (T*)a.Lf32 : (T*)a.Lf) + (size_t)sys * n * klp;
+    T* Uf = (f32 ? (T*)a.Uf32 : (T*)a.Uf) + (size_t)sys * n * kvp;
     int32_t* ip = a.ipiv + (size_t)sys * n;
     const int tid = threadIdx.x;
 
@@ -258,7 +264,7 @@ __global__ void __launch_bounds__(FACT_THREADS) local_factor_kernel(LocalArgs a)
                 const double val = (i == jp) ? colj[0] : colj[i];
                 const double m = val * rcp;
                 mult[i] = m;
-                Lf[(size_t)j * a.klp + (i - 1)] = m;
+                Lf[(size_t)j * klp + (i - 1)] = (T)m;
             }
             if (jp != 0) {
                 const int rp = (j + jp) % RW;
@@ -271,12 +277,12 @@ __global__ void __launch_bounds__(FACT_THREADS) local_factor_kernel(LocalArgs a)
             }
         } else {
             set_error(a.status, VERB_ERR_PIVOT);
-            for (int i = 1 + tid; i <= km; i += blockDim.x) Lf[(size_t)j * a.klp + (i - 1)] = colj[i];
+            for (int i = 1 + tid; i <= km; i += blockDim.x) Lf[(size_t)j * klp + (i - 1)] = (T)colj[i];
         }
         __syncthreads();
         // [C] U row j out; rank-1 update of rows j+1..j+km, columns j+1..ju
         for (int c = j + tid; c <= ju && c <= j + kv; c += blockDim.x)
-            Uf[(size_t)c * a.kvp + (kv - (c - j))] = W[rsj * CW + (c % CW)];
+            Uf[(size_t)c * kvp + (kv - (c - j))] = (T)W[rsj * CW + (c % CW)];
         if (nz && km > 0 && ju > j) {
             const int ncol = ju - j;
             const int cg = tid & 127;        // column lane
@@ -417,11 +423,16 @@ constexpr int BWD_DEPTH = 2;   // U columns in flight per warp
 constexpr int FWD_WIN = 128;   // >= kl + 1
 constexpr int BWD_WIN = 256;   // >= kv + 1
 
-__host__ __device__ constexpr size_t solve_ring_doubles(int klp, int kvp)
+// ring of factor columns per warp, in doubles (16-byte multiples)
+__host__ __device__ constexpr size_t solve_ring_doubles(int klp, int kvp, int esize)
 {
-    return (size_t)(FWD_DEPTH * klp > BWD_DEPTH * kvp ? FWD_DEPTH * klp : BWD_DEPTH * kvp);
+    return ((size_t)(FWD_DEPTH * klp > BWD_DEPTH * kvp ? FWD_DEPTH * klp : BWD_DEPTH * kvp) * esize +
+            15) / 16 * 2;
 }
 
+// T: storage type of the factors.  The substitutions run in FP64 either way
+// (float factors are widened as they are used).
+template <typename T>
 __global__ void __launch_bounds__(SOLVE_WARPS * 32) local_solve_kernel(LocalArgs a, int nsys)
 {
     extern __shared__ double sm[];
@@ -429,22 +440,24 @@ __global__ void __launch_bounds__(SOLVE_WARPS * 32) local_solve_kernel(LocalArgs
     const int sys = blockIdx.x * SOLVE_WARPS + warp;
     if (sys >= nsys || skip_system(a, sys)) return;
     const int n = a.d.V * a.d.K;
-    const int kl = a.kl, kv = a.kv, klp = a.klp, kvp = a.kvp;
-    const size_t per_warp = BWD_WIN + solve_ring_doubles(klp, kvp);
+    const bool f32 = sizeof(T) == sizeof(float);
+    const int kl = a.kl, kv = a.kv, klp = f32 ? a.klp32 : a.klp, kvp = f32 ? a.kvp32 : a.kvp;
+    constexpr int VEC = 16 / sizeof(T);  // elements per 16-byte cp.async
+    const size_t per_warp = BWD_WIN + solve_ring_doubles(klp, kvp, sizeof(T));
     double* win = sm + (size_t)warp * per_warp;
-    double* ring = win + BWD_WIN;
+    T* ring = (T*)(win + BWD_WIN);
     double* w = a.work + (size_t)sys * n;
-    const double* Lf = a.Lf + (size_t)sys * n * klp;
-    const double* Uf = a.Uf + (size_t)sys * n * kvp;
+    const T* Lf = (f32 ? (const T*)a.Lf32 : (const T*)a.Lf) + (size_t)sys * n * klp;
+    const T* Uf = (f32 ? (const T*)a.Uf32 : (const T*)a.Uf) + (size_t)sys * n * kvp;
     const int32_t* ip = a.ipiv + (size_t)sys * n;
 
     // ---------------- forward: L with interleaved row interchanges (xGBTRS) --------
     for (int i = lane; i < FWD_WIN && i < n; i += 32) win[i] = w[i];
     auto issue_L = [&](int col) {
         if (col < n - 1) {
-            double* dst = ring + (col % FWD_DEPTH) * klp;
-            const double* src = Lf + (size_t)col * klp;
-            for (int c = lane; c < klp / 2; c += 32) cp_async16(dst + 2 * c, src + 2 * c);
+            T* dst = ring + (col % FWD_DEPTH) * klp;
+            const T* src = Lf + (size_t)col * klp;
+            for (int c = lane; c < klp / VEC; c += 32) cp_async16(dst + VEC * c, src + VEC * c);
         }
     };
     for (int c = 0; c < FWD_DEPTH; c++) {
@@ -467,7 +480,7 @@ __global__ void __launch_bounds__(SOLVE_WARPS * 32) local_solve_kernel(LocalArgs
         const double bj_old = win[j & (FWD_WIN - 1)];
         const double bl = win[l & (FWD_WIN - 1)];
         const double bj = (l != j) ? bl : bj_old;
-        const double* Lc = ring + (j % FWD_DEPTH) * klp;
+        const T* Lc = ring + (j % FWD_DEPTH) * klp;
         const double tmp = -bj;
         const bool upd = bj != 0.0;
 #pragma unroll
@@ -476,7 +489,7 @@ __global__ void __launch_bounds__(SOLVE_WARPS * 32) local_solve_kernel(LocalArgs
             const int i = j + 1 + t;
             if (t < lm) {
                 double cur = (i == l) ? bj_old : win[i & (FWD_WIN - 1)];
-                if (upd) cur = cur + Lc[t] * tmp;  // xGER in xGBTRS
+                if (upd) cur = cur + (double)Lc[t] * tmp;  // xGER in xGBTRS
                 win[i & (FWD_WIN - 1)] = cur;
             }
         }
@@ -497,9 +510,9 @@ __global__ void __launch_bounds__(SOLVE_WARPS * 32) local_solve_kernel(LocalArgs
     for (int i = n - 1 - lane; i >= 0 && i > n - 1 - BWD_WIN; i -= 32) win[i & (BWD_WIN - 1)] = w[i];
     auto issue_U = [&](int col) {
         if (col >= 0) {
-            double* dst = ring + ((n - 1 - col) % BWD_DEPTH) * kvp;
-            const double* src = Uf + (size_t)col * kvp;
-            for (int c = lane; c < kvp / 2; c += 32) cp_async16(dst + 2 * c, src + 2 * c);
+            T* dst = ring + ((n - 1 - col) % BWD_DEPTH) * kvp;
+            const T* src = Uf + (size_t)col * kvp;
+            for (int c = lane; c < kvp / VEC; c += 32) cp_async16(dst + VEC * c, src + VEC * c);
         }
     };
     for (int c = 0; c < BWD_DEPTH; c++) {
@@ -510,17 +523,17 @@ __global__ void __launch_bounds__(SOLVE_WARPS * 32) local_solve_kernel(LocalArgs
     for (int j = n - 1; j >= 0; j--) {
         cp_wait<BWD_DEPTH - 1>();
         __syncwarp();
-        const double* Uc = ring + ((n - 1 - j) % BWD_DEPTH) * kvp;
+        const T* Uc = ring + ((n - 1 - j) % BWD_DEPTH) * kvp;
         double bj = win[j & (BWD_WIN - 1)];
         if (bj != 0.0) {
-            bj = bj / Uc[kv];
+            bj = bj / (double)Uc[kv];
 #pragma unroll
             for (int k = 0; k < 7; k++) {
                 const int d = 1 + lane + 32 * k;
                 const int i = j - d;
                 if (d <= kv && i >= 0) {
                     double* x = &win[i & (BWD_WIN - 1)];
-                    *x = *x - bj * Uc[kv - d];  // xTBSV: X(I) - TEMP*A(L+I,J)
+                    *x = *x - bj * (double)Uc[kv - d];  // xTBSV: X(I) - TEMP*A(L+I,J)
                 }
             }
         }
@@ -535,7 +548,78 @@ __global__ void __launch_bounds__(SOLVE_WARPS * 32) local_solve_kernel(LocalArgs
     cp_wait<0>();
 }
 
+// r = b - A x per unknown (refinement of the mixed-precision form).  A's row
+// comes from assemble_row, so it is the matrix the factorisation saw; the
+// 9-point product is summed in FP64.
+__global__ void local_residual_kernel(LocalArgs a, const double* b, const double* x, double* r)
+{
+    const int sys = blockIdx.y;
+    if (skip_system(a, sys)) return;
+    const int nx = a.d.V;
+    const int n = a.d.V * a.d.K;
+    const SysView v = sys_view(a, sys);
+    int types[4] = {a.Vl_t, a.Vu_t, a.Kl_t, a.Ku_t};
+    const size_t base = (size_t)sys * n;
+    for (int in = blockIdx.x * blockDim.x + threadIdx.x; in < n; in += gridDim.x * blockDim.x) {
+        double row[9];
+        const int st = assemble_row(v, types, a.dt, in, row);
+        if (st) set_error(a.status, st);
+        double acc = b[base + in];
+#pragma unroll
+        for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+            for (int dx = -1; dx <= 1; dx++) {
+                const double m = row[dslot(dx, dy)];
+                const int col = in + dy * nx + dx;
+                if (m != 0.0 && col >= 0 && col < n) acc -= m * x[base + col];
+            }
+        r[base + in] = acc;
+    }
+}
+
+// x += d over all systems; red[0] = max |d|, red[1] = max |x| as dkey values.
+__global__ void local_update_kernel(LocalArgs a, double* x, const double* d, size_t total,
+                                    unsigned long long* red)
+{
+    const size_t n = (size_t)a.d.V * a.d.K;
+    double md = 0.0, mx = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (size_t)gridDim.x * blockDim.x) {
+        if (skip_system(a, (int)(i / n))) continue;
+        const double v = x[i] + d[i];
+        x[i] = v;
+        md = fmax(md, fabs(d[i]));
+        mx = fmax(mx, fabs(v));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        md = fmax(md, __shfl_xor_sync(0xffffffffu, md, o));
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&red[0], dkey(md));
+        atomicMax(&red[1], dkey(mx));
+    }
+}
+
 }  // namespace
+
+void launch_local_residual(const LocalArgs& a, const double* b, const double* x, double* r,
+                           cudaStream_t s)
+{
+    const int n = a.d.V * a.d.K;
+    dim3 grid((n + 255) / 256, a.d.P * a.d.R);
+    local_residual_kernel<<<grid, 256, 0, s>>>(a, b, x, r);
+}
+
+void launch_local_update(const LocalArgs& a, double* x, const double* d, unsigned long long* red,
+                         cudaStream_t s)
+{
+    const size_t total = (size_t)a.d.P * a.d.R * a.d.V * a.d.K;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    local_update_kernel<<<sms * 8, 256, 0, s>>>(a, x, d, total, red);
+}
 
 size_t local_factor_smem(int V)
 {
@@ -546,8 +630,15 @@ size_t local_factor_smem(int V)
 void launch_local_factor(const LocalArgs& a, cudaStream_t s)
 {
     const size_t smem = local_factor_smem(a.d.V);
-    cudaFuncSetAttribute(local_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    local_factor_kernel<<<a.d.P * a.d.R, FACT_THREADS, smem, s>>>(a);
+    if (a.factors32) {
+        cudaFuncSetAttribute(local_factor_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        local_factor_kernel<float><<<a.d.P * a.d.R, FACT_THREADS, smem, s>>>(a);
+    } else {
+        cudaFuncSetAttribute(local_factor_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        local_factor_kernel<double><<<a.d.P * a.d.R, FACT_THREADS, smem, s>>>(a);
+    }
 }
 
 void launch_local_rhs(const LocalArgs& a, bool from_work, cudaStream_t s)
@@ -565,10 +656,22 @@ void launch_local_store(const LocalArgs& a, cudaStream_t s)
 void launch_local_solve(const LocalArgs& a, cudaStream_t s)
 {
     const int nsys = a.d.P * a.d.R;
-    const size_t smem =
-        (size_t)SOLVE_WARPS * (BWD_WIN + solve_ring_doubles(a.klp, a.kvp)) * sizeof(double);
-    cudaFuncSetAttribute(local_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    local_solve_kernel<<<(nsys + SOLVE_WARPS - 1) / SOLVE_WARPS, SOLVE_WARPS * 32, smem, s>>>(a, nsys);
+    const int grid = (nsys + SOLVE_WARPS - 1) / SOLVE_WARPS;
+    if (a.factors32) {
+        const size_t smem = (size_t)SOLVE_WARPS *
+                            (BWD_WIN + solve_ring_doubles(a.klp32, a.kvp32, sizeof(float))) *
+                            sizeof(double);
+        cudaFuncSetAttribute(local_solve_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        local_solve_kernel<float><<<grid, SOLVE_WARPS * 32, smem, s>>>(a, nsys);
+    } else {
+        const size_t smem = (size_t)SOLVE_WARPS *
+                            (BWD_WIN + solve_ring_doubles(a.klp, a.kvp, sizeof(double))) *
+                            sizeof(double);
+        cudaFuncSetAttribute(local_solve_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        local_solve_kernel<double><<<grid, SOLVE_WARPS * 32, smem, s>>>(a, nsys);
+    }
 }
 
 }  // namespace verb

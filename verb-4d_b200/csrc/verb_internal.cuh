@@ -76,6 +76,11 @@ struct LocalArgs {
     int kl, kv, klp, kvp;  // band sizes and padded column strides
     double* Lf;         // [sys][n][klp]   L multipliers of column j
     double* Uf;         // [sys][n][kvp]   U column j, rows j-kv..j (index kv = diagonal)
+    // FP32 copies of the factors (mixed-precision form; the same layout with
+    // the strides klp32, kvp32), used instead of Lf/Uf when factors32 is set
+    int factors32, klp32, kvp32;
+    float* Lf32;
+    float* Uf32;
     int32_t* ipiv;      // [sys][n]        0-based pivot rows
     double* work;       // [sys][n]        rhs / solution in unknown order (iK*V + iV)
     unsigned long long* negatives;  // optional: count of PSD < 0 written by the store kernel
@@ -86,6 +91,12 @@ void launch_local_factor(const LocalArgs& a, cudaStream_t s);
 void launch_local_rhs(const LocalArgs& a, bool from_work, cudaStream_t s);
 void launch_local_solve(const LocalArgs& a, cudaStream_t s);
 void launch_local_store(const LocalArgs& a, cudaStream_t s);
+// r = b - A x for every system (A assembled on the fly in the reference's order)
+void launch_local_residual(const LocalArgs& a, const double* b, const double* x, double* r,
+                           cudaStream_t s);
+// x += d; red[0] = max |d|, red[1] = max |x| (dkey-ordered, atomicMax)
+void launch_local_update(const LocalArgs& a, double* x, const double* d, unsigned long long* red,
+                         cudaStream_t s);
 
 // --- reductions / elementwise ---------------------------------------------------
 void launch_negative_count(const double* psd, size_t n, unsigned long long* out, cudaStream_t s);

@@ -13,6 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libverb4d_b200.so")
 
 VERB_OK = 0
+VERB_PREC_FP64 = 0
+VERB_PREC_MIXED = 1
 STATUS_NAMES = {
     0: "VERB_OK", 1: "VERB_ERR_PIVOT", 2: "VERB_ERR_ARG", 3: "VERB_ERR_CFL", 4: "VERB_ERR_BC",
     5: "VERB_ERR_TENSOR", 6: "VERB_ERR_NAN", 7: "VERB_ERR_CUDA", 8: "VERB_ERR_NOMEM",
@@ -65,6 +67,8 @@ SIGNATURES = {
     "verb_set_bc_types": (C.c_int, [_vp, _ip]),
     "verb_set_options": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int]),
     "verb_invalidate_lu": (C.c_int, [_vp]),
+    "verb_set_local_precision": (C.c_int, [_vp, C.c_int, C.c_int]),
+    "verb_local_refinement": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "verb_download_psd": (C.c_int, [_vp, _dp]),
     "verb_download_field": (C.c_int, [_vp, C.c_int, _dp]),
     "verb_field_device_ptr": (C.c_int, [_vp, C.c_int, C.POINTER(_dp)]),

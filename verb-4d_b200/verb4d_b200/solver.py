@@ -59,6 +59,18 @@ class Context:
     def invalidate_lu(self) -> None:
         L.check(self.lib.verb_invalidate_lu(self.h), "invalidate")
 
+    def set_local_precision(self, mode: str = "fp64", refinements: int = 0):
+        """'fp64' (LAPACK-equivalent factors) or 'mixed' (the same factors stored
+        in FP32); each solve is then refined `refinements` times in FP64."""
+        m = {"fp64": L.VERB_PREC_FP64, "mixed": L.VERB_PREC_MIXED}[mode]
+        L.check(self.lib.verb_set_local_precision(self.h, m, int(refinements)), "precision")
+
+    def local_refinement(self) -> float:
+        """max |d| / max |x| of the last refinement step (0 without refinement)."""
+        out = C.c_double()
+        L.check(self.lib.verb_local_refinement(self.h, C.byref(out)), "refinement")
+        return out.value
+
     # ----------------------------------------------------------------- phases
     def convection(self, dt: float) -> None:
         L.check(self.lib.verb_convection(self.h, float(dt)), "convection")
