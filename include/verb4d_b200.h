@@ -132,6 +132,31 @@ int verb_download_field(verb_ctx* ctx, int field, double* host);
 /* Device pointer of a field (for zero-copy use from the caller's CUDA code). */
 int verb_field_device_ptr(verb_ctx* ctx, int field, double** dev);
 
+/* ---- updatable input fields -------------------------------------------------
+ * The reference's UpdatableMatrix / UpdatableListMatrix time-update system
+ * (src/UpdatableMatrix.cpp:602-846, 913-961) on the device.  A field (D_LL
+ * .. the loss rates) becomes a list of components; each has a base array and
+ * time-ordered queues of replacement arrays (the .lst data files), scale
+ * factors and from/to limits per grid axis (0 MLT, 1 R, or L* for D_LL, 2 V,
+ * 3 K; `which` 0 = from, 1 = to).  verb_update_fields(t) pops every entry due
+ * at t as update() does, rebuilds the changed fields on the device (component
+ * = base * scale, zeroed outside the limits; field = sum, or mean over finite
+ * component values) and marks the cached LU / Thomas factors for
+ * recomputation as the driver does (src/VERB4D_Solver.cpp:1091-1096).
+ * Replacement arrays are copied to the device when queued.  A field with
+ * components cannot also be uploaded or scaled directly. */
+#define VERB_MERGE_SUM 0
+#define VERB_MERGE_MEAN 1
+int verb_field_add_component(verb_ctx* ctx, int field, const double* host_base, int* component);
+int verb_field_set_merge(verb_ctx* ctx, int field, int merge);
+int verb_component_queue_data(verb_ctx* ctx, int field, int component, double time,
+                              const double* host);
+int verb_component_queue_scale(verb_ctx* ctx, int field, int component, double time, double scale);
+int verb_component_queue_limit(verb_ctx* ctx, int field, int component, int axis, int which,
+                               double time, double value);
+/* updated_mask: bit f set when field f was rebuilt. */
+int verb_update_fields(verb_ctx* ctx, double current_time, unsigned int* updated_mask);
+
 /* ---- the step ------------------------------------------------------------ */
 /* Convection_2D over every (V,K) slice (src/Convection_2D.cpp:36-169). */
 int verb_convection(verb_ctx* ctx, double dt);

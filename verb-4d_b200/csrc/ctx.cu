@@ -5,7 +5,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <deque>
 #include <new>
+#include <utility>
 #include <vector>
 
 #include "verb_internal.cuh"
@@ -21,6 +23,23 @@ struct EventPair {
 };
 
 }  // namespace
+
+// One component of an updatable field (src/UpdatableMatrix.h:60-90): base
+// array, queued replacement arrays, scale and limit queues.
+struct UpdComponent {
+    double* base = nullptr;
+    std::deque<std::pair<double, double*>> data_q;           // (time, device array)
+    std::deque<std::pair<double, double>> scale_q;
+    std::deque<std::pair<double, double>> limit_q[4][2];     // [axis][from, to]
+    double scale = 1.0;                                       // latest_scale_coefficient
+    double lim[4][2] = {{-1e99, 1e99}, {-1e99, 1e99}, {-1e99, 1e99}, {-1e99, 1e99}};
+    double last_update_time = -1;
+};
+struct UpdField {
+    std::vector<UpdComponent> comps;
+    int merge = VERB_MERGE_SUM;
+    bool built = false;
+};
 
 struct verb_ctx {
     Dims d{};
@@ -65,6 +84,8 @@ struct verb_ctx {
     double *Pa = nullptr, *kfwork = nullptr, *obs = nullptr;
     size_t kfwork_bytes = 0;
     int* kfticket = nullptr;
+    // updatable fields (nullptr: plain uploaded field)
+    UpdField* upd[VERB_F_COUNT] = {};
     // timing
     bool timing = false;
     std::vector<EventPair> ev[PH_N];
@@ -550,6 +571,13 @@ int verb_destroy(verb_ctx* c)
     for (int i = 0; i < VERB_F_COUNT; i++) {
         cudaFree(c->f[i]);
         cudaFree(c->fbase[i]);
+        if (c->upd[i]) {
+            for (UpdComponent& k : c->upd[i]->comps) {
+                cudaFree(k.base);
+                for (auto& e : k.data_q) cudaFree(e.second);
+            }
+            delete c->upd[i];
+        }
     }
     for (int i = 0; i < VERB_BCF_COUNT; i++) cudaFree(c->bc[i]);
     for (void* p : {(void*)c->Lf32, (void*)c->Uf32, (void*)c->lrhs, (void*)c->lres,
@@ -591,7 +619,7 @@ int verb_device_bytes(const verb_ctx* c, size_t* bytes)
 
 static int upload_common(verb_ctx* c, int fid, const void* src, cudaMemcpyKind kind)
 {
-    if (!c || fid < 0 || fid >= VERB_F_COUNT || !src) return VERB_ERR_ARG;
+    if (!c || fid < 0 || fid >= VERB_F_COUNT || !src || c->upd[fid]) return VERB_ERR_ARG;
     const size_t bytes = npts(c) * sizeof(double);
     int s = ensure_field(c, fid);
     if (s) return s;
@@ -624,7 +652,7 @@ int verb_upload_field_device(verb_ctx* c, int fid, const double* dev)
 
 int verb_set_field_scale(verb_ctx* c, int fid, double scale)
 {
-    if (!c || fid < 0 || fid >= VERB_F_COUNT) return VERB_ERR_ARG;
+    if (!c || fid < 0 || fid >= VERB_F_COUNT || c->upd[fid]) return VERB_ERR_ARG;
     if (scale == c->scale[fid]) return VERB_OK;
     const size_t bytes = npts(c) * sizeof(double);
     if (c->f[fid]) {
@@ -1129,3 +1157,174 @@ int verb_assimilate_radial(verb_ctx* c, const double* obs_host, double dt, doubl
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Updatable fields (src/UpdatableMatrix.cpp:602-846, 913-961).
+
+namespace {
+
+bool updatable_field(int fid)
+{
+    return fid >= VERB_F_DLL && fid < VERB_F_COUNT;  // coefficients, velocities, G, sources, losses
+}
+
+int component_of(verb_ctx* c, int fid, int comp, UpdComponent** out)
+{
+    if (!c || fid < 0 || fid >= VERB_F_COUNT || !c->upd[fid] || comp < 0 ||
+        comp >= (int)c->upd[fid]->comps.size())
+        return VERB_ERR_ARG;
+    *out = &c->upd[fid]->comps[comp];
+    return VERB_OK;
+}
+
+// one UpdatableMatrix::update on the host side: pop every queue entry due at
+// current_time and report whether anything changed
+bool pop_component(UpdComponent& k, double t, double** new_base)
+{
+    bool updated = false;
+    // data: the last due entry, loaded only if newer than the last load (:636-661)
+    double* data = nullptr;
+    double data_time = 0;
+    while (!k.data_q.empty() && t >= k.data_q.front().first) {
+        if (data) cudaFree(data);  // superseded before it was used
+        data = k.data_q.front().second;
+        data_time = k.data_q.front().first;
+        k.data_q.pop_front();
+    }
+    if (data) {
+        if (t >= data_time && k.last_update_time < data_time) {
+            *new_base = data;
+            k.last_update_time = t;
+            updated = true;
+        } else {
+            cudaFree(data);
+        }
+    }
+    // scale (:676-695) and limits (:724-788): the latest due value, updated
+    // whenever an entry is popped
+    while (!k.scale_q.empty() && t >= k.scale_q.front().first) {
+        k.scale = k.scale_q.front().second;
+        k.scale_q.pop_front();
+        updated = true;
+    }
+    for (int a = 0; a < 4; a++)
+        for (int w = 0; w < 2; w++)
+            while (!k.limit_q[a][w].empty() && t >= k.limit_q[a][w].front().first) {
+                k.lim[a][w] = k.limit_q[a][w].front().second;
+                k.limit_q[a][w].pop_front();
+                updated = true;
+            }
+    return updated;
+}
+
+}  // namespace
+
+int verb_field_add_component(verb_ctx* c, int fid, const double* host_base, int* comp)
+{
+    if (!c || !host_base || !updatable_field(fid)) return VERB_ERR_ARG;
+    if (!c->upd[fid]) c->upd[fid] = new (std::nothrow) UpdField();
+    if (!c->upd[fid]) return VERB_ERR_NOMEM;
+    UpdField& u = *c->upd[fid];
+    if ((int)u.comps.size() >= MAX_COMPONENTS) return VERB_ERR_SIZE;
+    UpdComponent k;
+    CK(cudaMalloc(&k.base, npts(c) * sizeof(double)));
+    CK(cudaMemcpyAsync(k.base, host_base, npts(c) * sizeof(double), cudaMemcpyHostToDevice,
+                       c->stream));
+    u.comps.push_back(k);
+    u.built = false;
+    if (comp) *comp = (int)u.comps.size() - 1;
+    return VERB_OK;
+}
+
+int verb_field_set_merge(verb_ctx* c, int fid, int merge)
+{
+    if (!c || fid < 0 || fid >= VERB_F_COUNT || !c->upd[fid] ||
+        (merge != VERB_MERGE_SUM && merge != VERB_MERGE_MEAN))
+        return VERB_ERR_ARG;
+    c->upd[fid]->merge = merge;
+    c->upd[fid]->built = false;
+    return VERB_OK;
+}
+
+int verb_component_queue_data(verb_ctx* c, int fid, int comp, double time, const double* host)
+{
+    UpdComponent* k = nullptr;
+    if (int s = component_of(c, fid, comp, &k)) return s;
+    if (!host || (!k->data_q.empty() && time < k->data_q.back().first)) return VERB_ERR_ARG;
+    double* d = nullptr;
+    CK(cudaMalloc(&d, npts(c) * sizeof(double)));
+    CK(cudaMemcpyAsync(d, host, npts(c) * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    k->data_q.emplace_back(time, d);
+    return VERB_OK;
+}
+
+int verb_component_queue_scale(verb_ctx* c, int fid, int comp, double time, double scale)
+{
+    UpdComponent* k = nullptr;
+    if (int s = component_of(c, fid, comp, &k)) return s;
+    if (!k->scale_q.empty() && time < k->scale_q.back().first) return VERB_ERR_ARG;
+    k->scale_q.emplace_back(time, scale);
+    return VERB_OK;
+}
+
+int verb_component_queue_limit(verb_ctx* c, int fid, int comp, int axis, int which, double time,
+                               double value)
+{
+    UpdComponent* k = nullptr;
+    if (int s = component_of(c, fid, comp, &k)) return s;
+    if (axis < 0 || axis > 3 || (which != 0 && which != 1)) return VERB_ERR_ARG;
+    auto& q = k->limit_q[axis][which];
+    if (!q.empty() && time < q.back().first) return VERB_ERR_ARG;
+    q.emplace_back(time, value);
+    return VERB_OK;
+}
+
+int verb_update_fields(verb_ctx* c, double current_time, unsigned int* updated_mask)
+{
+    if (!c) return VERB_ERR_ARG;
+    unsigned int mask = 0;
+    for (int fid = 0; fid < VERB_F_COUNT; fid++) {
+        UpdField* u = c->upd[fid];
+        if (!u || u->comps.empty()) continue;
+        bool changed = !u->built;
+        for (UpdComponent& k : u->comps) {
+            double* nb = nullptr;
+            if (pop_component(k, current_time, &nb)) changed = true;
+            if (nb) {
+                // the replacement becomes the base once the stream has used the old one
+                double* old = k.base;
+                k.base = nb;
+                CK(cudaStreamSynchronize(c->stream));
+                cudaFree(old);
+            }
+        }
+        if (!changed) continue;
+        // grid axes of the field (src/VERB4D_Solver.cpp:635-682; D_LL uses L*)
+        const int ax[4] = {VERB_F_P, fid == VERB_F_DLL ? VERB_F_L : VERB_F_R, VERB_F_V, VERB_F_K};
+        MergeArgs m{};
+        for (int a = 0; a < 4; a++) {
+            if (int s = need_field(c, ax[a])) return s;
+            m.axis[a] = c->f[ax[a]];
+        }
+        m.ncomp = (int)u->comps.size();
+        m.mean = u->merge == VERB_MERGE_MEAN;
+        for (int i = 0; i < m.ncomp; i++) {
+            const UpdComponent& k = u->comps[i];
+            m.comp[i].base = k.base;
+            m.comp[i].scale = k.scale;
+            for (int a = 0; a < 4; a++) {
+                m.comp[i].from[a] = k.lim[a][0];
+                m.comp[i].to[a] = k.lim[a][1];
+            }
+        }
+        if (int s = ensure_field(c, fid)) return s;
+        launch_merge_components(c->f[fid], m, npts(c), c->stream);
+        c->acc.kernel_launches++;
+        c->uploaded[fid] = true;
+        u->built = true;
+        mark_dirty(c, fid);
+        mask |= 1u << fid;
+    }
+    if (updated_mask) *updated_mask = mask;
+    return check_launch();
+}

@@ -105,6 +105,21 @@ void launch_tensor_min(const double* dvv, const double* dkk, const double* dvk, 
 void launch_clamp_positive(double* psd, size_t n, cudaStream_t s);
 void launch_scale_copy(double* dst, const double* src, double scale, size_t n, cudaStream_t s);
 
+// --- updatable fields ------------------------------------------------------------------
+constexpr int MAX_COMPONENTS = 8;
+struct MergeComp {
+    const double* base;
+    double scale;
+    double from[4], to[4];  // limits per grid axis (P, R or L, V, K)
+};
+struct MergeArgs {
+    MergeComp comp[MAX_COMPONENTS];
+    int ncomp;
+    int mean;                // 0: sum, 1: mean over finite component values
+    const double* axis[4];   // grid coordinates of every point
+};
+void launch_merge_components(double* out, const MergeArgs& m, size_t n, cudaStream_t s);
+
 // Monotone mapping of doubles to unsigned 64-bit keys (for atomicMin on doubles).
 __host__ __device__ __forceinline__ unsigned long long dkey(double v)
 {

@@ -67,6 +67,13 @@ SIGNATURES = {
     "verb_set_bc_types": (C.c_int, [_vp, _ip]),
     "verb_set_options": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int]),
     "verb_invalidate_lu": (C.c_int, [_vp]),
+    "verb_field_add_component": (C.c_int, [_vp, C.c_int, _dp, C.POINTER(C.c_int)]),
+    "verb_field_set_merge": (C.c_int, [_vp, C.c_int, C.c_int]),
+    "verb_component_queue_data": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double, _dp]),
+    "verb_component_queue_scale": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double, C.c_double]),
+    "verb_component_queue_limit": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                             C.c_double]),
+    "verb_update_fields": (C.c_int, [_vp, C.c_double, C.POINTER(C.c_uint)]),
     "verb_set_local_precision": (C.c_int, [_vp, C.c_int, C.c_int]),
     "verb_local_refinement": (C.c_int, [_vp, C.POINTER(C.c_double)]),
     "verb_download_psd": (C.c_int, [_vp, _dp]),

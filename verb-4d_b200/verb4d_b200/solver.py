@@ -65,6 +65,41 @@ class Context:
         m = {"fp64": L.VERB_PREC_FP64, "mixed": L.VERB_PREC_MIXED}[mode]
         L.check(self.lib.verb_set_local_precision(self.h, m, int(refinements)), "precision")
 
+    # ---- updatable fields (UpdatableMatrix / UpdatableListMatrix on the device)
+    def add_component(self, name: str, base) -> int:
+        """Turn field `name` into a component list (if it is not one yet) and
+        add a component with the given base array; returns its index."""
+        a = np.ascontiguousarray(base, dtype=np.float64)
+        out = C.c_int()
+        L.check(self.lib.verb_field_add_component(self.h, L.FIELD_IDS[name],
+                                                  a.ctypes.data_as(L._dp), C.byref(out)),
+                "add_component")
+        return out.value
+
+    def set_merge(self, name: str, merge: str = "sum"):
+        L.check(self.lib.verb_field_set_merge(self.h, L.FIELD_IDS[name],
+                                              {"sum": 0, "mean": 1}[merge]), "merge")
+
+    def queue_data(self, name: str, comp: int, time: float, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        L.check(self.lib.verb_component_queue_data(self.h, L.FIELD_IDS[name], comp, float(time),
+                                                   a.ctypes.data_as(L._dp)), "queue_data")
+
+    def queue_scale(self, name: str, comp: int, time: float, scale: float):
+        L.check(self.lib.verb_component_queue_scale(self.h, L.FIELD_IDS[name], comp, float(time),
+                                                    float(scale)), "queue_scale")
+
+    def queue_limit(self, name: str, comp: int, axis: int, which: str, time: float, value: float):
+        L.check(self.lib.verb_component_queue_limit(self.h, L.FIELD_IDS[name], comp, int(axis),
+                                                    {"from": 0, "to": 1}[which], float(time),
+                                                    float(value)), "queue_limit")
+
+    def update_fields(self, time: float) -> list:
+        """Pop every queued update due at `time`; returns the rebuilt fields."""
+        mask = C.c_uint()
+        L.check(self.lib.verb_update_fields(self.h, float(time), C.byref(mask)), "update_fields")
+        return [n for n, f in L.FIELD_IDS.items() if mask.value >> f & 1]
+
     def local_refinement(self) -> float:
         """max |d| / max |x| of the last refinement step (0 without refinement)."""
         out = C.c_double()
