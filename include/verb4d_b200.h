@@ -56,7 +56,9 @@ typedef enum {
     VERB_ERR_NOMEM = 8,   /* device allocation failed / would not fit */
     VERB_ERR_GRID = 9,    /* convection line shorter than 11 points (QUICKEST6.cpp:56-59) */
     VERB_TIMEOUT = 10,    /* a bounded device wait gave up */
-    VERB_ERR_SIZE = 11    /* larger than the fixed scratch of verb_convection_2d_noalloc */
+    VERB_ERR_SIZE = 11,   /* size beyond a fixed limit (the no-allocation scratch, line
+                             length, component count) or a file of other dimensions */
+    VERB_ERR_IO = 12      /* a file could not be opened, read or written */
 } verb_status;
 
 enum { VERB_BC_PERIODIC = 0, VERB_BC_CONSTANT_VALUE = 1, VERB_BC_CONSTANT_DERIVATIVE = 2 };
@@ -156,6 +158,25 @@ int verb_component_queue_limit(verb_ctx* ctx, int field, int component, int axis
                                double time, double value);
 /* updated_mask: bit f set when field f was rebuilt. */
 int verb_update_fields(verb_ctx* ctx, double current_time, unsigned int* updated_mask);
+
+/* ---- output and restart files ----------------------------------------------
+ * .pltb files as the reference writes and reads them (Matrix4D::
+ * writeToBinaryFile / readFromBinaryFile, src/Matrix.cpp:5700-5720,
+ * 5780-5808): four int32 sizes (P, R, V, K), then the values.  A write takes a
+ * device snapshot of the field on the context stream and returns; the copy to
+ * pinned host memory runs on an output stream and a host thread writes the
+ * file, as the reference's asynchronous output_writer does
+ * (src/VERB4D_Solver.cpp:1255-1267).  One write is in flight at a time (the
+ * next write waits for it); verb_output_wait joins it and returns its status.
+ * Restart: read the PSD file back into VERB_F_PSD and continue from its time
+ * (the reference's initial_PSD / time_first / it_first,
+ * src/ReadInitialData.cpp:207-208). */
+int verb_write_field_pltb(verb_ctx* ctx, int field, const char* path, int async_write);
+int verb_output_wait(verb_ctx* ctx);
+int verb_read_field_pltb(verb_ctx* ctx, int field, const char* path);
+/* Append "time<TAB>filename" to a PSD.lst list (Matrix4D::writeToLstFile,
+ * src/Matrix.cpp:5760-5778; time printed with 5 decimals). */
+int verb_append_lst(const char* lst_path, double time, const char* filename);
 
 /* ---- the step ------------------------------------------------------------ */
 /* Convection_2D over every (V,K) slice (src/Convection_2D.cpp:36-169). */

@@ -150,6 +150,20 @@ class _Lib:
         return st, f, pa, F, Pf
 
     # ------------------------------------------------------------- band LU
+    def write_pltb(self, path, arr):
+        """Reference writer (Matrix4D::writeToBinaryFile) through oracle/_ref."""
+        a = _f64(arr)
+        w, x, y, z = a.shape
+        return self.lib.ref_write_pltb(_p(a), C.c_int(w), C.c_int(x), C.c_int(y), C.c_int(z),
+                                       str(path).encode())
+
+    def read_pltb(self, path, shape):
+        out = np.zeros(shape)
+        w, x, y, z = shape
+        self.lib.ref_read_pltb(_p(out), C.c_int(w), C.c_int(x), C.c_int(y), C.c_int(z),
+                               str(path).encode())
+        return out
+
     def gbtrf(self, ab, n, kl, ku):
         ab = _f64(ab).copy()
         ipiv = np.zeros(n, dtype=np.int64)

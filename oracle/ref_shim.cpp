@@ -179,6 +179,24 @@ int ref_kf_diffusion_1d(double* forecast, double* Pa, double* F, double* Pf, con
     return 0;
 }
 
+// PSD output / restart files: Matrix4D::writeToBinaryFile and
+// readFromBinaryFile (src/Matrix.cpp:5700-5720, 5780-5808), the .pltb format.
+int ref_write_pltb(const double* data, int w, int x, int y, int z, const char* path)
+{
+    Matrix4D<double> m((size_t)w, (size_t)x, (size_t)y, (size_t)z);
+    std::memcpy(&m[0][0][0][0], data, sizeof(double) * (size_t)w * x * y * z);
+    m.writeToBinaryFile(path);
+    return 0;
+}
+
+int ref_read_pltb(double* data, int w, int x, int y, int z, const char* path)
+{
+    Matrix4D<double> m((size_t)w, (size_t)x, (size_t)y, (size_t)z);
+    m.readFromBinaryFile(path);
+    std::memcpy(data, &m[0][0][0][0], sizeof(double) * (size_t)w * x * y * z);
+    return 0;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------

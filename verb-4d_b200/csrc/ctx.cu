@@ -7,6 +7,8 @@
 #include <cstring>
 #include <deque>
 #include <new>
+#include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -86,6 +88,14 @@ struct verb_ctx {
     int* kfticket = nullptr;
     // updatable fields (nullptr: plain uploaded field)
     UpdField* upd[VERB_F_COUNT] = {};
+    // asynchronous output: device snapshot -> pinned host copy on a copy
+    // stream -> file written by a host thread
+    double* out_snap = nullptr;
+    double* out_host = nullptr;
+    cudaStream_t out_stream = nullptr;
+    cudaEvent_t out_ev_snap = nullptr, out_ev_host = nullptr;
+    std::thread out_thread;
+    int out_status = VERB_OK;
     // timing
     bool timing = false;
     std::vector<EventPair> ev[PH_N];
@@ -529,7 +539,8 @@ const char* verb_status_string(int s)
         case VERB_ERR_NOMEM: return "out of device memory";
         case VERB_ERR_GRID: return "convection grid shorter than 11 points";
         case VERB_TIMEOUT: return "device wait timed out";
-        case VERB_ERR_SIZE: return "slice larger than the no-allocation scratch";
+        case VERB_ERR_SIZE: return "size beyond a fixed limit or file dimensions differ";
+        case VERB_ERR_IO: return "file could not be opened, read or written";
         default: return "unknown status";
     }
 }
@@ -567,6 +578,12 @@ int verb_create(verb_ctx** out, int P, int R, int V, int K, void* stream)
 int verb_destroy(verb_ctx* c)
 {
     if (!c) return VERB_OK;
+    if (c->out_thread.joinable()) c->out_thread.join();
+    if (c->out_stream) cudaStreamDestroy(c->out_stream);
+    if (c->out_ev_snap) cudaEventDestroy(c->out_ev_snap);
+    if (c->out_ev_host) cudaEventDestroy(c->out_ev_host);
+    cudaFree(c->out_snap);
+    cudaFreeHost(c->out_host);
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (int i = 0; i < VERB_F_COUNT; i++) {
         cudaFree(c->f[i]);
@@ -1327,4 +1344,95 @@ int verb_update_fields(verb_ctx* c, double current_time, unsigned int* updated_m
     }
     if (updated_mask) *updated_mask = mask;
     return check_launch();
+}
+
+// ---------------------------------------------------------------------------
+// PSD output and restart files (.pltb: Matrix4D::writeToBinaryFile /
+// readFromBinaryFile, src/Matrix.cpp:5700-5720, 5780-5808: four int32 sizes,
+// then the values in [P][R][V][K] order), written asynchronously as the
+// reference's output_writer does (src/VERB4D_Solver.cpp:1255-1267).
+
+namespace {
+
+int write_pltb(const char* path, const Dims& d, const double* host)
+{
+    FILE* f = fopen(path, "wb");
+    if (!f) return VERB_ERR_IO;
+    const int32_t sz[4] = {d.P, d.R, d.V, d.K};
+    bool ok = fwrite(sz, sizeof(int32_t), 4, f) == 4;
+    ok = ok && fwrite(host, sizeof(double), d.npts(), f) == d.npts();
+    ok = (fclose(f) == 0) && ok;
+    return ok ? VERB_OK : VERB_ERR_IO;
+}
+
+}  // namespace
+
+int verb_output_wait(verb_ctx* c)
+{
+    if (!c) return VERB_ERR_ARG;
+    if (c->out_thread.joinable()) c->out_thread.join();
+    const int s = c->out_status;
+    c->out_status = VERB_OK;
+    return s;
+}
+
+int verb_write_field_pltb(verb_ctx* c, int fid, const char* path, int async_write)
+{
+    if (!c || !path || fid < 0 || fid >= VERB_F_COUNT || !c->f[fid]) return VERB_ERR_ARG;
+    // one output in flight, as the reference waits for its previous writer
+    if (int s = verb_output_wait(c)) return s;
+    const size_t bytes = npts(c) * sizeof(double);
+    if (!c->out_snap) {
+        CK(cudaMalloc(&c->out_snap, bytes));
+        CK(cudaMallocHost(&c->out_host, bytes));
+        CK(cudaStreamCreateWithFlags(&c->out_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&c->out_ev_snap, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&c->out_ev_host, cudaEventDisableTiming));
+    }
+    // snapshot on the compute stream (the next step may overwrite the field),
+    // then the device-to-host copy on the output stream, overlapping compute
+    CK(cudaMemcpyAsync(c->out_snap, c->f[fid], bytes, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaEventRecord(c->out_ev_snap, c->stream));
+    CK(cudaStreamWaitEvent(c->out_stream, c->out_ev_snap, 0));
+    CK(cudaMemcpyAsync(c->out_host, c->out_snap, bytes, cudaMemcpyDeviceToHost, c->out_stream));
+    CK(cudaEventRecord(c->out_ev_host, c->out_stream));
+    std::string p(path);
+    c->out_thread = std::thread([c, p]() {
+        int s = cuda_ok(cudaEventSynchronize(c->out_ev_host));
+        if (!s) s = write_pltb(p.c_str(), c->d, c->out_host);
+        c->out_status = s;
+    });
+    return async_write ? VERB_OK : verb_output_wait(c);
+}
+
+int verb_read_field_pltb(verb_ctx* c, int fid, const char* path)
+{
+    if (!c || !path || fid < 0 || fid >= VERB_F_COUNT) return VERB_ERR_ARG;
+    FILE* f = fopen(path, "rb");
+    if (!f) return VERB_ERR_IO;
+    int32_t sz[4];
+    std::vector<double> buf;
+    int s = VERB_OK;
+    if (fread(sz, sizeof(int32_t), 4, f) != 4) s = VERB_ERR_IO;
+    else if (sz[0] != c->d.P || sz[1] != c->d.R || sz[2] != c->d.V || sz[3] != c->d.K) s = VERB_ERR_SIZE;
+    if (!s) {
+        buf.resize(npts(c));
+        if (fread(buf.data(), sizeof(double), buf.size(), f) != buf.size()) s = VERB_ERR_IO;
+    }
+    fclose(f);
+    if (s) return s;
+    s = verb_upload_field(c, fid, buf.data());
+    if (!s) s = cuda_ok(cudaStreamSynchronize(c->stream));
+    return s;
+}
+
+int verb_append_lst(const char* lst_path, double time, const char* filename)
+{
+    // Matrix4D::writeToLstFile (src/Matrix.cpp:5760-5778) with the time as
+    // write_PSD_output formats it (fixed, 5 decimals; VERB4D_Solver.cpp:180-184)
+    if (!lst_path || !filename) return VERB_ERR_ARG;
+    FILE* f = fopen(lst_path, "a");
+    if (!f) return VERB_ERR_IO;
+    const bool ok = fprintf(f, "%.5f\t%s\n", time, filename) > 0;
+    return (fclose(f) == 0 && ok) ? VERB_OK : VERB_ERR_IO;
 }

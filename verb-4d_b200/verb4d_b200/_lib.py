@@ -18,7 +18,7 @@ VERB_PREC_MIXED = 1
 STATUS_NAMES = {
     0: "VERB_OK", 1: "VERB_ERR_PIVOT", 2: "VERB_ERR_ARG", 3: "VERB_ERR_CFL", 4: "VERB_ERR_BC",
     5: "VERB_ERR_TENSOR", 6: "VERB_ERR_NAN", 7: "VERB_ERR_CUDA", 8: "VERB_ERR_NOMEM",
-    9: "VERB_ERR_GRID", 10: "VERB_TIMEOUT", 11: "VERB_ERR_SIZE",
+    9: "VERB_ERR_GRID", 10: "VERB_TIMEOUT", 11: "VERB_ERR_SIZE", 12: "VERB_ERR_IO",
 }
 
 # 4-D fields (verb_field)
@@ -67,6 +67,10 @@ SIGNATURES = {
     "verb_set_bc_types": (C.c_int, [_vp, _ip]),
     "verb_set_options": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int]),
     "verb_invalidate_lu": (C.c_int, [_vp]),
+    "verb_write_field_pltb": (C.c_int, [_vp, C.c_int, C.c_char_p, C.c_int]),
+    "verb_output_wait": (C.c_int, [_vp]),
+    "verb_read_field_pltb": (C.c_int, [_vp, C.c_int, C.c_char_p]),
+    "verb_append_lst": (C.c_int, [C.c_char_p, C.c_double, C.c_char_p]),
     "verb_field_add_component": (C.c_int, [_vp, C.c_int, _dp, C.POINTER(C.c_int)]),
     "verb_field_set_merge": (C.c_int, [_vp, C.c_int, C.c_int]),
     "verb_component_queue_data": (C.c_int, [_vp, C.c_int, C.c_int, C.c_double, _dp]),

@@ -65,6 +65,20 @@ class Context:
         m = {"fp64": L.VERB_PREC_FP64, "mixed": L.VERB_PREC_MIXED}[mode]
         L.check(self.lib.verb_set_local_precision(self.h, m, int(refinements)), "precision")
 
+    # ---- output and restart files (.pltb)
+    def write_pltb(self, path: str, name: str = "psd", wait: bool = True):
+        """Write a field as a .pltb file; with wait=False the write finishes in
+        the background (output_wait() joins it)."""
+        L.check(self.lib.verb_write_field_pltb(self.h, L.FIELD_IDS[name], path.encode(),
+                                               0 if wait else 1), "write_pltb")
+
+    def output_wait(self):
+        L.check(self.lib.verb_output_wait(self.h), "output_wait")
+
+    def read_pltb(self, path: str, name: str = "psd"):
+        L.check(self.lib.verb_read_field_pltb(self.h, L.FIELD_IDS[name], path.encode()),
+                "read_pltb")
+
     # ---- updatable fields (UpdatableMatrix / UpdatableListMatrix on the device)
     def add_component(self, name: str, base) -> int:
         """Turn field `name` into a component list (if it is not one yet) and
