@@ -159,6 +159,18 @@ int verb_component_queue_limit(verb_ctx* ctx, int field, int component, int axis
 /* updated_mask: bit f set when field f was rebuilt. */
 int verb_update_fields(verb_ctx* ctx, double current_time, unsigned int* updated_mask);
 
+/* L* remapping (src/VERB4D_Solver.cpp:557-619): interpolate every (P,V,K)
+ * line of the PSD from the current L* field to new_L_host ([P][R][V][K],
+ * strictly increasing along R) with the reference's monotone cubic
+ * interpolator (Opm::MonotCubicInterpolator), then make new_L the L* field.
+ * The reference's Cubic1D wrapper (src/Interpolation.cpp:26-51) builds its
+ * point vectors after reserving them (n zero points precede the grid) and
+ * returns an empty matrix that the caller assigns over the result, so its
+ * output is undefined; this entry point interpolates the line as the
+ * wrapper's documentation describes.  Jacobians that depend on L* are
+ * updated by the caller, as the reference's driver does (:563-565). */
+int verb_remap_L(verb_ctx* ctx, const double* new_L_host);
+
 /* ---- output and restart files ----------------------------------------------
  * .pltb files as the reference writes and reads them (Matrix4D::
  * writeToBinaryFile / readFromBinaryFile, src/Matrix.cpp:5700-5720,

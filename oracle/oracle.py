@@ -150,6 +150,15 @@ class _Lib:
         return st, f, pa, F, Pf
 
     # ------------------------------------------------------------- band LU
+    def monot_cubic(self, x, f, xq):
+        """Monotone cubic interpolation: orc_monot_cubic in the oracle,
+        ref_monot_cubic (Opm::MonotCubicInterpolator) in the reference build."""
+        x, f, xq = _f64(x), _f64(f), _f64(xq)
+        out = np.zeros(len(xq))
+        fn = self.lib.orc_monot_cubic if self.has("orc_monot_cubic") else self.lib.ref_monot_cubic
+        st = fn(_p(x), _p(f), C.c_int(len(x)), _p(xq), _p(out), C.c_int(len(xq)))
+        return st, out
+
     def write_pltb(self, path, arr):
         """Reference writer (Matrix4D::writeToBinaryFile) through oracle/_ref."""
         a = _f64(arr)

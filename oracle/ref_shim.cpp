@@ -13,6 +13,7 @@
 // convection slice is [P][R].
 #include <cstring>
 #include <tuple>
+#include <vector>
 
 #include "BoundaryConditionType.hpp"
 #include "Convection_1D_ULTIMATE_QUICKEST6.h"
@@ -23,6 +24,7 @@
 #include "Diffusion_2D.h"
 #include "Matrix.h"
 #include "MatrixSolver.h"
+#include "MonotCubicInterpolator.hpp"
 
 namespace {
 
@@ -176,6 +178,16 @@ int ref_kf_diffusion_1d(double* forecast, double* Pa, double* F, double* Pf, con
     std::memcpy(forecast, &f[0], sizeof(double) * n);
     std::memcpy(Pa, pa[0], sizeof(double) * n * n);
     std::memcpy(F, model[0], sizeof(double) * n * n);
+    return 0;
+}
+
+// The interpolator behind the L* remapping (Opm::MonotCubicInterpolator,
+// src/MonotCubicInterpolator.cpp), built from the points themselves.
+int ref_monot_cubic(const double* x, const double* f, int n, const double* xq, double* out, int m)
+{
+    std::vector<double> xv(x, x + n), fv(f, f + n);
+    Opm::MonotCubicInterpolator ip(xv, fv);
+    for (int j = 0; j < m; j++) out[j] = ip.evaluate(xq[j]);
     return 0;
 }
 

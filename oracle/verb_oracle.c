@@ -912,3 +912,68 @@ long orc_step(orc_state* s, double dt, double sub_dt, int recompute_lu)
     return neg;
 #undef I4
 }
+
+/* ---------------------------------------------------------------------------
+ * Monotone cubic Hermite interpolation (test oracle for the L* remapping).
+ * src/MonotCubicInterpolator.cpp:613-650 (derivatives), :379-470 (monotone
+ * test), :653-700 (adjustment), :160-225 (evaluation), Hermite basis
+ * MonotCubicInterpolator.hpp:522-537, isMonotoneCoeff :579-585. */
+static double h00(double t) { return 2 * t * t * t - 3 * t * t + 1; }
+static double h10(double t) { return t * t * t - 2 * t * t + t; }
+static double h01(double t) { return -2 * t * t * t + 3 * t * t; }
+static double h11(double t) { return t * t * t - t * t; }
+
+int orc_monot_cubic(const double* x, const double* f, int n, const double* xq, double* out, int m)
+{
+    if (n < 2) return -1;
+    for (int i = 0; i + 1 < n; i++)
+        if (!(x[i] < x[i + 1])) return -1;
+    double* d = (double*)malloc(sizeof(double) * n);
+    d[0] = (f[1] - f[0]) / (x[1] - x[0]);
+    d[n - 1] = (f[n - 1] - f[n - 2]) / (x[n - 1] - x[n - 2]);
+    for (int i = 1; i + 1 < n; i++)
+        d[i] = (f[i + 1] - f[i]) / (2 * (x[i + 1] - x[i])) + (f[i] - f[i - 1]) / (2 * (x[i] - x[i - 1]));
+    /* monotone: skip equal leading values, take the direction of the first
+     * change, fail at the first pair that goes the other way */
+    int monotone = 1, i = 0;
+    while (i + 1 < n && f[i] == f[i + 1]) i++;
+    if (i + 1 < n) {
+        const int dec = f[i] > f[i + 1];
+        for (i = i + 1; i + 1 < n; i++) {
+            if (dec ? (f[i] < f[i + 1]) : (f[i] > f[i + 1])) {
+                monotone = 0;
+                break;
+            }
+        }
+    }
+    if (monotone) {
+        for (int j = 0; j + 1 < n; j++) {
+            const double delta = (f[j + 1] - f[j]) / (x[j + 1] - x[j]);
+            if (fabs(delta) < 1e-14) {
+                d[j] = 0.0;
+                d[j + 1] = 0.0;
+            } else {
+                const double alpha = d[j] / delta, beta = d[j + 1] / delta;
+                if (!((alpha * alpha + beta * beta) <= 9)) {
+                    const double tau = 3 / sqrt(alpha * alpha + beta * beta);
+                    d[j] = tau * alpha * delta;
+                    d[j + 1] = tau * beta * delta;
+                }
+            }
+        }
+    }
+    for (int q = 0; q < m; q++) {
+        const double v = xq[q];
+        int k = 0;  /* lower_bound: first x[k] >= v */
+        while (k < n && x[k] < v) k++;
+        if (k == 0) out[q] = f[0];
+        else if (k == n) out[q] = f[n - 1];
+        else {
+            const double t = (v - x[k - 1]) / (x[k] - x[k - 1]);
+            const double h = x[k] - x[k - 1];
+            out[q] = f[k - 1] * h00(t) + d[k - 1] * h10(t) * h + f[k] * h01(t) + d[k] * h11(t) * h;
+        }
+    }
+    free(d);
+    return 0;
+}

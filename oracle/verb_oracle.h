@@ -69,6 +69,13 @@ int orc_kf_diffusion_1d(double* forecast, double* Pa, double* F, double* Pf, con
                         int lbc_t, int ubc_t, const double* obs, double dt, double model_error,
                         double obs_error);
 
+/* Monotone cubic interpolation of (x[i], f[i]), i < n, at xq[j], j < m
+ * (Opm::MonotCubicInterpolator, src/MonotCubicInterpolator.cpp:95-104,
+ * 160-225, 379-470, 613-700: averaged-secant derivatives, the monotone
+ * adjustment when the data are monotone, cubic Hermite evaluation, constant
+ * extrapolation).  x must be strictly increasing; returns -1 otherwise. */
+int orc_monot_cubic(const double* x, const double* f, int n, const double* xq, double* out, int m);
+
 /* Whole operator-split step over 4-D fields [P][R][V][K] (K fastest), in the
  * order and with the source/loss routing of src/VERB4D_Solver.cpp:851-1242. */
 typedef struct {

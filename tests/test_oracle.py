@@ -151,3 +151,26 @@ def test_oracle_vs_reference_fresh_inputs(oracle_lib):
         o2 = ref_lu.diffusion_2d(s2(f["psd"]), *la, lu=lu2, ipiv=ip2)[1]
         assert np.array_equal(ip1 + 1, ip2)
         assert rel(o1, o2) < LOCAL_RTOL
+
+
+@pytest.mark.skipif(not O.have_reference(), reason="reference not built here")
+def test_monot_cubic_matches_reference_interpolator(oracle_lib):
+    # the interpolator of the L* remapping (Opm::MonotCubicInterpolator compiled
+    # from the reference sources) against the C restatement, including
+    # monotone data (derivative adjustment), flat starts and extrapolation
+    ref = O.reference(lu_caching=True)
+    rng = np.random.default_rng(0)
+    for trial in range(300):
+        n = int(rng.integers(2, 40))
+        x = np.unique(rng.uniform(0, 10, n))
+        if len(x) < 2:
+            continue
+        f = rng.standard_normal(len(x))
+        if trial % 3 == 0:
+            f = np.sort(f) * (1 if trial % 2 else -1)
+        if trial % 7 == 0:
+            f[:3] = f[0]
+        xq = np.concatenate([rng.uniform(-1, 11, 50), x])
+        st, a = oracle_lib.monot_cubic(x, f, xq)
+        _, b = ref.monot_cubic(x, f, xq)
+        assert st == 0 and np.array_equal(a, b), trial

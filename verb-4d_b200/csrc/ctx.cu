@@ -1436,3 +1436,34 @@ int verb_append_lst(const char* lst_path, double time, const char* filename)
     const bool ok = fprintf(f, "%.5f\t%s\n", time, filename) > 0;
     return (fclose(f) == 0 && ok) ? VERB_OK : VERB_ERR_IO;
 }
+
+// ---------------------------------------------------------------------------
+// L* remapping (src/VERB4D_Solver.cpp:557-619).
+
+int verb_remap_L(verb_ctx* c, const double* new_L_host)
+{
+    if (!c || !new_L_host) return VERB_ERR_ARG;
+    for (int fid : {VERB_F_PSD, VERB_F_L}) {
+        int s = need_field(c, fid);
+        if (s) return s;
+    }
+    if (c->upd[VERB_F_L]) return VERB_ERR_ARG;
+    const size_t bytes = npts(c) * sizeof(double);
+    double *newL = nullptr, *scratch = nullptr;
+    CK(cudaMalloc(&newL, bytes));
+    int s = cuda_ok(cudaMalloc(&scratch, 2 * bytes));
+    if (!s) s = cuda_ok(cudaMemcpyAsync(newL, new_L_host, bytes, cudaMemcpyHostToDevice, c->stream));
+    if (!s) {
+        launch_remap(c->f[VERB_F_PSD], c->f[VERB_F_L], newL, scratch, scratch + npts(c), c->d,
+                     c->status, c->stream);
+        c->acc.kernel_launches++;
+        s = check_launch();
+    }
+    if (!s) s = cuda_ok(cudaMemcpyAsync(c->f[VERB_F_L], newL, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    if (!s) s = cuda_ok(cudaStreamSynchronize(c->stream));
+    cudaFree(newL);
+    cudaFree(scratch);
+    if (s) return s;
+    mark_dirty(c, VERB_F_L);
+    return verb_sync(c);
+}

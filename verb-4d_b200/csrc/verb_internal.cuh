@@ -119,6 +119,10 @@ struct MergeArgs {
     const double* axis[4];   // grid coordinates of every point
 };
 void launch_merge_components(double* out, const MergeArgs& m, size_t n, cudaStream_t s);
+// PSD lines interpolated from the old L* grid to the new one (scratch D, O: one
+// field each); the result is copied into psd
+void launch_remap(double* psd, const double* oldL, const double* newL, double* D, double* O,
+                  const Dims& d, int* status, cudaStream_t s);
 
 // Monotone mapping of doubles to unsigned 64-bit keys (for atomicMin on doubles).
 __host__ __device__ __forceinline__ unsigned long long dkey(double v)

@@ -67,6 +67,7 @@ SIGNATURES = {
     "verb_set_bc_types": (C.c_int, [_vp, _ip]),
     "verb_set_options": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int]),
     "verb_invalidate_lu": (C.c_int, [_vp]),
+    "verb_remap_L": (C.c_int, [_vp, _dp]),
     "verb_write_field_pltb": (C.c_int, [_vp, C.c_int, C.c_char_p, C.c_int]),
     "verb_output_wait": (C.c_int, [_vp]),
     "verb_read_field_pltb": (C.c_int, [_vp, C.c_int, C.c_char_p]),

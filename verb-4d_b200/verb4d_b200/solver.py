@@ -65,6 +65,11 @@ class Context:
         m = {"fp64": L.VERB_PREC_FP64, "mixed": L.VERB_PREC_MIXED}[mode]
         L.check(self.lib.verb_set_local_precision(self.h, m, int(refinements)), "precision")
 
+    def remap_L(self, new_L):
+        """Interpolate the PSD to a new L* grid and make it the L* field."""
+        a = np.ascontiguousarray(new_L, dtype=np.float64)
+        L.check(self.lib.verb_remap_L(self.h, a.ctypes.data_as(L._dp)), "remap_L")
+
     # ---- output and restart files (.pltb)
     def write_pltb(self, path: str, name: str = "psd", wait: bool = True):
         """Write a field as a .pltb file; with wait=False the write finishes in
