@@ -171,6 +171,14 @@ int verb_update_fields(verb_ctx* ctx, double current_time, unsigned int* updated
  * updated by the caller, as the reference's driver does (:563-565). */
 int verb_remap_L(verb_ctx* ctx, const double* new_L_host);
 
+/* Device bytes a context of this size will need once it has run a step
+ * (fields, boundary arrays, cached radial and local factors in the given
+ * precision, convection scratch, and Kalman-filter covariances of kf_columns
+ * columns).  Allocates nothing; used to admit ensemble members within an HBM
+ * budget.  No counterpart in the reference. */
+int verb_estimate_device_bytes(int P, int R, int V, int K, int precision, int refinements,
+                               long long kf_columns, size_t* bytes);
+
 /* ---- output and restart files ----------------------------------------------
  * .pltb files as the reference writes and reads them (Matrix4D::
  * writeToBinaryFile / readFromBinaryFile, src/Matrix.cpp:5700-5720,
@@ -228,7 +236,9 @@ int verb_local_factor_lapack(verb_ctx* ctx, int p, int r, double* ab_host, long*
  * p_index >= 0 restricts it the same way, -1 runs all P).  obs is a host
  * [P][R][V][K] array with NaN where there is no observation.  The analysis
  * covariances live on the device, initialised to 5*model_error*I on first use
- * (src/DataAssimilationDiffusion.cpp:212-218). */
+ * (src/DataAssimilationDiffusion.cpp:212-218).
+ * The covariances are held for the columns in use (one MLT for p_index >= 0,
+ * all for -1); later calls must pass the first call's p_index. */
 int verb_assimilate_radial(verb_ctx* ctx, const double* obs_host, double dt, double model_error,
                            double obs_error, int p_index);
 

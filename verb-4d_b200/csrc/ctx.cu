@@ -86,6 +86,7 @@ struct verb_ctx {
     double *Pa = nullptr, *kfwork = nullptr, *obs = nullptr;
     size_t kfwork_bytes = 0;
     int* kfticket = nullptr;
+    int pa_p_index = -2;  // the p_index Pa was sized for (-2: not yet)
     // updatable fields (nullptr: plain uploaded field)
     UpdField* upd[VERB_F_COUNT] = {};
     // asynchronous output: device snapshot -> pinned host copy on a copy
@@ -630,6 +631,13 @@ int verb_device_bytes(const verb_ctx* c, size_t* bytes)
     if (c->Lf32) b += ns * (c->klp32 + c->kvp32) * sizeof(float);
     if (c->ipiv) b += ns * (sizeof(double) + sizeof(int32_t));  // work vector and pivots
     if (c->lrhs) b += 2 * ns * sizeof(double);
+    if (c->conv_scratch)
+        b += (size_t)c->conv_nctas * conv_scratch_doubles(c->d.P, c->d.R) * sizeof(double);
+    if (c->Pa)
+        b += (size_t)(c->pa_p_index >= 0 ? 1 : c->d.P) * c->d.V * c->d.K * c->d.R * c->d.R *
+             sizeof(double);
+    if (c->obs) b += ns * sizeof(double);
+    b += c->kfwork_bytes;
     *bytes = b;
     return VERB_OK;
 }
@@ -1130,10 +1138,15 @@ int verb_assimilate_radial(verb_ctx* c, const double* obs_host, double dt, doubl
         int s = need_bc(c, b);
         if (s) return s;
     }
-    const size_t cols = (size_t)d.P * d.V * d.K, RR = (size_t)d.R * d.R;
+    // covariances of the columns in use: one MLT (the reference's P index,
+    // src/DataAssimilationDiffusion.cpp:116,139) or all of them
+    if (p_index < -1 || p_index >= d.P) return VERB_ERR_ARG;
+    if (c->Pa && p_index != c->pa_p_index) return VERB_ERR_ARG;
+    const size_t cols = (size_t)(p_index >= 0 ? 1 : d.P) * d.V * d.K, RR = (size_t)d.R * d.R;
     if (!c->Pa) {
         CK(cudaMalloc(&c->Pa, cols * RR * sizeof(double)));
         CK(cudaMemsetAsync(c->Pa, 0, cols * RR * sizeof(double), c->stream));
+        c->pa_p_index = p_index;
     }
     CK(alloc((void**)&c->obs, npts(c) * sizeof(double)));
     CK(cudaMemcpyAsync(c->obs, obs_host, npts(c) * sizeof(double), cudaMemcpyHostToDevice,
@@ -1466,4 +1479,41 @@ int verb_remap_L(verb_ctx* c, const double* new_L_host)
     if (s) return s;
     mark_dirty(c, VERB_F_L);
     return verb_sync(c);
+}
+
+// ---------------------------------------------------------------------------
+// Device memory a context of the given size will hold (no allocation): the
+// fields and boundary arrays, the cached radial and local factors in the
+// chosen precision, the convection scratch and, with kf_columns > 0, the
+// Kalman-filter covariances of that many columns.  Used to admit ensemble
+// members within an HBM budget.
+int verb_estimate_device_bytes(int P, int R, int V, int K, int precision, int refinements,
+                               long long kf_columns, size_t* bytes)
+{
+    if (!bytes || P < 1 || R < 1 || V < 1 || K < 1) return VERB_ERR_ARG;
+    const size_t np = (size_t)P * R * V * K;
+    size_t b = (VERB_F_COUNT + 1) * np * sizeof(double);                  // fields + D_LL base
+    b += (2 * (size_t)R * V * K + 4 * (size_t)P * V * K + 2 * (size_t)P * R * K +
+          2 * (size_t)P * R * V) * sizeof(double);                          // boundary arrays
+    b += 3 * np * sizeof(double);                                           // radial factors
+    if (V >= 3 && K >= 3) {
+        const int kl = V + 1, kv = 2 * kl;
+        if (precision == VERB_PREC_MIXED)
+            b += np * ((size_t)((kl + 3) & ~3) + ((kv + 4) & ~3)) * sizeof(float);
+        else
+            b += np * ((size_t)((kl + 1) & ~1) + ((kv + 2) & ~1)) * sizeof(double);
+        b += np * (sizeof(double) + sizeof(int32_t));                       // work, pivots
+        if (refinements > 0) b += 2 * np * sizeof(double);
+    }
+    if (P >= 3 || R >= 3) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        b += (size_t)2 * sms * conv_scratch_doubles(P, R) * sizeof(double);
+    }
+    if (kf_columns > 0)
+        b += ((size_t)kf_columns * R * R + np) * sizeof(double) +
+             (size_t)2 * 148 * 5 * R * R * sizeof(double);
+    *bytes = b;
+    return VERB_OK;
 }

@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(KF_THREADS) kf_kernel(KFArgs a)
         if (col >= ncols) break;
         const size_t p = a.p_index >= 0 ? (size_t)a.p_index : (size_t)col / VK;
         const size_t vk = a.p_index >= 0 ? (size_t)col : (size_t)col % VK;
-        const size_t cid = p * VK + vk;
+        const size_t cid = a.p_index >= 0 ? vk : p * VK + vk;  // Pa holds the columns in use
         double* Pa = a.Pa + cid * RR;
         auto gi = [&](int r) { return (p * d.R + r) * VK + vk; };
 
