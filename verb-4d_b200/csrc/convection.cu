@@ -1110,7 +1110,7 @@ int conv_ctas(int P, int R)
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const size_t smem = conv_smem_bytes(P, R);
-    cudaFuncSetAttribute(convection_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    allow_max_dynamic_smem((const void*)convection_kernel);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, convection_kernel, C3_THREADS, smem);
     if (per < 1) per = 1;
     return sms * per;
@@ -1119,7 +1119,7 @@ int conv_ctas(int P, int R)
 void launch_convection(const ConvArgs& a, int nctas, cudaStream_t s)
 {
     const size_t smem = conv_smem_bytes(a.d.P, a.d.R);
-    cudaFuncSetAttribute(convection_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    allow_max_dynamic_smem((const void*)convection_kernel);
     convection_kernel<<<nctas, C3_THREADS, smem, s>>>(a);
 }
 
@@ -1127,8 +1127,7 @@ void launch_convection_line(double* psd, const double* x, int n, double lbc, dou
                             int ubc_t, const double* ux, double dt, int* status, cudaStream_t s)
 {
     const size_t smem = (size_t)(4 * n + 32) * sizeof(double);
-    cudaFuncSetAttribute(convection_line_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem);
+    allow_max_dynamic_smem((const void*)convection_line_kernel);
     convection_line_kernel<<<1, CONV_THREADS, smem, s>>>(psd, x, n, lbc, ubc, lbc_t, ubc_t, ux, dt,
                                                         status);
 }

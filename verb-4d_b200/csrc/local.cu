@@ -631,12 +631,10 @@ void launch_local_factor(const LocalArgs& a, cudaStream_t s)
 {
     const size_t smem = local_factor_smem(a.d.V);
     if (a.factors32) {
-        cudaFuncSetAttribute(local_factor_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
+        allow_max_dynamic_smem((const void*)local_factor_kernel<float>);
         local_factor_kernel<float><<<a.d.P * a.d.R, FACT_THREADS, smem, s>>>(a);
     } else {
-        cudaFuncSetAttribute(local_factor_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
+        allow_max_dynamic_smem((const void*)local_factor_kernel<double>);
         local_factor_kernel<double><<<a.d.P * a.d.R, FACT_THREADS, smem, s>>>(a);
     }
 }
@@ -661,15 +659,13 @@ void launch_local_solve(const LocalArgs& a, cudaStream_t s)
         const size_t smem = (size_t)SOLVE_WARPS *
                             (BWD_WIN + solve_ring_doubles(a.klp32, a.kvp32, sizeof(float))) *
                             sizeof(double);
-        cudaFuncSetAttribute(local_solve_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
+        allow_max_dynamic_smem((const void*)local_solve_kernel<float>);
         local_solve_kernel<float><<<grid, SOLVE_WARPS * 32, smem, s>>>(a, nsys);
     } else {
         const size_t smem = (size_t)SOLVE_WARPS *
                             (BWD_WIN + solve_ring_doubles(a.klp, a.kvp, sizeof(double))) *
                             sizeof(double);
-        cudaFuncSetAttribute(local_solve_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
+        allow_max_dynamic_smem((const void*)local_solve_kernel<double>);
         local_solve_kernel<double><<<grid, SOLVE_WARPS * 32, smem, s>>>(a, nsys);
     }
 }

@@ -4,9 +4,30 @@
 //  * max(PSD, 1e-21)        (src/VERB4D_Solver.cpp:621, 980, 1072, 1219)
 //  * field = base * scale   (UpdatableMatrix scale queue, src/UpdatableMatrix.cpp:698-708)
 // Grid-stride loops sized to a multiple of the SM count; one atomic per block.
+#include <mutex>
+#include <set>
+#include <utility>
+
 #include "verb_internal.cuh"
 
 namespace verb {
+
+void allow_max_dynamic_smem(const void* func)
+{
+    static std::mutex mu;
+    static std::set<std::pair<const void*, int>> done;
+    int dev = 0, maxsm = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if (done.count({func, dev})) return;
+    cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, func) != cudaSuccess) return;
+    // the limit counts dynamic shared memory on top of the kernel's static part
+    const int dyn = maxsm - (int)fa.sharedSizeBytes;
+    if (cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) == cudaSuccess)
+        done.insert({func, dev});
+}
 
 namespace {
 

@@ -9,6 +9,12 @@
 
 namespace verb {
 
+// Raise a kernel's dynamic shared-memory limit to the device maximum, once per
+// (kernel, device).  The attribute belongs to the function, not to a launch,
+// so setting it per launch to that launch's size would race when contexts of
+// different sizes are driven from different host threads (ensembles).
+void allow_max_dynamic_smem(const void* func);
+
 struct Dims {
     int P, R, V, K;
     __host__ __device__ size_t npts() const { return (size_t)P * R * V * K; }
