@@ -147,6 +147,8 @@ def run_ours(args):
         sv = Solver(wl, stream=stream.cuda_stream, velocity_provider=None)
         sv.load()
         sv.ctx.set_local_precision(form, args.refine if form == "mixed" else 0)
+        if args.trim:
+            sv.ctx.set_local_trim(W.loss_cone_k0(wl))
         return sv
 
     solver = make_solver(args.form)
@@ -230,6 +232,8 @@ def run_ours(args):
         sv = Solver(wl, stream=stream.cuda_stream, velocity_provider=None)
         sv.load()
         sv.ctx.set_local_precision("fp64", 3)
+        if args.trim:
+            sv.ctx.set_local_trim(W.loss_cone_k0(wl))
         update_dev(1, sv)
         sv.ctx.step(wl.dt, wl.sub_dt, fl["run_convection"], fl["run_radial"], fl["run_local"])
         p64r = sv.ctx.download()
@@ -274,6 +278,8 @@ def run_ours(args):
         s2 = Solver(wl, stream=stream.cuda_stream, velocity_provider=host_provider)
         s2.load()
         s2.ctx.set_local_precision(args.form, args.refine if args.form == "mixed" else 0)
+        if args.trim:
+            s2.ctx.set_local_trim(W.loss_cone_k0(wl))
         h2d = sum(np.asarray(v).nbytes for k, v in wl.fields.items() if k != "DLL")
         d2h = 0
         for it in range(1, args.steps + 1):
@@ -330,6 +336,7 @@ def run_ours(args):
                                f"(P,R,V,K)={spec.shape}, dt=5 min, hourly Kp in [1,6]",
                    "P_mlt": P, "R_L": R, "V_energy": V, "K_alpha": K, "dt_min": 5,
                    "parallelism": f"replicas{world}",
+                   "local_systems": "loss-cone trimmed (ragged)" if args.trim else "full",
                    "l2": "inputs larger than L2 (110 GB of LU factors streamed per step)"},
         "phases_ms_per_step": {"convection": round(conv_ms, 3),
                                "radial": round(tm["radial_ms"] / args.steps, 3),
@@ -559,6 +566,8 @@ def main():
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"],
                     help="local solve: FP64 factors, or FP32 factors with FP64 refinement")
     ap.add_argument("--refine", type=int, default=2, help="refinement steps of the mixed form")
+    ap.add_argument("--trim", action="store_true",
+                    help="ragged local systems: pitch angles outside the loss cone only")
     ap.add_argument("--ensemble", action="store_true", help="run the member ensemble instead")
     ap.add_argument("--members", type=int, default=64)
     ap.add_argument("--ens-steps", type=int, default=12)

@@ -126,6 +126,15 @@ int verb_invalidate_lu(verb_ctx* ctx);
 #define VERB_PREC_FP64 0
 #define VERB_PREC_MIXED 1
 int verb_set_local_precision(verb_ctx* ctx, int mode, int refinements);
+/* Ragged local systems (the batched form of the loss-cone trimmed local
+ * diffusion; no counterpart in the reference): system (p, r), index p*R + r,
+ * keeps pitch-angle indices k0[p*R + r] .. K-1 and is the Diffusion_2D system
+ * of that sub-grid (src/Diffusion_2D.cpp:19-153) with a ConstantValue 0
+ * boundary at its lower pitch-angle edge; PSD below the edge is left as it
+ * is, and systems with fewer than 3 pitch angles are not solved.  Factor
+ * storage shrinks with the trimmed unknowns.  nullptr restores full systems.
+ * Local pivots / LAPACK-layout factors are not available while trimmed. */
+int verb_set_local_trim(verb_ctx* ctx, const int* k0_host);
 /* max |d| / max |x| of the last refinement step of the last verb_local()
  * (0 without refinement). */
 int verb_local_refinement(verb_ctx* ctx, double* rel_correction);

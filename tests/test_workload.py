@@ -48,3 +48,14 @@ def test_convection_substeps_cfg1():
 def test_kp_series():
     k = W.kp_series(3, 24)
     assert k.shape == (24,) and k.min() >= 1 and k.max() <= 6
+
+
+def test_loss_cone_rows():
+    wl = W.make_workload(W.CONFIGS["cfg1"], seed=41)
+    k0 = W.loss_cone_k0(wl)
+    K = wl.spec.K
+    kept = K - k0[0]
+    assert kept[0] == 0                       # L = 1: everything in the loss cone
+    assert kept[-1] >= K - 1                  # L = 6.6: alpha_lc ~ 0.4 deg
+    assert np.all(np.diff(kept) >= 0)
+    assert abs(W.loss_cone_deg(2.0) - 8.08) < 0.01

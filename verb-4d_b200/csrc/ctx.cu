@@ -69,6 +69,11 @@ struct verb_ctx {
     int klp32 = 0, kvp32 = 0;
     double *lrhs = nullptr, *lres = nullptr;
     unsigned long long* refine_red = nullptr;  // max |last correction|, max |x|
+    // ragged (trimmed) local systems: first pitch-angle index per (P,R)
+    // system and the first unknown of each system
+    int* trim_k0 = nullptr;
+    long long* trim_uoff = nullptr;
+    size_t local_unknowns = 0;  // unknowns of all systems (trimmed or full)
     bool local_dirty = true;
     double local_dt = -1;
     const double* dkv_override = nullptr;  // Dyx for the per-slice entry point
@@ -304,21 +309,22 @@ int local_prepare(verb_ctx* c, LocalArgs& a, double dts)
     c->kvp = (c->kv + 2) & ~1;
     c->klp32 = (c->kl + 3) & ~3;  // 16-byte columns for cp.async
     c->kvp32 = (c->kv + 4) & ~3;
-    const size_t nsys = (size_t)d.P * d.R, n = (size_t)d.V * d.K;
+    const size_t nu = c->trim_k0 ? c->local_unknowns : (size_t)d.P * d.R * d.V * d.K;
+    c->local_unknowns = nu;
     if (c->refine_iters > 0) {
-        CK(alloc((void**)&c->lrhs, nsys * n * sizeof(double)));
-        CK(alloc((void**)&c->lres, nsys * n * sizeof(double)));
+        CK(alloc((void**)&c->lrhs, nu * sizeof(double)));
+        CK(alloc((void**)&c->lres, nu * sizeof(double)));
         CK(alloc((void**)&c->refine_red, 2 * sizeof(unsigned long long)));
     }
     if (c->local_prec == VERB_PREC_MIXED) {
-        CK(alloc((void**)&c->Lf32, nsys * n * c->klp32 * sizeof(float)));
-        CK(alloc((void**)&c->Uf32, nsys * n * c->kvp32 * sizeof(float)));
+        CK(alloc((void**)&c->Lf32, nu * c->klp32 * sizeof(float)));
+        CK(alloc((void**)&c->Uf32, nu * c->kvp32 * sizeof(float)));
     } else {
-        CK(alloc((void**)&c->Lf, nsys * n * c->klp * sizeof(double)));
-        CK(alloc((void**)&c->Uf, nsys * n * c->kvp * sizeof(double)));
+        CK(alloc((void**)&c->Lf, nu * c->klp * sizeof(double)));
+        CK(alloc((void**)&c->Uf, nu * c->kvp * sizeof(double)));
     }
-    CK(alloc((void**)&c->ipiv, nsys * n * sizeof(int32_t)));
-    CK(alloc((void**)&c->lwork, nsys * n * sizeof(double)));
+    CK(alloc((void**)&c->ipiv, nu * sizeof(int32_t)));
+    CK(alloc((void**)&c->lwork, nu * sizeof(double)));
     a.d = d;
     a.psd = c->f[VERB_F_PSD];
     a.Vg = c->f[VERB_F_V];
@@ -353,6 +359,8 @@ int local_prepare(verb_ctx* c, LocalArgs& a, double dts)
     a.Lf32 = c->Lf32;
     a.Uf32 = c->Uf32;
     a.ipiv = c->ipiv;
+    a.k0 = c->trim_k0;
+    a.uoff = c->trim_uoff;
     a.work = c->lwork;
     a.status = c->status;
     return VERB_OK;
@@ -361,11 +369,11 @@ int local_prepare(verb_ctx* c, LocalArgs& a, double dts)
 int local_factor(verb_ctx* c, LocalArgs& a)
 {
     PhaseTimer t(c, PH_LOCF);
-    const size_t nsys = (size_t)c->d.P * c->d.R, n = (size_t)c->d.V * c->d.K;
+    const size_t nu = c->local_unknowns;
     if (a.factors32)
-        CK(cudaMemsetAsync(c->Uf32, 0, nsys * n * c->kvp32 * sizeof(float), c->stream));
+        CK(cudaMemsetAsync(c->Uf32, 0, nu * c->kvp32 * sizeof(float), c->stream));
     else
-        CK(cudaMemsetAsync(c->Uf, 0, nsys * n * c->kvp * sizeof(double), c->stream));
+        CK(cudaMemsetAsync(c->Uf, 0, nu * c->kvp * sizeof(double), c->stream));
     launch_local_factor(a, c->stream);
     c->acc.kernel_launches++;
     c->local_dirty = false;
@@ -390,7 +398,7 @@ int local_run(verb_ctx* c, double dt, double sub_dt)
         if (s) return s;
     }
     const bool refine = c->refine_iters > 0;
-    const size_t nall = (size_t)d.P * d.R * d.V * d.K;
+    const size_t nall = c->local_unknowns;
     for (int k = 0; k < nsub; k++) {
         launch_local_rhs(a, k > 0, c->stream);
         c->acc.kernel_launches++;
@@ -599,7 +607,7 @@ int verb_destroy(verb_ctx* c)
     }
     for (int i = 0; i < VERB_BCF_COUNT; i++) cudaFree(c->bc[i]);
     for (void* p : {(void*)c->Lf32, (void*)c->Uf32, (void*)c->lrhs, (void*)c->lres,
-                    (void*)c->refine_red})
+                    (void*)c->refine_red, (void*)c->trim_k0, (void*)c->trim_uoff})
         cudaFree(p);
     for (void* p : {(void*)c->rfa, (void*)c->rfbet, (void*)c->rfgam, (void*)c->Lf, (void*)c->Uf,
                     (void*)c->lwork, (void*)c->ipiv, (void*)c->conv_scratch,
@@ -626,7 +634,7 @@ int verb_device_bytes(const verb_ctx* c, size_t* bytes)
     for (int i = 0; i < VERB_BCF_COUNT; i++)
         if (c->bc[i]) b += bc_elems(c, i) * sizeof(double);
     if (c->rfa) b += 3 * F;
-    const size_t ns = (size_t)c->d.P * c->d.R * c->d.V * c->d.K;
+    const size_t ns = c->local_unknowns;
     if (c->Lf) b += ns * (c->klp + c->kvp) * sizeof(double);
     if (c->Lf32) b += ns * (c->klp32 + c->kvp32) * sizeof(float);
     if (c->ipiv) b += ns * (sizeof(double) + sizeof(int32_t));  // work vector and pivots
@@ -636,7 +644,7 @@ int verb_device_bytes(const verb_ctx* c, size_t* bytes)
     if (c->Pa)
         b += (size_t)(c->pa_p_index >= 0 ? 1 : c->d.P) * c->d.V * c->d.K * c->d.R * c->d.R *
              sizeof(double);
-    if (c->obs) b += ns * sizeof(double);
+    if (c->obs) b += npts(c) * sizeof(double);
     b += c->kfwork_bytes;
     *bytes = b;
     return VERB_OK;
@@ -924,7 +932,7 @@ int verb_convection_substeps(verb_ctx* c, int* host)
 
 int verb_local_pivots(verb_ctx* c, int32_t* host)
 {
-    if (!c || !host || !c->ipiv) return VERB_ERR_ARG;
+    if (!c || !host || !c->ipiv || c->trim_k0) return VERB_ERR_ARG;
     CK(cudaMemcpyAsync(host, c->ipiv, c->d.npts() * sizeof(int32_t), cudaMemcpyDeviceToHost,
                        c->stream));
     CK(cudaStreamSynchronize(c->stream));
@@ -933,7 +941,8 @@ int verb_local_pivots(verb_ctx* c, int32_t* host)
 
 int verb_local_factor_lapack(verb_ctx* c, int p, int r, double* ab, long* ipiv1)
 {
-    if (!c || !c->Lf || p < 0 || r < 0 || p >= c->d.P || r >= c->d.R) return VERB_ERR_ARG;
+    if (!c || !c->Lf || c->trim_k0 || p < 0 || r < 0 || p >= c->d.P || r >= c->d.R)
+        return VERB_ERR_ARG;
     const int n = c->d.V * c->d.K, kl = c->kl, kv = c->kv, ldab = 2 * kl + kl + 1;
     const size_t sys = (size_t)p * c->d.R + r;
     std::vector<double> L((size_t)n * c->klp), U((size_t)n * c->kvp);
@@ -1515,5 +1524,46 @@ int verb_estimate_device_bytes(int P, int R, int V, int K, int precision, int re
         b += ((size_t)kf_columns * R * R + np) * sizeof(double) +
              (size_t)2 * 148 * 5 * R * R * sizeof(double);
     *bytes = b;
+    return VERB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Ragged local systems: each (P,R) system keeps pitch-angle indices
+// k0[sys]..K-1 (the trapped range outside the loss cone), with a
+// ConstantValue 0 boundary at its new lower edge.  Systems with fewer than 3
+// pitch angles left are not solved.  Passing nullptr restores full systems.
+int verb_set_local_trim(verb_ctx* c, const int* k0_host)
+{
+    if (!c) return VERB_ERR_ARG;
+    const Dims& d = c->d;
+    const size_t nsys = (size_t)d.P * d.R;
+    CK(cudaStreamSynchronize(c->stream));
+    // the factor arrays change size: release them (refactored at the next solve)
+    for (void** p : {(void**)&c->Lf, (void**)&c->Uf, (void**)&c->Lf32, (void**)&c->Uf32,
+                     (void**)&c->ipiv, (void**)&c->lwork, (void**)&c->lrhs, (void**)&c->lres}) {
+        cudaFree(*p);
+        *p = nullptr;
+    }
+    cudaFree(c->trim_k0);
+    cudaFree(c->trim_uoff);
+    c->trim_k0 = nullptr;
+    c->trim_uoff = nullptr;
+    c->local_dirty = true;
+    if (!k0_host) {
+        c->local_unknowns = nsys * d.V * d.K;
+        return VERB_OK;
+    }
+    std::vector<long long> off(nsys);
+    long long tot = 0;
+    for (size_t s = 0; s < nsys; s++) {
+        if (k0_host[s] < 0 || k0_host[s] > d.K) return VERB_ERR_ARG;
+        off[s] = tot;
+        tot += (long long)d.V * (d.K - k0_host[s]);
+    }
+    CK(cudaMalloc(&c->trim_k0, nsys * sizeof(int)));
+    CK(cudaMalloc(&c->trim_uoff, nsys * sizeof(long long)));
+    CK(cudaMemcpy(c->trim_k0, k0_host, nsys * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(c->trim_uoff, off.data(), nsys * sizeof(long long), cudaMemcpyHostToDevice));
+    c->local_unknowns = (size_t)tot;
     return VERB_OK;
 }

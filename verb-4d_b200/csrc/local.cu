@@ -41,13 +41,23 @@ __device__ __forceinline__ int dslot(int dx, int dy) { return (dy + 1) * 3 + (dx
 struct SysView {
     const double *x, *y, *Dxx, *Dyy, *Dxy, *Dyx, *G, *S, *loss;
     const double *xl, *xu, *yl, *yu;
-    int nx, ny;
+    int nx, ny;      // logical grid of the system (ny = K - k0)
+    int ld;          // stride of the V index in the [V][K] fields (K)
+    bool trimmed;    // lower K edge is the loss-cone edge (ConstantValue 0)
 };
+
+__device__ __forceinline__ int sys_k0(const LocalArgs& a, int sys) { return a.k0 ? a.k0[sys] : 0; }
+
+// first unknown of system sys in the work / pivot arrays
+__device__ __forceinline__ size_t sys_uoff(const LocalArgs& a, int sys)
+{
+    return a.uoff ? (size_t)a.uoff[sys] : (size_t)sys * a.d.V * a.d.K;
+}
 
 __device__ __forceinline__ SysView sys_view(const LocalArgs& a, int sys)
 {
-    const size_t n = (size_t)a.d.V * a.d.K;
-    const size_t base = (size_t)sys * n;
+    const int k0 = sys_k0(a, sys);
+    const size_t base = (size_t)sys * a.d.V * a.d.K + k0;
     SysView v;
     v.x = a.Vg + base;
     v.y = a.Kg + base;
@@ -58,12 +68,14 @@ __device__ __forceinline__ SysView sys_view(const LocalArgs& a, int sys)
     v.G = a.G + base;
     v.S = a.S + base;
     v.loss = a.loss + base;
-    v.xl = a.Vl + (size_t)sys * a.d.K;
-    v.xu = a.Vu + (size_t)sys * a.d.K;
+    v.xl = a.Vl + (size_t)sys * a.d.K + k0;
+    v.xu = a.Vu + (size_t)sys * a.d.K + k0;
     v.yl = a.Kl + (size_t)sys * a.d.V;
     v.yu = a.Ku + (size_t)sys * a.d.V;
     v.nx = a.d.V;
-    v.ny = a.d.K;
+    v.ny = a.d.K - k0;
+    v.ld = a.d.K;
+    v.trimmed = k0 > 0;
     return v;
 }
 
@@ -72,8 +84,8 @@ __device__ __forceinline__ SysView sys_view(const LocalArgs& a, int sys)
 __device__ __forceinline__ void sda2(double* r, const SysView& v, int ix, int iy, int dx1, int dy1,
                                      int dx2, int dy2, const double* D, double mult)
 {
-    const int ny = v.ny;
-#define P2(a, b) ((a) * ny + (b))
+    const int ld = v.ld;
+#define P2(a, b) ((a) * ld + (b))
     const double x0 = v.x[P2(ix, iy)] + v.y[P2(ix, iy)];
     const double x1 = v.x[P2(ix + dx1, iy + dy1)] + v.y[P2(ix + dx1, iy + dy1)];
     const double x2 = v.x[P2(ix + dx2, iy + dy2)] + v.y[P2(ix + dx2, iy + dy2)];
@@ -94,9 +106,9 @@ __device__ __forceinline__ void sda2(double* r, const SysView& v, int ix, int iy
 // One row of matr_A (src/Diffusion_2D.cpp:68-130).  Returns 0 or VERB_ERR_BC.
 __device__ int assemble_row(const SysView& v, int types[4], double dt, int in, double r[9])
 {
-    const int nx = v.nx, ny = v.ny;
+    const int nx = v.nx, ny = v.ny, ld = v.ld;
     const int ix = in % nx, iy = in / nx;
-    const int p = ix * ny + iy;
+    const int p = ix * ld + iy;
 #pragma unroll
     for (int s = 0; s < 9; s++) r[s] = 0.0;
     int t = -1, s1 = 0;
@@ -104,13 +116,13 @@ __device__ int assemble_row(const SysView& v, int types[4], double dt, int in, d
     if (ix == 0 && nx >= 3) {
         t = types[0];
         s1 = dslot(1, 0);
-        dh = v.x[p + ny] - v.x[p];
+        dh = v.x[p + ld] - v.x[p];
     } else if (ix == nx - 1 && nx >= 3) {
         t = types[1];
         s1 = dslot(-1, 0);
-        dh = v.x[p] - v.x[p - ny];
+        dh = v.x[p] - v.x[p - ld];
     } else if (iy == 0 && ny >= 3) {
-        t = types[2];
+        t = v.trimmed ? VERB_BC_CONSTANT_VALUE : types[2];
         s1 = dslot(0, 1);
         dh = v.y[p + 1] - v.y[p];
     } else if (iy == ny - 1 && ny >= 3) {
@@ -155,6 +167,7 @@ __device__ int assemble_row(const SysView& v, int types[4], double dt, int in, d
 
 __device__ __forceinline__ bool skip_system(const LocalArgs& a, int sys)
 {
+    if (a.k0 && a.d.K - a.k0[sys] < 3) return true;  // trimmed below a solvable grid
     if (a.include_boundary) return false;
     const int r = sys % a.d.R;
     return r == 0 || r == a.d.R - 1;
@@ -173,7 +186,8 @@ __global__ void __launch_bounds__(FACT_THREADS) local_factor_kernel(LocalArgs a)
     const int sys = blockIdx.x;
     if (skip_system(a, sys)) return;
     const int nx = a.d.V;
-    const int n = a.d.V * a.d.K;
+    const int n = a.d.V * (a.d.K - sys_k0(a, sys));
+    const size_t u0 = sys_uoff(a, sys);
     const int kl = a.kl, ku = a.kl, kv = a.kv;
     const int RW = kl + 1;          // window rows
     const int CW = kv + 1;          // window columns (row pitch)
@@ -187,9 +201,9 @@ __global__ void __launch_bounds__(FACT_THREADS) local_factor_kernel(LocalArgs a)
     int types[4] = {a.Vl_t, a.Vu_t, a.Kl_t, a.Ku_t};
     const bool f32 = sizeof(T) == sizeof(float);
     const int klp = f32 ? a.klp32 : a.klp, kvp = f32 ? a.kvp32 : a.kvp;
-    T* Lf = (f32 ? (T*)a.Lf32 : (T*)a.Lf) + (size_t)sys * n * klp;
-    T* Uf = (f32 ? (T*)a.Uf32 : (T*)a.Uf) + (size_t)sys * n * kvp;
-    int32_t* ip = a.ipiv + (size_t)sys * n;
+    T* Lf = (f32 ? (T*)a.Lf32 : (T*)a.Lf) + u0 * klp;
+    T* Uf = (f32 ? (T*)a.Uf32 : (T*)a.Uf) + u0 * kvp;
+    int32_t* ip = a.ipiv + u0;
     const int tid = threadIdx.x;
 
     auto stage_rows = [&](int q0) {
@@ -329,9 +343,9 @@ __global__ void local_rhs_kernel(LocalArgs a, int from_work)
     const int sys = blockIdx.z;
     if (skip_system(a, sys)) return;
     const int V = a.d.V, K = a.d.K;
-    const size_t n = (size_t)V * K;
-    const double* psd = a.psd + (size_t)sys * n;
-    double* w = a.work + (size_t)sys * n;
+    const int kz = sys_k0(a, sys), ny = K - kz;  // unknowns: pitch-angle indices kz..K-1
+    const double* psd = a.psd + (size_t)sys * V * K;
+    double* w = a.work + sys_uoff(a, sys);
     const int v0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
     if (!from_work) {
@@ -342,7 +356,7 @@ __global__ void local_rhs_kernel(LocalArgs a, int from_work)
     } else {
         for (int r = ty; r < 32; r += 8) {
             const int ik = k0 + r, iv = v0 + tx;
-            if (iv < V && ik < K) tile[tx][r] = w[(size_t)ik * V + iv];
+            if (iv < V && ik >= kz && ik < K) tile[tx][r] = w[(size_t)(ik - kz) * V + iv];
         }
     }
     __syncthreads();
@@ -351,8 +365,8 @@ __global__ void local_rhs_kernel(LocalArgs a, int from_work)
     const double ls = (double)a.local_sources;
     for (int r = ty; r < 32; r += 8) {
         const int ik = k0 + r, iv = v0 + tx;
-        if (iv >= V || ik >= K) continue;
-        const int ix = iv, iy = ik;
+        if (iv >= V || ik >= K || ik < kz) continue;
+        const int ix = iv, iy = ik - kz;
         double b, c;
         if (ix == 0 && V >= 3) {
             b = 0.0;
@@ -360,10 +374,10 @@ __global__ void local_rhs_kernel(LocalArgs a, int from_work)
         } else if (ix == V - 1 && V >= 3) {
             b = 0.0;
             c = sv.xu[iy];
-        } else if (iy == 0 && K >= 3) {
+        } else if (iy == 0 && ny >= 3) {
             b = 0.0;
-            c = sv.yl[ix];
-        } else if (iy == K - 1 && K >= 3) {
+            c = sv.trimmed ? 0.0 : sv.yl[ix];
+        } else if (iy == ny - 1 && ny >= 3) {
             b = 0.0;
             c = sv.yu[ix];
         } else {
@@ -374,7 +388,7 @@ __global__ void local_rhs_kernel(LocalArgs a, int from_work)
         double rhs = tile[tx][r];
         rhs *= b;
         rhs += c;
-        w[(size_t)ik * V + iv] = rhs;
+        w[(size_t)iy * V + iv] = rhs;
     }
 }
 
@@ -384,19 +398,19 @@ __global__ void local_store_kernel(LocalArgs a)
     const int sys = blockIdx.z;
     if (skip_system(a, sys)) return;
     const int V = a.d.V, K = a.d.K;
-    const size_t n = (size_t)V * K;
-    double* psd = a.psd + (size_t)sys * n;
-    const double* w = a.work + (size_t)sys * n;
+    const int kz = sys_k0(a, sys);
+    double* psd = a.psd + (size_t)sys * V * K;
+    const double* w = a.work + sys_uoff(a, sys);
     const int v0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
     for (int r = ty; r < 32; r += 8) {
         const int ik = k0 + r, iv = v0 + tx;
-        if (iv < V && ik < K) tile[tx][r] = w[(size_t)ik * V + iv];
+        if (iv < V && ik >= kz && ik < K) tile[tx][r] = w[(size_t)(ik - kz) * V + iv];
     }
     __syncthreads();
     for (int r = ty; r < 32; r += 8) {
         const int iv = v0 + r, ik = k0 + tx;
-        if (iv < V && ik < K) psd[(size_t)iv * K + ik] = tile[r][tx];
+        if (iv < V && ik >= kz && ik < K) psd[(size_t)iv * K + ik] = tile[r][tx];
     }
 }
 
@@ -439,17 +453,18 @@ __global__ void __launch_bounds__(SOLVE_WARPS * 32) local_solve_kernel(LocalArgs
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int sys = blockIdx.x * SOLVE_WARPS + warp;
     if (sys >= nsys || skip_system(a, sys)) return;
-    const int n = a.d.V * a.d.K;
+    const int n = a.d.V * (a.d.K - sys_k0(a, sys));
+    const size_t u0 = sys_uoff(a, sys);
     const bool f32 = sizeof(T) == sizeof(float);
     const int kl = a.kl, kv = a.kv, klp = f32 ? a.klp32 : a.klp, kvp = f32 ? a.kvp32 : a.kvp;
     constexpr int VEC = 16 / sizeof(T);  // elements per 16-byte cp.async
     const size_t per_warp = BWD_WIN + solve_ring_doubles(klp, kvp, sizeof(T));
     double* win = sm + (size_t)warp * per_warp;
     T* ring = (T*)(win + BWD_WIN);
-    double* w = a.work + (size_t)sys * n;
-    const T* Lf = (f32 ? (const T*)a.Lf32 : (const T*)a.Lf) + (size_t)sys * n * klp;
-    const T* Uf = (f32 ? (const T*)a.Uf32 : (const T*)a.Uf) + (size_t)sys * n * kvp;
-    const int32_t* ip = a.ipiv + (size_t)sys * n;
+    double* w = a.work + u0;
+    const T* Lf = (f32 ? (const T*)a.Lf32 : (const T*)a.Lf) + u0 * klp;
+    const T* Uf = (f32 ? (const T*)a.Uf32 : (const T*)a.Uf) + u0 * kvp;
+    const int32_t* ip = a.ipiv + u0;
 
     // ---------------- forward: L with interleaved row interchanges (xGBTRS) --------
     for (int i = lane; i < FWD_WIN && i < n; i += 32) win[i] = w[i];
@@ -556,10 +571,10 @@ __global__ void local_residual_kernel(LocalArgs a, const double* b, const double
     const int sys = blockIdx.y;
     if (skip_system(a, sys)) return;
     const int nx = a.d.V;
-    const int n = a.d.V * a.d.K;
+    const int n = a.d.V * (a.d.K - sys_k0(a, sys));
     const SysView v = sys_view(a, sys);
     int types[4] = {a.Vl_t, a.Vu_t, a.Kl_t, a.Ku_t};
-    const size_t base = (size_t)sys * n;
+    const size_t base = sys_uoff(a, sys);
     for (int in = blockIdx.x * blockDim.x + threadIdx.x; in < n; in += gridDim.x * blockDim.x) {
         double row[9];
         const int st = assemble_row(v, types, a.dt, in, row);
@@ -577,18 +592,19 @@ __global__ void local_residual_kernel(LocalArgs a, const double* b, const double
     }
 }
 
-// x += d over all systems; red[0] = max |d|, red[1] = max |x| as dkey values.
-__global__ void local_update_kernel(LocalArgs a, double* x, const double* d, size_t total,
-                                    unsigned long long* red)
+// x += d over every system (blockIdx.y); red[0] = max |d|, red[1] = max |x|
+// as dkey values.
+__global__ void local_update_kernel(LocalArgs a, double* x, const double* d, unsigned long long* red)
 {
-    const size_t n = (size_t)a.d.V * a.d.K;
+    const int sys = blockIdx.y;
+    if (skip_system(a, sys)) return;
+    const int n = a.d.V * (a.d.K - sys_k0(a, sys));
+    const size_t base = sys_uoff(a, sys);
     double md = 0.0, mx = 0.0;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-         i += (size_t)gridDim.x * blockDim.x) {
-        if (skip_system(a, (int)(i / n))) continue;
-        const double v = x[i] + d[i];
-        x[i] = v;
-        md = fmax(md, fabs(d[i]));
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const double v = x[base + i] + d[base + i];
+        x[base + i] = v;
+        md = fmax(md, fabs(d[base + i]));
         mx = fmax(mx, fabs(v));
     }
     for (int o = 16; o > 0; o >>= 1) {
@@ -614,11 +630,9 @@ void launch_local_residual(const LocalArgs& a, const double* b, const double* x,
 void launch_local_update(const LocalArgs& a, double* x, const double* d, unsigned long long* red,
                          cudaStream_t s)
 {
-    const size_t total = (size_t)a.d.P * a.d.R * a.d.V * a.d.K;
-    int dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    local_update_kernel<<<sms * 8, 256, 0, s>>>(a, x, d, total, red);
+    const int n = a.d.V * a.d.K;
+    dim3 grid((n + 255) / 256, a.d.P * a.d.R);
+    local_update_kernel<<<grid, 256, 0, s>>>(a, x, d, red);
 }
 
 size_t local_factor_smem(int V)

@@ -87,6 +87,11 @@ struct LocalArgs {
     int factors32, klp32, kvp32;
     float* Lf32;
     float* Uf32;
+    // ragged (trimmed) systems: system s keeps pitch-angle indices k0[s]..K-1
+    // (unknowns V*(K-k0[s]) from offset uoff[s]); the new lower K edge is a
+    // ConstantValue 0 boundary.  nullptr: every system is the full V*K grid.
+    const int* k0;
+    const long long* uoff;
     int32_t* ipiv;      // [sys][n]        0-based pivot rows
     double* work;       // [sys][n]        rhs / solution in unknown order (iK*V + iV)
     unsigned long long* negatives;  // optional: count of PSD < 0 written by the store kernel
@@ -103,6 +108,7 @@ void launch_local_residual(const LocalArgs& a, const double* b, const double* x,
 // x += d; red[0] = max |d|, red[1] = max |x| (dkey-ordered, atomicMax)
 void launch_local_update(const LocalArgs& a, double* x, const double* d, unsigned long long* red,
                          cudaStream_t s);
+// unknowns of all systems (V*K*P*R, or the sum over trimmed systems)
 
 // --- reductions / elementwise ---------------------------------------------------
 void launch_negative_count(const double* psd, size_t n, unsigned long long* out, cudaStream_t s);

@@ -68,6 +68,7 @@ SIGNATURES = {
     "verb_set_options": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int]),
     "verb_invalidate_lu": (C.c_int, [_vp]),
     "verb_remap_L": (C.c_int, [_vp, _dp]),
+    "verb_set_local_trim": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "verb_estimate_device_bytes": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                              C.c_longlong, C.POINTER(C.c_size_t)]),
     "verb_write_field_pltb": (C.c_int, [_vp, C.c_int, C.c_char_p, C.c_int]),

@@ -65,6 +65,15 @@ class Context:
         m = {"fp64": L.VERB_PREC_FP64, "mixed": L.VERB_PREC_MIXED}[mode]
         L.check(self.lib.verb_set_local_precision(self.h, m, int(refinements)), "precision")
 
+    def set_local_trim(self, k0=None):
+        """Ragged local systems: k0[p, r] is the first pitch-angle index kept
+        for system (p, r) (None: full systems)."""
+        if k0 is None:
+            L.check(self.lib.verb_set_local_trim(self.h, None), "trim")
+            return
+        a = np.ascontiguousarray(k0, dtype=np.int32).ravel()
+        L.check(self.lib.verb_set_local_trim(self.h, a.ctypes.data_as(C.POINTER(C.c_int))), "trim")
+
     def remap_L(self, new_L):
         """Interpolate the PSD to a new L* grid and make it the L* field."""
         a = np.ascontiguousarray(new_L, dtype=np.float64)

@@ -197,6 +197,26 @@ def make_workload(spec: GridSpec, seed: int = 1, kp: float | np.ndarray = 3.0,
     return wl
 
 
+def loss_cone_deg(L):
+    """Equatorial bounce loss cone of a dipole, alpha_lc(L) =
+    asin(sqrt(1 / (L^5 sqrt(4 - 3/L)))), in degrees."""
+    L = np.asarray(L, dtype=np.float64)
+    return np.rad2deg(np.arcsin(np.sqrt(1.0 / (L ** 5 * np.sqrt(4.0 - 3.0 / L)))))
+
+
+def loss_cone_k0(wl: Workload) -> np.ndarray:
+    """First pitch-angle index outside the loss cone for every (MLT, L)
+    system, [P][R] int32: the trimmed (ragged) local systems keep K indices
+    k0..K-1."""
+    f = wl.fields
+    L = f["Lg"][:, :, 0, 0]
+    alpha = np.rad2deg(f["Kg"][:, :, 0, :])  # [P][R][K]
+    lc = loss_cone_deg(L)[:, :, None]
+    keep = alpha > lc
+    k0 = np.where(keep.any(axis=2), keep.argmax(axis=2), alpha.shape[2])
+    return k0.astype(np.int32)
+
+
 def oracle_inputs(wl: Workload) -> dict:
     d = dict(wl.fields)
     d["bc_types"] = wl.bc_types
