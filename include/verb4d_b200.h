@@ -188,6 +188,70 @@ int verb_remap_L(verb_ctx* ctx, const double* new_L_host);
 int verb_estimate_device_bytes(int P, int R, int V, int K, int precision, int refinements,
                                long long kf_columns, size_t* bytes);
 
+/* ---- learned warm start -----------------------------------------------------
+ * A small CNN of 3x3 convolutions (zero padding, ReLU between layers, FP16
+ * weights, FP32 accumulation) with hand-written forward, backward and Adam
+ * kernels.  It is trained on (coefficient fields, right-hand side, solution)
+ * triples of the local (V,K) systems and gives the warm start of their
+ * Krylov solve (verb_local_krylov).  No counterpart in the reference.
+ * channels[0..layers] are the channel counts (input first); images are
+ * H x W; tensors are device NCHW FP32.  Parameters are ordered layer by
+ * layer: weights [Cout][Cin][3][3], then bias [Cout]. */
+typedef struct verb_cnn verb_cnn;
+int verb_cnn_create(verb_cnn** out, int layers, const int* channels, int H, int W, int max_batch,
+                    void* stream);
+int verb_cnn_destroy(verb_cnn* cnn);
+int verb_cnn_param_count(const verb_cnn* cnn, long long* count);
+int verb_cnn_set_params(verb_cnn* cnn, const float* host);
+/* grad_host (may be NULL) receives the gradients of the last training step */
+int verb_cnn_get_params(verb_cnn* cnn, float* host, float* grad_host);
+int verb_cnn_forward(verb_cnn* cnn, const float* in_dev, float* out_dev, int batch);
+/* MSE loss against target_dev, backward pass, Adam step (lr <= 0: gradients only) */
+int verb_cnn_train_step(verb_cnn* cnn, const float* in_dev, const float* target_dev, int batch,
+                        float lr, float* loss_host);
+
+/* ---- Krylov form of the local (V,K) solve ----------------------------------
+ * verb_local_krylov takes the same local step as verb_local but solves each
+ * (P,R) system by iterative refinement in FP64 around an FP32 BiCGSTAB with
+ * a Jacobi (diagonal) preconditioner, one CTA per system, starting from
+ * x0 = 0 (VERB_GUESS_ZERO), x0 = f (VERB_GUESS_PREV: the state the step
+ * starts from) or the CNN's prediction x0 = f + max|f| * cnn(features)
+ * (VERB_GUESS_CNN), followed by `smooth` weighted-Jacobi sweeps
+ * x += omega (b - A x) / diag(A) in FP64.  Each outer pass forms r = b - A x in FP64, solves
+ * A d = r to inner_tol in FP32 (at most inner_maxit iterations) and adds d.
+ * A system is done when max|b - A x| / max|b| <= resid_tol; systems still
+ * above it after max_outer passes, or whose residual a pass did not reduce
+ * at least tenfold, are solved by the banded LU (factorised
+ * for those systems only; the factors are allocated on first use) so the
+ * step is always accurate to the residual tolerance or exact.  The features
+ * are [sys][4][K][V] FP32: (log10 D_VV - m)/2, (log10 D_KK - m)/2 with
+ * m = log10(0.864), D_VK / sqrt(D_VV D_KK) and f / max|f|; the network's
+ * output is the step's relative increment (x - f) / max|f| on the same grid.
+ * (The system's right-hand side is not a guess: its interior rows are
+ * scaled by 1/dt.)  The CNN form needs untrimmed systems.  No counterpart in
+ * the reference (its local step is the LU). */
+#define VERB_GUESS_ZERO 0
+#define VERB_GUESS_PREV 1
+#define VERB_GUESS_CNN 2
+typedef struct {
+    long long systems;           /* systems solved (per sub-step, summed) */
+    long long fallbacks;         /* systems finished by the LU */
+    long long inner_iterations;  /* BiCGSTAB iterations over all systems */
+    long long solved_iterations; /* ... over the systems the Krylov solve finished */
+    long long outer_passes;      /* refinement passes taken (max over sub-steps, summed) */
+    double max_rel_residual;     /* largest max|b-Ax|/max|b| before the fallback */
+    double guess_rel_residual;   /* largest relative residual of the initial guess */
+} verb_krylov_stats;
+int verb_local_krylov(verb_ctx* ctx, double dt, double sub_dt, int guess, verb_cnn* cnn,
+                      int smooth, double omega, int max_outer, int inner_maxit, double inner_tol,
+                      double resid_tol, verb_krylov_stats* stats);
+/* One local step by the LU (as verb_local, without refinement) that also
+ * writes, for the last sub-step, the CNN features of every system
+ * (feat_dev, [P*R][4][K][V] floats) and the training target
+ * (target_dev, [P*R][K][V] floats, (x - f) / max|f|).  Untrimmed systems only;
+ * skipped (boundary) systems are left unwritten. */
+int verb_local_triples(verb_ctx* ctx, double dt, double sub_dt, float* feat_dev, float* target_dev);
+
 /* ---- output and restart files ----------------------------------------------
  * .pltb files as the reference writes and reads them (Matrix4D::
  * writeToBinaryFile / readFromBinaryFile, src/Matrix.cpp:5700-5720,

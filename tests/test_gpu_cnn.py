@@ -1,0 +1,52 @@
+"""The warm-start CNN's CUDA kernels against the CPU restatement
+(oracle/cnn_ref.py): forward pass and the gradients of one training step
+(FP32 device sums against float64 ones, checked norm-wise at 1e-4), and a few
+Adam steps that reduce the loss of a fixed batch."""
+import numpy as np
+import pytest
+
+import cnn_ref as R
+from verb4d_b200.learned import CNN
+
+pytestmark = pytest.mark.gpu
+CH = (4, 8, 8, 1)
+
+
+def test_forward_and_gradients_match_cpu(gpu):
+    import torch
+
+    rng = np.random.default_rng(0)
+    B, H, W = 3, 9, 7
+    net = CNN(H, W, B, channels=CH, seed=1)
+    p = net.params()
+    x = rng.standard_normal((B, 4, H, W)).astype(np.float32)
+    t = rng.standard_normal((B, 1, H, W)).astype(np.float32)
+    xd = torch.from_numpy(x).cuda()
+    td = torch.from_numpy(t).cuda()
+    out = torch.zeros((B, 1, H, W), device="cuda")
+    net.forward(xd.data_ptr(), out.data_ptr(), B)
+    torch.cuda.synchronize()
+    acts = R.forward(p.astype(np.float64), CH, x.astype(np.float64))
+    ref = acts[-1]
+    assert np.abs(out.cpu().numpy() - ref).max() <= 1e-5 * np.abs(ref).max()
+    loss = net.train_step(xd.data_ptr(), td.data_ptr(), B, 0.0)   # gradients only
+    _, g = net.params(with_grad=True)
+    rloss, rg = R.gradients(p.astype(np.float64), CH, x.astype(np.float64), t.astype(np.float64))
+    assert abs(loss - rloss) <= 1e-5 * rloss
+    assert np.abs(g - rg).max() <= 1e-4 * np.abs(rg).max()
+    net.close()
+
+
+def test_adam_reduces_loss(gpu):
+    import torch
+
+    rng = np.random.default_rng(2)
+    B, H, W = 8, 11, 11
+    net = CNN(H, W, B, channels=CH, seed=3)
+    x = torch.from_numpy(rng.standard_normal((B, 4, H, W)).astype(np.float32)).cuda()
+    t = torch.from_numpy(rng.standard_normal((B, 1, H, W)).astype(np.float32)).cuda()
+    first = net.train_step(x.data_ptr(), t.data_ptr(), B, 1e-2)
+    for _ in range(200):
+        last = net.train_step(x.data_ptr(), t.data_ptr(), B, 1e-2)
+    assert last < 0.5 * first
+    net.close()

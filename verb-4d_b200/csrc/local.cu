@@ -167,6 +167,7 @@ __device__ int assemble_row(const SysView& v, int types[4], double dt, int in, d
 
 __device__ __forceinline__ bool skip_system(const LocalArgs& a, int sys)
 {
+    if (a.sel && !(a.sel[sys] & a.sel_mask)) return true;
     if (a.k0 && a.d.K - a.k0[sys] < 3) return true;  // trimmed below a solvable grid
     if (a.include_boundary) return false;
     const int r = sys % a.d.R;
@@ -617,6 +618,307 @@ __global__ void local_update_kernel(LocalArgs a, double* x, const double* d, uns
     }
 }
 
+// ---------------------------------------------------------------------------
+// Krylov form of the local solve (learned warm start).
+
+__global__ void local_assemble32_kernel(LocalArgs a, float* A9)
+{
+    const int sys = blockIdx.y;
+    if (skip_system(a, sys)) return;
+    const int n = a.d.V * (a.d.K - sys_k0(a, sys));
+    const SysView v = sys_view(a, sys);
+    int types[4] = {a.Vl_t, a.Vu_t, a.Kl_t, a.Ku_t};
+    float* A = A9 + sys_uoff(a, sys) * 9;
+    for (int in = blockIdx.x * blockDim.x + threadIdx.x; in < n; in += gridDim.x * blockDim.x) {
+        double row[9];
+        const int st = assemble_row(v, types, a.dt, in, row);
+        if (st) set_error(a.status, st);
+#pragma unroll
+        for (int k = 0; k < 9; k++) A[(size_t)k * n + in] = (float)row[k];
+    }
+}
+
+// block-wide sum of v (all threads get the result); red has 32 floats
+__device__ __forceinline__ float block_sum(float v, float* red)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    __syncthreads();
+    if (l == 0) red[w] = v;
+    __syncthreads();
+    float t = l < nw ? red[l] : 0.f;
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    return t;
+}
+
+__device__ __forceinline__ float mv_row(const float* A, const float* y, int n, int nx, int i)
+{
+    float acc = 0.f;
+#pragma unroll
+    for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+        for (int dx = -1; dx <= 1; dx++) {
+            const int col = i + dy * nx + dx;
+            const float m = A[(size_t)((dy + 1) * 3 + (dx + 1)) * n + i];
+            if (m != 0.f && col >= 0 && col < n) acc = fmaf(m, y[col], acc);
+        }
+    return acc;
+}
+
+// One CTA per system.  Right preconditioning with M = diag(A) (Jacobi):
+// van der Vorst's BiCGSTAB on A M^-1 u = r, d = M^-1 u accumulated directly.
+__global__ void bicgstab_kernel(LocalArgs a, const float* A9, const double* rr, double* dd,
+                                float* scratch, int maxit, float tol, int* iters, unsigned char* ok)
+{
+    __shared__ float red[32];
+    const int sys = blockIdx.x;
+    if (skip_system(a, sys)) return;
+    const int nx = a.d.V;
+    const int n = a.d.V * (a.d.K - sys_k0(a, sys));
+    const size_t u0 = sys_uoff(a, sys);
+    const float* A = A9 + u0 * 9;
+    const float* dg = A + (size_t)4 * n;
+    float* r = scratch + u0 * 6;
+    float* rh = r + n;
+    float* p = rh + n;
+    float* v = p + n;
+    float* y = v + n;  // y, then z
+    float* t = y + n;
+    double* d = dd + u0;
+    const double* b = rr + u0;
+    float bn = 0.f;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const float bi = (float)b[i];
+        r[i] = bi;
+        rh[i] = bi;
+        p[i] = 0.f;
+        v[i] = 0.f;
+        d[i] = 0.0;
+        bn = fmaf(bi, bi, bn);
+    }
+    bn = sqrtf(block_sum(bn, red));
+    float rho = 1.f, alpha = 1.f, omega = 1.f;
+    int it = 0;
+    bool conv = bn == 0.f;
+    while (!conv && it < maxit) {
+        it++;
+        float rho1 = 0.f;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) rho1 = fmaf(rh[i], r[i], rho1);
+        rho1 = block_sum(rho1, red);
+        if (rho1 == 0.f || !isfinite(rho1)) break;
+        const float beta = (rho1 / rho) * (alpha / omega);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            p[i] = r[i] + beta * (p[i] - omega * v[i]);
+            y[i] = p[i] / dg[i];
+        }
+        __syncthreads();
+        float rv = 0.f;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const float vi = mv_row(A, y, n, nx, i);
+            v[i] = vi;
+            rv = fmaf(rh[i], vi, rv);
+        }
+        rv = block_sum(rv, red);
+        if (rv == 0.f || !isfinite(rv)) break;
+        alpha = rho1 / rv;
+        float sn = 0.f;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            d[i] += (double)(alpha * y[i]);
+            const float si = r[i] - alpha * v[i];
+            r[i] = si;  // r now holds s
+            sn = fmaf(si, si, sn);
+        }
+        sn = sqrtf(block_sum(sn, red));
+        if (sn <= tol * bn) {
+            conv = true;
+            break;
+        }
+        for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = r[i] / dg[i];  // z
+        __syncthreads();
+        float ts = 0.f, tt = 0.f;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const float ti = mv_row(A, y, n, nx, i);
+            t[i] = ti;
+            ts = fmaf(ti, r[i], ts);
+            tt = fmaf(ti, ti, tt);
+        }
+        ts = block_sum(ts, red);
+        tt = block_sum(tt, red);
+        if (tt == 0.f || !isfinite(tt)) break;
+        omega = ts / tt;
+        float rn = 0.f;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            d[i] += (double)(omega * y[i]);
+            const float ri = r[i] - omega * t[i];
+            r[i] = ri;
+            rn = fmaf(ri, ri, rn);
+        }
+        rn = sqrtf(block_sum(rn, red));
+        if (rn <= tol * bn) conv = true;
+        if (omega == 0.f) break;
+        rho = rho1;
+    }
+    if (threadIdx.x == 0) {
+        iters[sys] += it;
+        if (ok) ok[sys] = conv ? 1 : 0;
+    }
+}
+
+// the PSD of every system in the unknown order (the state the step starts from)
+__global__ void gather_state_kernel(LocalArgs a, double* x)
+{
+    const int sys = blockIdx.y;
+    if (skip_system(a, sys)) return;
+    const int V = a.d.V, K = a.d.K, kz = sys_k0(a, sys), n = V * (K - kz);
+    const size_t u0 = sys_uoff(a, sys);
+    const double* f = a.psd + (size_t)sys * V * K + kz;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int iy = i / V, iv = i - iy * V;
+        x[u0 + i] = f[(size_t)iv * K + iy];
+    }
+}
+
+// features [sys][4][K'][V] over the system's pitch-angle rows (K' = K - k0);
+// f is the state the step starts from (unknown order)
+__global__ void local_features_kernel(LocalArgs a, const double* fstate, float* feat, double* scale)
+{
+    __shared__ float red[32];
+    const int sys = blockIdx.x;
+    if (skip_system(a, sys)) return;
+    const int V = a.d.V, K = a.d.K, kz = sys_k0(a, sys), ny = K - kz;
+    const int n = V * ny;
+    const size_t u0 = sys_uoff(a, sys);
+    const double* b = fstate + u0;
+    float m = 0.f;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmaxf(m, fabsf((float)b[i]));
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float t = 0.f;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t = fmaxf(t, red[w]);
+        red[0] = t > 0.f ? t : 1.f;
+    }
+    __syncthreads();
+    const float sc = red[0];
+    if (threadIdx.x == 0) scale[sys] = sc;
+    const size_t fb = (size_t)sys * V * K;  // field slab [V][K]
+    const float med = log10f(1e-5f * 86400.f);
+    float* f = feat + u0 * 4;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const int iy = i / V, iv = i - iy * V;
+        const size_t g = fb + (size_t)iv * K + kz + iy;
+        const float dvv = (float)a.DVV[g], dkk = (float)a.DKK[g], dvk = (float)a.DVK[g];
+        f[i] = (log10f(dvv) - med) * 0.5f;
+        f[(size_t)n + i] = (log10f(dkk) - med) * 0.5f;
+        f[(size_t)2 * n + i] = dvk / sqrtf(dvv * dkk);
+        f[(size_t)3 * n + i] = (float)b[i] / sc;
+    }
+}
+
+__global__ void warm_start_kernel(LocalArgs a, const double* b, const float* out, const double* scale,
+                                  double* x)
+{
+    const int sys = blockIdx.y;
+    if (skip_system(a, sys)) return;
+    const int n = a.d.V * (a.d.K - sys_k0(a, sys));
+    const size_t u0 = sys_uoff(a, sys);
+    const double s = scale[sys];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        x[u0 + i] = out ? b[u0 + i] + (double)out[u0 + i] * s : b[u0 + i];
+}
+
+__global__ void local_targets_kernel(LocalArgs a, const double* b, const double* x, const double* scale,
+                                     float* target)
+{
+    const int sys = blockIdx.y;
+    if (skip_system(a, sys)) return;
+    const int n = a.d.V * (a.d.K - sys_k0(a, sys));
+    const size_t u0 = sys_uoff(a, sys);
+    const double s = scale[sys];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        target[u0 + i] = (float)((x[u0 + i] - b[u0 + i]) / s);
+}
+
+__global__ void residual_check_kernel(LocalArgs a, const double* b, const double* x, double tol,
+                                      double stall, double* prev, unsigned char* pend,
+                                      unsigned int* cnt, unsigned long long* maxkey)
+{
+    __shared__ double rmax[32], bmax[32];
+    const int sys = blockIdx.x;
+    if (skip_system(a, sys)) return;
+    const int nx = a.d.V;
+    const int n = a.d.V * (a.d.K - sys_k0(a, sys));
+    const SysView v = sys_view(a, sys);
+    int types[4] = {a.Vl_t, a.Vu_t, a.Kl_t, a.Ku_t};
+    const size_t base = sys_uoff(a, sys);
+    double mr = 0.0, mb = 0.0;
+    for (int in = threadIdx.x; in < n; in += blockDim.x) {
+        double row[9];
+        assemble_row(v, types, a.dt, in, row);
+        double acc = b[base + in];
+        for (int dy = -1; dy <= 1; dy++)
+            for (int dx = -1; dx <= 1; dx++) {
+                const double m = row[dslot(dx, dy)];
+                const int col = in + dy * nx + dx;
+                if (m != 0.0 && col >= 0 && col < n) acc -= m * x[base + col];
+            }
+        mr = fmax(mr, fabs(acc));
+        mb = fmax(mb, fabs(b[base + in]));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+        mb = fmax(mb, __shfl_xor_sync(0xffffffffu, mb, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        rmax[threadIdx.x >> 5] = mr;
+        bmax[threadIdx.x >> 5] = mb;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double R = 0, Bm = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+            R = fmax(R, rmax[w]);
+            Bm = fmax(Bm, bmax[w]);
+        }
+        const double rel = Bm > 0 ? R / Bm : R;
+        const bool nan = !(rel == rel);
+        unsigned char st = 0;
+        if (!(rel <= tol)) {
+            const double p = prev[sys];
+            st = (nan || (p > 0 && rel > stall * p)) ? 2 : 1;
+            atomicAdd(&cnt[st - 1], 1u);
+        }
+        pend[sys] = st;
+        prev[sys] = nan ? 1e300 : rel;
+        atomicMax(maxkey, dkey(nan ? 1e300 : rel));
+    }
+}
+
+// weighted Jacobi sweep on the guess: x += omega * r / diag(A) (r = b - A x)
+__global__ void jacobi_update_kernel(LocalArgs a, const float* A9, const double* r, double* x,
+                                     double omega)
+{
+    const int sys = blockIdx.y;
+    if (skip_system(a, sys)) return;
+    const int n = a.d.V * (a.d.K - sys_k0(a, sys));
+    const size_t u0 = sys_uoff(a, sys);
+    const float* dg = A9 + u0 * 9 + (size_t)4 * n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        x[u0 + i] += omega * r[u0 + i] / (double)dg[i];
+}
+
+__global__ void masked_copy_kernel(LocalArgs a, double* x, const double* y)
+{
+    const int sys = blockIdx.y;
+    if (skip_system(a, sys)) return;  // a.sel selects the systems to copy
+    const int n = a.d.V * (a.d.K - sys_k0(a, sys));
+    const size_t u0 = sys_uoff(a, sys);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        x[u0 + i] = y[u0 + i];
+}
+
 }  // namespace
 
 void launch_local_residual(const LocalArgs& a, const double* b, const double* x, double* r,
@@ -633,6 +935,65 @@ void launch_local_update(const LocalArgs& a, double* x, const double* d, unsigne
     const int n = a.d.V * a.d.K;
     dim3 grid((n + 255) / 256, a.d.P * a.d.R);
     local_update_kernel<<<grid, 256, 0, s>>>(a, x, d, red);
+}
+
+void launch_local_assemble32(const LocalArgs& a, float* A9, cudaStream_t s)
+{
+    const int n = a.d.V * a.d.K;
+    local_assemble32_kernel<<<dim3((n + 255) / 256, a.d.P * a.d.R), 256, 0, s>>>(a, A9);
+}
+
+void launch_bicgstab(const LocalArgs& a, const float* A9, const double* r, double* d, float* scratch,
+                     int maxit, float tol, int* iters, unsigned char* ok, cudaStream_t s)
+{
+    bicgstab_kernel<<<a.d.P * a.d.R, 256, 0, s>>>(a, A9, r, d, scratch, maxit, tol, iters, ok);
+}
+
+void launch_gather_state(const LocalArgs& a, double* x, cudaStream_t s)
+{
+    const int n = a.d.V * a.d.K;
+    gather_state_kernel<<<dim3((n + 255) / 256, a.d.P * a.d.R), 256, 0, s>>>(a, x);
+}
+
+void launch_local_features(const LocalArgs& a, const double* f, float* feat, double* scale,
+                           cudaStream_t s)
+{
+    local_features_kernel<<<a.d.P * a.d.R, 256, 0, s>>>(a, f, feat, scale);
+}
+
+void launch_warm_start(const LocalArgs& a, const double* b, const float* out, const double* scale,
+                       double* x, cudaStream_t s)
+{
+    const int n = a.d.V * a.d.K;
+    warm_start_kernel<<<dim3((n + 255) / 256, a.d.P * a.d.R), 256, 0, s>>>(a, b, out, scale, x);
+}
+
+void launch_local_targets(const LocalArgs& a, const double* b, const double* x, const double* scale,
+                          float* target, cudaStream_t s)
+{
+    const int n = a.d.V * a.d.K;
+    local_targets_kernel<<<dim3((n + 255) / 256, a.d.P * a.d.R), 256, 0, s>>>(a, b, x, scale, target);
+}
+
+void launch_residual_check(const LocalArgs& a, const double* b, const double* x, double tol,
+                           double stall, double* prev, unsigned char* pend, unsigned int* cnt,
+                           unsigned long long* maxkey, cudaStream_t s)
+{
+    residual_check_kernel<<<a.d.P * a.d.R, 256, 0, s>>>(a, b, x, tol, stall, prev, pend, cnt,
+                                                         maxkey);
+}
+
+void launch_jacobi_update(const LocalArgs& a, const float* A9, const double* r, double* x,
+                          double omega, cudaStream_t s)
+{
+    const int n = a.d.V * a.d.K;
+    jacobi_update_kernel<<<dim3((n + 255) / 256, a.d.P * a.d.R), 256, 0, s>>>(a, A9, r, x, omega);
+}
+
+void launch_masked_copy(const LocalArgs& a, double* x, const double* y, cudaStream_t s)
+{
+    const int n = a.d.V * a.d.K;
+    masked_copy_kernel<<<dim3((n + 255) / 256, a.d.P * a.d.R), 256, 0, s>>>(a, x, y);
 }
 
 size_t local_factor_smem(int V)

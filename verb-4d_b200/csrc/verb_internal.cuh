@@ -92,6 +92,10 @@ struct LocalArgs {
     // ConstantValue 0 boundary.  nullptr: every system is the full V*K grid.
     const int* k0;
     const long long* uoff;
+    // optional per-system selection: only systems with (sel[sys] & sel_mask)
+    // != 0 are processed
+    const unsigned char* sel;
+    unsigned char sel_mask;
     int32_t* ipiv;      // [sys][n]        0-based pivot rows
     double* work;       // [sys][n]        rhs / solution in unknown order (iK*V + iV)
     unsigned long long* negatives;  // optional: count of PSD < 0 written by the store kernel
@@ -108,6 +112,42 @@ void launch_local_residual(const LocalArgs& a, const double* b, const double* x,
 // x += d; red[0] = max |d|, red[1] = max |x| (dkey-ordered, atomicMax)
 void launch_local_update(const LocalArgs& a, double* x, const double* d, unsigned long long* red,
                          cudaStream_t s);
+// ---- Krylov form of the local solve (learned warm start) -------------------
+// FP32 copy of every system's 9 diagonals, [sys][9][n] (slot (dy+1)*3+(dx+1))
+void launch_local_assemble32(const LocalArgs& a, float* A9, cudaStream_t s);
+// batched right-Jacobi-preconditioned BiCGSTAB in FP32: A d = r for every
+// selected system, d from 0; iters[sys] += iterations, ok[sys] = converged
+// (ok may be nullptr);
+// scratch: 6 vectors of n floats per system
+void launch_bicgstab(const LocalArgs& a, const float* A9, const double* r, double* d, float* scratch,
+                     int maxit, float tol, int* iters, unsigned char* ok, cudaStream_t s);
+// the PSD of every system in the unknown order
+void launch_gather_state(const LocalArgs& a, double* x, cudaStream_t s);
+// features of the state f (unknown order) for the warm-start CNN:
+// feat [sys][4][K][V] = (log10 D_VV - m)/2, (log10 D_KK - m)/2,
+// D_VK/sqrt(D_VV D_KK), f/max|f|; scale[sys] = max|f| (1 where f = 0)
+void launch_local_features(const LocalArgs& a, const double* f, float* feat, double* scale,
+                           cudaStream_t s);
+// warm start x = f + out * scale (out == nullptr: x = f)  /  target = (x - f) / scale
+void launch_warm_start(const LocalArgs& a, const double* b, const float* out, const double* scale,
+                       double* x, cudaStream_t s);
+void launch_local_targets(const LocalArgs& a, const double* b, const double* x, const double* scale,
+                          float* target, cudaStream_t s);
+// per system: rel = max|b - A x| / max|b| (FP64).  pend[sys] = 0 when
+// rel <= tol, 2 (give up: LU) when a previous rel is recorded and
+// rel > stall * prev, else 1; cnt[0] / cnt[1] count the 1s / 2s; prev[sys]
+// becomes rel; maxkey holds the largest rel (as a dkey)
+void launch_residual_check(const LocalArgs& a, const double* b, const double* x, double tol,
+                           double stall, double* prev, unsigned char* pend, unsigned int* cnt,
+                           unsigned long long* maxkey, cudaStream_t s);
+// forward pass of a warm-start network on stream s (cnn.cu)
+int cnn_forward_on(verb_cnn* n, const float* in, float* out, int B, cudaStream_t s);
+int cnn_shape(const verb_cnn* n, int* cin, int* cout, int* H, int* W, int* maxb);
+// weighted Jacobi sweep x += omega * r / diag (diag from the FP32 diagonals)
+void launch_jacobi_update(const LocalArgs& a, const float* A9, const double* r, double* x,
+                          double omega, cudaStream_t s);
+// x[sys] <- y[sys] for systems with sel[sys] != 0
+void launch_masked_copy(const LocalArgs& a, double* x, const double* y, cudaStream_t s);
 // unknowns of all systems (V*K*P*R, or the sum over trimmed systems)
 
 // --- reductions / elementwise ---------------------------------------------------

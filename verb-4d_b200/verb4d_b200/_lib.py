@@ -20,6 +20,15 @@ STATUS_NAMES = {
     5: "VERB_ERR_TENSOR", 6: "VERB_ERR_NAN", 7: "VERB_ERR_CUDA", 8: "VERB_ERR_NOMEM",
     9: "VERB_ERR_GRID", 10: "VERB_TIMEOUT", 11: "VERB_ERR_SIZE", 12: "VERB_ERR_IO",
 }
+VERB_GUESS_ZERO, VERB_GUESS_PREV, VERB_GUESS_CNN = 0, 1, 2
+GUESS_IDS = {"zero": VERB_GUESS_ZERO, "prev": VERB_GUESS_PREV, "cnn": VERB_GUESS_CNN}
+
+
+class KrylovStats(C.Structure):
+    _fields_ = [("systems", C.c_longlong), ("fallbacks", C.c_longlong),
+                ("inner_iterations", C.c_longlong), ("solved_iterations", C.c_longlong),
+                ("outer_passes", C.c_longlong),
+                ("max_rel_residual", C.c_double), ("guess_rel_residual", C.c_double)]
 
 # 4-D fields (verb_field)
 F_PSD, F_P, F_R, F_V, F_K, F_L, F_DLL, F_DVV, F_DKK, F_DVK, F_VP, F_VR, F_G_LOCAL, F_G_RADIAL, \
@@ -68,6 +77,17 @@ SIGNATURES = {
     "verb_set_options": (C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int]),
     "verb_invalidate_lu": (C.c_int, [_vp]),
     "verb_remap_L": (C.c_int, [_vp, _dp]),
+    "verb_cnn_create": (C.c_int, [C.POINTER(_vp), C.c_int, C.POINTER(C.c_int), C.c_int, C.c_int,
+                                  C.c_int, _vp]),
+    "verb_cnn_destroy": (C.c_int, [_vp]),
+    "verb_cnn_param_count": (C.c_int, [_vp, C.POINTER(C.c_longlong)]),
+    "verb_cnn_set_params": (C.c_int, [_vp, C.POINTER(C.c_float)]),
+    "verb_cnn_get_params": (C.c_int, [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "verb_cnn_forward": (C.c_int, [_vp, _vp, _vp, C.c_int]),
+    "verb_cnn_train_step": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_float, C.POINTER(C.c_float)]),
+    "verb_local_krylov": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, _vp, C.c_int,
+                                    C.c_double, C.c_int, C.c_int, C.c_double, C.c_double, _vp]),
+    "verb_local_triples": (C.c_int, [_vp, C.c_double, C.c_double, _vp, _vp]),
     "verb_set_local_trim": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "verb_estimate_device_bytes": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                              C.c_longlong, C.POINTER(C.c_size_t)]),

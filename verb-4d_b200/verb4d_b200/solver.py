@@ -74,6 +74,30 @@ class Context:
         a = np.ascontiguousarray(k0, dtype=np.int32).ravel()
         L.check(self.lib.verb_set_local_trim(self.h, a.ctypes.data_as(C.POINTER(C.c_int))), "trim")
 
+    def local_krylov(self, dt: float, sub_dt: float, guess: str = "prev", cnn=None,
+                     smooth: int = 0, omega: float = 2.0 / 3.0, max_outer: int = 10,
+                     inner_maxit: int = 100, inner_tol: float = 1e-3,
+                     resid_tol: float = 1e-10) -> dict:
+        """The local step solved by FP64-refined FP32 BiCGSTAB from the given
+        initial guess ("zero", "prev": the state the step starts from, or "cnn"
+        with a learned.CNN) after
+        `smooth` weighted-Jacobi sweeps, with the LU for systems that stay
+        above resid_tol.  Returns the solve stats."""
+        st = L.KrylovStats()
+        L.check(self.lib.verb_local_krylov(self.h, dt, sub_dt, L.GUESS_IDS[guess],
+                                           cnn.h if cnn is not None else None, smooth, omega,
+                                           max_outer, inner_maxit, inner_tol, resid_tol,
+                                           C.byref(st)),
+                "local_krylov")
+        return {k: getattr(st, k) for k, _ in L.KrylovStats._fields_}
+
+    def local_triples(self, dt: float, sub_dt: float, feat_ptr: int, target_ptr: int) -> None:
+        """A local LU step that writes the CNN features and targets of every
+        system into the device buffers at feat_ptr ([P*R][4][K][V] float32)
+        and target_ptr ([P*R][K][V] float32)."""
+        L.check(self.lib.verb_local_triples(self.h, dt, sub_dt, C.c_void_p(feat_ptr),
+                                            C.c_void_p(target_ptr)), "local_triples")
+
     def remap_L(self, new_L):
         """Interpolate the PSD to a new L* grid and make it the L* field."""
         a = np.ascontiguousarray(new_L, dtype=np.float64)
