@@ -59,3 +59,20 @@ def test_loss_cone_rows():
     assert kept[-1] >= K - 1                  # L = 6.6: alpha_lc ~ 0.4 deg
     assert np.all(np.diff(kept) >= 0)
     assert abs(W.loss_cone_deg(2.0) - 8.08) < 0.01
+
+
+def test_smooth_coefficients_option():
+    spec = W.CONFIGS["cfg1"]
+    a = W.make_workload(spec, seed=5)
+    b = W.make_workload(spec, seed=5, coeff_corr=0.0)
+    for k in ("DVV", "DKK", "DVK", "psd"):
+        assert np.array_equal(a.fields[k], b.fields[k])
+    c = W.make_workload(spec, seed=5, coeff_corr=4.0)
+    z = np.log10(c.fields["DVV"] / (1e-5 * 86400.0))
+    # unit variance per (MLT, L) slice, and far smoother along alpha than i.i.d. draws
+    assert np.allclose(z.std(axis=(2, 3)), 1.0, atol=1e-6)
+    rough = np.abs(np.diff(np.log10(a.fields["DVV"]), axis=3)).mean()
+    smooth = np.abs(np.diff(z, axis=3)).mean()
+    assert smooth < 0.3 * rough
+    r = c.fields["DVK"] / np.sqrt(c.fields["DVV"] * c.fields["DKK"])
+    assert np.all(np.abs(r) <= 0.99)

@@ -42,7 +42,8 @@ def features(dvv, dkk, dvk, state):
     return np.ascontiguousarray(out.transpose(0, 1, 3, 2)), scale
 
 
-def collect_triples(seeds, steps_per_seed: int, spec=None, sources=True, losses=True):
+def collect_triples(seeds, steps_per_seed: int, spec=None, sources=True, losses=True,
+                    coeff_corr: float = 0.0):
     """Run whole operator-split steps at `spec` (default 24 x 25 x 31 x 31)
     for each seed; the local part of every step is taken by the LU through
     verb_local_triples, which emits one (features, target) pair per (P,R)
@@ -58,7 +59,8 @@ def collect_triples(seeds, steps_per_seed: int, spec=None, sources=True, losses=
     targ = torch.empty((n, 1, spec.K, spec.V), dtype=torch.float32, device="cuda")
     i = 0
     for seed in seeds:
-        wl = W.make_workload(spec, seed=seed, sources=sources, losses=losses)
+        wl = W.make_workload(spec, seed=seed, sources=sources, losses=losses,
+                             coeff_corr=coeff_corr)
         s = Solver(wl)
         s.load()
         fl = wl.flags

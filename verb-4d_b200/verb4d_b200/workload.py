@@ -138,10 +138,25 @@ class Workload:
         return 10.0 ** (0.506 * (kp - self.dll_base_kp))
 
 
+def _smooth_ek(z: np.ndarray, corr: float) -> np.ndarray:
+    """Gaussian-filter a field of unit normals along (E, alpha) with a width of
+    `corr` grid points and rescale each (MLT, L) slice back to unit variance."""
+    from scipy.ndimage import gaussian_filter
+
+    out = gaussian_filter(z, sigma=(0, 0, corr, corr), mode="nearest")
+    sd = out.std(axis=(2, 3), keepdims=True)
+    return out / np.where(sd > 0, sd, 1.0)
+
+
 def make_workload(spec: GridSpec, seed: int = 1, kp: float | np.ndarray = 3.0,
-                  sources: bool = False, losses: bool = False) -> Workload:
+                  sources: bool = False, losses: bool = False,
+                  coeff_corr: float = 0.0) -> Workload:
     """Build every input field of one run.  `sources`/`losses` switch on small
-    seeded source and loss-rate fields (off in the benchmark configurations)."""
+    seeded source and loss-rate fields (off in the benchmark configurations).
+    The local diffusion coefficients are log-normal with independent values
+    at every grid point (coeff_corr = 0), or, with coeff_corr > 0, smooth in
+    (E, alpha) with that correlation width in grid points (same draws,
+    filtered), as wave-model coefficient tables are."""
     rng = np.random.default_rng(seed)
     mlt, L, logE, alpha = axes(spec)
     shp = spec.shape
@@ -158,9 +173,18 @@ def make_workload(spec: GridSpec, seed: int = 1, kp: float | np.ndarray = 3.0,
     dll_base = np.ascontiguousarray(np.broadcast_to(
         dll_brautigam_albert(L, 3.0)[None, :, None, None], shp))
     med = 1e-5 * _DAY
-    dvv = med * 10.0 ** rng.standard_normal(shp)
-    dkk = med * 10.0 ** rng.standard_normal(shp)
-    dvk = rng.uniform(-1.0, 1.0, shp) * 0.99 * np.sqrt(dvv * dkk)
+    zv = rng.standard_normal(shp)
+    zk = rng.standard_normal(shp)
+    u = rng.uniform(-1.0, 1.0, shp)
+    if coeff_corr > 0:
+        from scipy.special import erf
+
+        zv, zk = _smooth_ek(zv, coeff_corr), _smooth_ek(zk, coeff_corr)
+        # a smooth field uniform on (-1, 1) from a smoothed normal one
+        u = erf(_smooth_ek(rng.standard_normal(shp), coeff_corr) / np.sqrt(2.0))
+    dvv = med * 10.0 ** zv
+    dkk = med * 10.0 ** zk
+    dvk = u * 0.99 * np.sqrt(dvv * dkk)
     VP, VR = drift_velocities(spec, float(kps[0]))
     ones = np.ones(shp)
     zeros = np.zeros(shp)
