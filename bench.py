@@ -147,6 +147,7 @@ def run_ours(args):
         sv = Solver(wl, stream=stream.cuda_stream, velocity_provider=None)
         sv.load()
         sv.ctx.set_local_precision(form, args.refine if form == "mixed" else 0)
+        sv.ctx.set_convection_arith(args.conv)
         if args.trim:
             sv.ctx.set_local_trim(W.loss_cone_k0(wl))
         return sv
@@ -232,6 +233,7 @@ def run_ours(args):
         sv = Solver(wl, stream=stream.cuda_stream, velocity_provider=None)
         sv.load()
         sv.ctx.set_local_precision("fp64", 3)
+        sv.ctx.set_convection_arith(args.conv)
         if args.trim:
             sv.ctx.set_local_trim(W.loss_cone_k0(wl))
         update_dev(1, sv)
@@ -278,6 +280,7 @@ def run_ours(args):
         s2 = Solver(wl, stream=stream.cuda_stream, velocity_provider=host_provider)
         s2.load()
         s2.ctx.set_local_precision(args.form, args.refine if args.form == "mixed" else 0)
+        s2.ctx.set_convection_arith(args.conv)
         if args.trim:
             s2.ctx.set_local_trim(W.loss_cone_k0(wl))
         h2d = sum(np.asarray(v).nbytes for k, v in wl.fields.items() if k != "DLL")
@@ -337,6 +340,9 @@ def run_ours(args):
                    "P_mlt": P, "R_L": R, "V_energy": V, "K_alpha": K, "dt_min": 5,
                    "parallelism": f"replicas{world}",
                    "local_systems": "loss-cone trimmed (ragged)" if args.trim else "full",
+                   "convection_arith": ("fma: multiply-add contraction, within 1e-12 of the "
+                                        "reference per step" if args.conv == "fma" else
+                                        "exact: bit-identical to the reference"),
                    "l2": "inputs larger than L2 (110 GB of LU factors streamed per step)"},
         "phases_ms_per_step": {"convection": round(conv_ms, 3),
                                "radial": round(tm["radial_ms"] / args.steps, 3),
@@ -566,6 +572,8 @@ def main():
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"],
                     help="local solve: FP64 factors, or FP32 factors with FP64 refinement")
     ap.add_argument("--refine", type=int, default=2, help="refinement steps of the mixed form")
+    ap.add_argument("--conv", default="fma", choices=["fma", "exact"],
+                    help="convection arithmetic: fma (contracted) or exact (bit-identical)")
     ap.add_argument("--trim", action="store_true",
                     help="ragged local systems: pitch angles outside the loss cone only")
     ap.add_argument("--ensemble", action="store_true", help="run the member ensemble instead")

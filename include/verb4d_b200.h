@@ -210,6 +210,15 @@ int verb_cnn_forward(verb_cnn* cnn, const float* in_dev, float* out_dev, int bat
 int verb_cnn_train_step(verb_cnn* cnn, const float* in_dev, const float* target_dev, int batch,
                         float lr, float* loss_host);
 
+/* Convection arithmetic.  VERB_CONV_EXACT (the default) restates the
+ * reference's operations one by one without contraction, so results are
+ * bit-identical to it (exp() of loss rates aside).  VERB_CONV_FMA runs the
+ * same kernel compiled with multiply-add contraction: about 10 % faster, and
+ * within a few units in the last place of the exact form per step. */
+#define VERB_CONV_EXACT 0
+#define VERB_CONV_FMA 1
+int verb_set_convection_arith(verb_ctx* ctx, int mode);
+
 /* ---- Krylov form of the local (V,K) solve ----------------------------------
  * verb_local_krylov takes the same local step as verb_local but solves each
  * (P,R) system by iterative refinement in FP64 around an FP32 BiCGSTAB with

@@ -9,6 +9,7 @@
 #include <new>
 #include <string>
 #include <thread>
+#include <algorithm>
 #include <utility>
 #include <vector>
 
@@ -91,6 +92,7 @@ struct verb_ctx {
     int* conv_substeps = nullptr;
     int* ticket = nullptr;
     int conv_nctas = 0;
+    int conv_arith = VERB_CONV_EXACT;
     // reductions / status
     unsigned long long* red = nullptr;  // [0] negatives, [1] tensor min key
     int* status = nullptr;
@@ -699,7 +701,7 @@ int conv_run(verb_ctx* c, double dt)
         if (s) return s;
     }
     if (int s = conv_check(d.P, d.R)) return s;
-    if (!c->conv_nctas) c->conv_nctas = conv_ctas(d.P, d.R);
+    if (!c->conv_nctas) c->conv_nctas = std::max(conv_ctas(d.P, d.R), conv_ctas_fma(d.P, d.R));
     CK(alloc((void**)&c->conv_scratch,
              (size_t)c->conv_nctas * conv_scratch_doubles(d.P, d.R) * sizeof(double)));
     CK(alloc((void**)&c->conv_substeps, (size_t)d.V * d.K * sizeof(int)));
@@ -729,7 +731,10 @@ int conv_run(verb_ctx* c, double dt)
     a.status = c->status;
     PhaseTimer t(c, PH_CONV);
     CK(cudaMemsetAsync(c->ticket, 0, sizeof(int), c->stream));
-    launch_convection(a, c->conv_nctas, c->stream);
+    if (c->conv_arith == VERB_CONV_FMA)
+        launch_convection_fma(a, c->conv_nctas, c->stream);
+    else
+        launch_convection(a, c->conv_nctas, c->stream);
     c->acc.kernel_launches++;
     return check_launch();
 }
@@ -1083,6 +1088,13 @@ int verb_local(verb_ctx* c, double dt, double sub_dt)
 {
     if (!c || !(dt > 0) || !(sub_dt > 0)) return VERB_ERR_ARG;
     return local_run(c, dt, sub_dt);
+}
+
+int verb_set_convection_arith(verb_ctx* c, int mode)
+{
+    if (!c || (mode != VERB_CONV_EXACT && mode != VERB_CONV_FMA)) return VERB_ERR_ARG;
+    c->conv_arith = mode;
+    return VERB_OK;
 }
 
 int verb_local_krylov(verb_ctx* c, double dt, double sub_dt, int guess, verb_cnn* cnn,

@@ -21,6 +21,7 @@ STATUS_NAMES = {
     9: "VERB_ERR_GRID", 10: "VERB_TIMEOUT", 11: "VERB_ERR_SIZE", 12: "VERB_ERR_IO",
 }
 VERB_GUESS_ZERO, VERB_GUESS_PREV, VERB_GUESS_CNN = 0, 1, 2
+CONV_ARITH = {"exact": 0, "fma": 1}
 GUESS_IDS = {"zero": VERB_GUESS_ZERO, "prev": VERB_GUESS_PREV, "cnn": VERB_GUESS_CNN}
 
 
@@ -88,6 +89,7 @@ SIGNATURES = {
     "verb_local_krylov": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, _vp, C.c_int,
                                     C.c_double, C.c_int, C.c_int, C.c_double, C.c_double, _vp]),
     "verb_local_triples": (C.c_int, [_vp, C.c_double, C.c_double, _vp, _vp]),
+    "verb_set_convection_arith": (C.c_int, [_vp, C.c_int]),
     "verb_set_local_trim": (C.c_int, [_vp, C.POINTER(C.c_int)]),
     "verb_estimate_device_bytes": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                              C.c_longlong, C.POINTER(C.c_size_t)]),

@@ -74,6 +74,11 @@ class Context:
         a = np.ascontiguousarray(k0, dtype=np.int32).ravel()
         L.check(self.lib.verb_set_local_trim(self.h, a.ctypes.data_as(C.POINTER(C.c_int))), "trim")
 
+    def set_convection_arith(self, mode: str = "exact"):
+        """"exact": bit-identical to the reference; "fma": multiply-add
+        contraction, ~10 % faster, a few ulp per step from "exact"."""
+        L.check(self.lib.verb_set_convection_arith(self.h, L.CONV_ARITH[mode]), "conv_arith")
+
     def local_krylov(self, dt: float, sub_dt: float, guess: str = "prev", cnn=None,
                      smooth: int = 0, omega: float = 2.0 / 3.0, max_outer: int = 10,
                      inner_maxit: int = 100, inner_tol: float = 1e-3,
