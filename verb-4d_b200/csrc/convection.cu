@@ -26,8 +26,9 @@
 // -DVERB_BUILD_CONV_FMA -fmad=true, which lets the compiler contract multiply-add
 // pairs into fused multiply-adds (one rounding instead of two).  That variant
 // runs about 10 % faster and differs from the reference by a few units in the
-// last place per step (launch_convection_fma; the Courant factors keep their
-// exactly rounded divisions, which are written with explicit intrinsics).
+// last place per step (launch_convection_fma); it also takes the Courant
+// factors as products with rounded reciprocals instead of exactly rounded
+// quotients.
 #include "verb_internal.cuh"
 
 #ifdef VERB_BUILD_CONV_FMA
@@ -121,6 +122,46 @@ __device__ __forceinline__ double quickest_face_k(double U1, double U2, double U
     f += k.k9 * (D8 + d9 / 2);
     return f;
 }
+
+#ifdef VERB_BUILD_CONV_FMA
+// quickest_face_k regrouped for the contracted form: the D terms are symmetric
+// and the d terms antisymmetric in the pairs (U_k, D_k+1) (upwind point k
+// cells behind the centre, downwind point k+1 cells ahead), so they are
+// formed from the pair sums s_k and differences t_k, with the same
+// polynomial in the Courant factors.  Fewer operations and shorter
+// dependency chains; the rounding differs from the reference order by a few
+// units in the last place.
+__device__ __forceinline__ double quickest_face_sym(double U1, double U2, double U3, double U4,
+                                                    double C, double D1, double D2v, double D3v,
+                                                    double D4v, double D5v, double cr,
+                                                    const FaceCoef& k)
+{
+    const double ca = fabs(cr);
+    const double s0 = C + D1, t0 = C - D1;
+    const double s1 = U1 + D2v, t1 = U1 - D2v;
+    const double s2 = U2 + D3v, t2 = U2 - D3v;
+    const double s3 = U3 + D4v, t3 = U3 - D4v;
+    const double s4 = U4 + D5v, t4 = U4 - D5v;
+    const double D2 = (s1 - s0) * 0.5;
+    const double d3 = t1 - 3 * t0;
+    const double D4 = ((s2 - 3 * s1) + 2 * s0) * 0.5;
+    const double d5 = (t2 - 5 * t1) + 10 * t0;
+    const double D6 = ((s3 - 5 * s2) + (9 * s1 - 5 * s0)) * 0.5;
+    const double d7 = (t3 - 7 * t2) + (21 * t1 - 35 * t0);
+    const double D8 = ((s4 - 7 * s3) + (20 * s2 - 28 * s1) + 14 * s0) * 0.5;
+    const double d9 = (t4 - 9 * t3) + (36 * t2 - 84 * t1) + 126 * t0;
+    double f = 0.5 * s0;
+    f += 0.5 * ca * t0;
+    f += k.k3 * (D2 + ca * 0.25 * d3);
+    f += k.k5 * (D4 + k.c6 * d5);
+    f += k.k7 * (D6 + ca * 0.125 * d7);
+    f += k.k9 * (D8 + d9 * 0.5);
+    return f;
+}
+#define QUICKEST_FACE quickest_face_sym
+#else
+#define QUICKEST_FACE quickest_face_k
+#endif
 
 // Limiter of src/Convection_1D_ULTIMATE_QUICKEST6.cpp:394-447 applied to the
 // unlimited face value f.
@@ -433,11 +474,21 @@ __device__ __forceinline__ FaceCoef face_coef_exact(double cr)
     // t1 = cs - 1 and ca = |cr| are never -0, nor is p3 = p2*(cs-9) (p2 = -0
     // only when cs = 1, and then p3 = +0); p2 and p4 are -0 when |cr| = 1
     FaceCoef k;
+#ifdef VERB_BUILD_CONV_FMA
+    // contracted form: a product with the rounded reciprocal (within an ulp
+    // of the quotient) instead of the exactly rounded division
+    k.k3 = t1 * (1.0 / 6.0);
+    k.c6 = ca * (1.0 / 6.0);
+    k.k5 = p2 * (1.0 / 120.0);
+    k.k7 = p3 * (1.0 / 5040.0);
+    k.k9 = p4 * (1.0 / 362880.0);
+#else
     k.k3 = div_const_nz(t1, 6.0, 1.0 / 6.0);
     k.c6 = div_const_nz(ca, 6.0, 1.0 / 6.0);
     k.k5 = div_const(p2, 120.0, 1.0 / 120.0);
     k.k7 = div_const_nz(p3, 5040.0, 1.0 / 5040.0);
     k.k9 = div_const(p4, 362880.0, 1.0 / 362880.0);
+#endif
     return k;
 }
 
@@ -451,11 +502,11 @@ __device__ __forceinline__ double face3(const double (&w)[10], double cr)
 {
     const FaceCoef k = face_coef_exact(cr);
     if (DIR == DIR_POS)
-        return quickest_face_k(w[3], w[2], w[1], w[0], w[4], w[5], w[6], w[7], w[8], w[9], cr, k);
+        return QUICKEST_FACE(w[3], w[2], w[1], w[0], w[4], w[5], w[6], w[7], w[8], w[9], cr, k);
     if (DIR == DIR_NEG)
-        return quickest_face_k(w[6], w[7], w[8], w[9], w[5], w[4], w[3], w[2], w[1], w[0], cr, k);
+        return QUICKEST_FACE(w[6], w[7], w[8], w[9], w[5], w[4], w[3], w[2], w[1], w[0], cr, k);
     const bool up = cr >= 0;
-    return quickest_face_k(up ? w[3] : w[6], up ? w[2] : w[7], up ? w[1] : w[8], up ? w[0] : w[9],
+    return QUICKEST_FACE(up ? w[3] : w[6], up ? w[2] : w[7], up ? w[1] : w[8], up ? w[0] : w[9],
                            up ? w[4] : w[5], up ? w[5] : w[4], up ? w[6] : w[3], up ? w[7] : w[2],
                            up ? w[8] : w[1], up ? w[9] : w[0], cr, k);
 }
