@@ -210,6 +210,27 @@ int verb_cnn_forward(verb_cnn* cnn, const float* in_dev, float* out_dev, int bat
 int verb_cnn_train_step(verb_cnn* cnn, const float* in_dev, const float* target_dev, int batch,
                         float lr, float* loss_host);
 
+/* ---- convection data assimilation ------------------------------------------
+ * runKalmanFilterConvection2D (src/DataAssimilationConvection.cpp:124-253)
+ * on every (V,K) slice, as DataAssimilationManagerConvection::assimilate
+ * (:45-121) calls it from the driver (src/VERB4D_Solver.cpp:1246): the state
+ * is the slice's N = P*R PSD values, the model matrix is the upwind transport
+ * operator of the step raised to its Courant split count (cached per slice
+ * until has_vx_updated), the loss rate is the Sources field over the PSD (the
+ * driver's argument), no saturation map.  obs_host is a [P][R][V][K] field
+ * with NaN where there is no observation.  Pa and the model matrices
+ * (2 N^2 doubles per slice) persist in the context; slice_chunk bounds the
+ * slices processed together (0: chunks of about 4 GB of work space).
+ * Deviation: a slice without observations keeps its PSD and takes Pa = Pf;
+ * the reference's dummy observation row (H = 0, y = 0) makes the linear
+ * form's innovation matrix singular (trans_solve exits) and the log form's
+ * innovation log(0) (the NaN check throws). */
+int verb_assimilate_convection(verb_ctx* ctx, const double* obs_host, double dt, double model_error,
+                               double obs_error, int use_log, double correlation_time,
+                               int growing_q, int has_vx_updated, int slice_chunk);
+/* Pa (N x N) and the cached model matrix of slice (v, k); either may be NULL. */
+int verb_convection_da_state(verb_ctx* ctx, int v, int k, double* Pa_host, double* model_host);
+
 /* Convection arithmetic.  VERB_CONV_EXACT (the default) restates the
  * reference's operations one by one without contraction, so results are
  * bit-identical to it (exp() of loss rates aside).  VERB_CONV_FMA runs the

@@ -149,6 +149,27 @@ class _Lib:
                 C.c_double(model_error), C.c_double(obs_error))
         return st, f, pa, F, Pf
 
+    def kf_convection_2d(self, forecast, Pa, model, Pg, Rg, VP, VR, has_vx_updated, loss, sat,
+                         obs, dt, model_error, obs_error, use_log=False,
+                         correlation_time=float("inf"), growing_q=False):
+        """runKalmanFilterConvection2D of the reference build (oracle/_ref) on
+        one [P][R] slice; returns (status, forecast, Pa, model, Pf)."""
+        f = _f64(forecast).copy()
+        nP, nR = f.shape
+        N = nP * nR
+        pa = _f64(Pa).copy()
+        mm = np.zeros((N, N)) if model is None else _f64(model).copy()
+        Pf = np.zeros((N, N))
+        sat_b = None if sat is None else np.ascontiguousarray(sat, dtype=np.uint8)
+        st = self.lib.ref_kf_convection_2d(
+            _p(f), _p(pa), _p(mm), C.c_int(model is not None), _p(Pf), _p(_f64(Pg)), _p(_f64(Rg)),
+            _p(_f64(VP)), _p(_f64(VR)), C.c_int(int(has_vx_updated)), _p(_f64(loss)),
+            sat_b.ctypes.data_as(C.POINTER(C.c_ubyte)) if sat_b is not None else None,
+            _p(_f64(obs)), C.c_int(nP), C.c_int(nR), C.c_double(dt), C.c_double(model_error),
+            C.c_double(obs_error), C.c_int(int(use_log)), C.c_double(correlation_time),
+            C.c_int(int(growing_q)))
+        return st, f, pa, mm, Pf
+
     # ------------------------------------------------------------- band LU
     def monot_cubic(self, x, f, xq):
         """Monotone cubic interpolation: orc_monot_cubic in the oracle,

@@ -19,6 +19,7 @@
 #include "Convection_1D_ULTIMATE_QUICKEST6.h"
 #include "Convection_2D.h"
 #include "DataAssimilation.h"
+#include "DataAssimilationConvection.h"
 #include "DataAssimilationDiffusion.h"
 #include "Diffusion_1D.h"
 #include "Diffusion_2D.h"
@@ -178,6 +179,47 @@ int ref_kf_diffusion_1d(double* forecast, double* Pa, double* F, double* Pf, con
     std::memcpy(forecast, &f[0], sizeof(double) * n);
     std::memcpy(Pa, pa[0], sizeof(double) * n * n);
     std::memcpy(F, model[0], sizeof(double) * n * n);
+    return 0;
+}
+
+// src/DataAssimilationConvection.cpp:124 runKalmanFilterConvection2D for one
+// (V,K) slice of nP x nR points (N = nP*nR).  forecast[N] ([P][R]) and Pa[N*N]
+// are updated in place; model[N*N] is the model-matrix cache (used as given
+// when model_valid and !has_vx_updated, else rebuilt and returned); Pf[N*N]
+// receives the forecast covariance.  P and R are the [P][R] grids; loss is the
+// loss-rate slice; sat (may be NULL) the saturation map as 0/1 bytes.
+int ref_kf_convection_2d(double* forecast, double* Pa, double* model, int model_valid, double* Pf,
+                         const double* P, const double* R, const double* VP, const double* VR,
+                         int has_vx_updated, const double* loss, const unsigned char* sat,
+                         const double* obs, int nP, int nR, double dt, double model_error,
+                         double obs_error, int use_log, double correlation_time, int growing_q)
+{
+    const long N = static_cast<long>(nP) * nR;
+    Matrix2D<double> f = mat(forecast, nP, nR);
+    Matrix2D<double> pa = mat(Pa, N, N);
+    Matrix2D<double> mm;
+    if (model_valid) mm = mat(model, N, N);
+    Matrix2D<bool> satm(static_cast<size_t>(nP), static_cast<size_t>(nR));
+    for (long i = 0; i < N; i++) satm[i / nR][i % nR] = sat ? sat[i] != 0 : false;
+    data_assimilation::Parameters prm{};
+    prm.runDataAssimilation = true;
+    prm.useLog = use_log != 0;
+    prm.timeStep = dt;
+    prm.modelError = model_error;
+    prm.observationError = obs_error;
+    prm.correlationTime = correlation_time;
+    prm.growing_Q_at_boundary = growing_q != 0;
+    try {
+        auto dbg = data_assimilation::runKalmanFilterConvection2D(
+            f, pa, mm, mat(P, nP, nR), mat(R, nP, nR), mat(VP, nP, nR), mat(VR, nP, nR),
+            has_vx_updated != 0, mat(loss, nP, nR), satm, mat(obs, nP, nR), dt, prm);
+        std::memcpy(Pf, dbg.a_priori_err_cov[0], sizeof(double) * N * N);
+    } catch (...) {
+        return 2;  // NaN after the update (src/DataAssimilation.cpp:62-67) or an unstable model
+    }
+    std::memcpy(forecast, f[0], sizeof(double) * N);
+    std::memcpy(Pa, pa[0], sizeof(double) * N * N);
+    std::memcpy(model, mm[0], sizeof(double) * N * N);
     return 0;
 }
 

@@ -1,0 +1,153 @@
+"""Convection data assimilation on the GPU (verb_assimilate_convection)
+against the CPU restatement (oracle/kfconv.py, itself pinned to the
+reference's runKalmanFilterConvection2D).
+
+Every (V,K) slice of a small grid goes through two assimilations (model
+matrix built, then reused from the cache), in chunks of slices that do not
+divide the slice count, in the linear and the log form; states,
+covariances and model matrices are compared norm-wise per slice (the
+linear form's states norm-wise over the field, see below).  The GPU
+forms products in another order than dgemm (batched tiles, binary
+exponentiation with the squarings in another order) and solves the gain by
+its own LU, so agreement is to rounding: 1e-10 for states and covariances,
+1e-12 for the model matrices.  A slice without observations keeps its PSD
+and takes Pa = Pf (the reference's dummy observation row makes the linear
+form's innovation matrix singular, so it exits, and gives log(0) in the log
+form, so it throws on the NaN state).  At
+24 x 25 x 31 x 31 (961 slices of 600 states) sampled slices are checked.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import kfconv as KC
+from verb4d_b200 import workload as W
+
+from test_gpu_step import load_ctx
+
+pytestmark = pytest.mark.gpu
+ME, OE = 1e-3, 1e-2
+TOL = 1e-10
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / np.abs(b).max()
+
+
+def make_obs(wl, seed, frac, empty=()):
+    rng = np.random.default_rng(seed)
+    psd = wl.fields["psd"]
+    obs = np.full(psd.shape, np.nan)
+    mask = rng.uniform(size=psd.shape) < frac
+    obs[mask] = psd[mask] * np.exp(0.1 * rng.standard_normal(mask.sum()))
+    P, R, V, K = psd.shape
+    for v, k in empty:
+        obs[:, :, v, k] = np.nan
+    # every other slice has at least one observation
+    for v in range(V):
+        for k in range(K):
+            if (v, k) not in empty and not np.isfinite(obs[:, :, v, k]).any():
+                obs[P // 2, R // 2, v, k] = psd[P // 2, R // 2, v, k]
+    return obs
+
+
+def oracle_slice(wl, psd, Pa, model, obs, v, k, first, use_log):
+    f = wl.fields
+    sl = lambda a: np.ascontiguousarray(a[:, :, v, k])  # noqa: E731
+    x = sl(psd)
+    loss = sl(f["S"]) / x
+    o = sl(obs)
+    if not np.isfinite(o).any():
+        # no observation: x unchanged, Pa = Pf (the reference fails here)
+        model = KC.model_matrix(sl(f["VP"]), sl(f["VR"]), loss, np.zeros(x.shape, bool), wl.dt,
+                                f["Pg"][1, 0, v, k] - f["Pg"][0, 0, v, k],
+                                f["Rg"][0, 1, v, k] - f["Rg"][0, 0, v, k], use_log,
+                                math.inf) if (first or model is None) else model
+        N = x.size
+        Pa = Pa.copy()
+        if np.abs(Pa).max() == 0:
+            Pa[np.arange(N), np.arange(N)] = 5 * ME
+        M1d = KC.matpow(model, int(math.ceil(3. / 24 / wl.dt)))
+        nR = x.shape[1]
+        t = np.full(N, ME)
+        bidx = [i for i in range(N) if i % nR in (0, nR - 1)]
+        t[bidx] = 0.0
+        Q = (M1d * t) @ M1d.T + np.diag(np.full(N, ME)) / 10
+        Q[bidx, bidx] = 0.0
+        return x, model @ Pa @ model.T + Q, model
+    xo, pao, mo, _ = KC.kf_convection_2d(x, Pa, model, sl(f["Pg"]), sl(f["Rg"]), sl(f["VP"]),
+                                          sl(f["VR"]), first, loss, None, o, wl.dt, ME, OE,
+                                          use_log=use_log)
+    return xo, pao, mo
+
+
+@pytest.mark.parametrize("use_log", [False, True])
+def test_small_grid_all_slices(gpu, use_log):
+    wl = W.make_workload(W.GridSpec(8, 11, 4, 3), seed=61, sources=True)
+    P, R, V, K = wl.spec.shape
+    N = P * R
+    empty = [(1, 2)]
+    c = load_ctx(wl)
+    psd = wl.fields["psd"].copy()
+    Pa = {(v, k): np.zeros((N, N)) for v in range(V) for k in range(K)}
+    model = {(v, k): None for v in range(V) for k in range(K)}
+    for it in range(2):
+        obs = make_obs(wl, 70 + it, 0.15, empty)
+        c.assimilate_convection(obs, wl.dt, ME, OE, use_log=use_log, has_vx_updated=(it == 0),
+                                slice_chunk=5)
+        got = c.download()
+        new = psd.copy()
+        for v in range(V):
+            for k in range(K):
+                x, Pa[v, k], model[v, k] = oracle_slice(wl, psd, Pa[v, k], model[v, k], obs, v, k,
+                                                        it == 0, use_log)
+                new[:, :, v, k] = x
+                gpa, gm = c.convection_da_state(v, k)
+                assert rel(gm, model[v, k]) < 1e-12, (it, v, k)
+                assert rel(gpa, Pa[v, k]) < TOL, (it, v, k)
+                if use_log:
+                    assert rel(got[:, :, v, k], x) < TOL, (it, v, k)
+        # the linear form's gain is ill-conditioned on slices whose PSD is far
+        # below the absolute model error (cond(H Pf H^T) ~ 1e20 at 10 MeV,
+        # PSD ~ 1e-22): a 1e-13 change of the inputs moves their state by
+        # tens of percent relative to the slice, so the state is compared
+        # norm-wise over the whole field
+        assert rel(got, new) < TOL, it
+        # the slice without observations kept its PSD (up to the log/exp
+        # round trip of the log form when its chunk has observations)
+        assert rel(got[:, :, 1, 2], psd[:, :, 1, 2]) < 1e-14
+        psd = new
+        c.upload("psd", got)
+    c.close()
+
+
+def test_cfg1_sampled_slices(gpu):
+    import time
+
+    wl = W.make_workload(W.CONFIGS["cfg1"], seed=62, sources=True)
+    P, R, V, K = wl.spec.shape
+    N = P * R
+    obs = make_obs(wl, 80, 0.02)
+    psd = wl.fields["psd"]
+    c = load_ctx(wl)
+    t0 = time.perf_counter()
+    c.assimilate_convection(obs, wl.dt, ME, OE, has_vx_updated=True)
+    c.sync()
+    t1 = time.perf_counter()
+    got = c.download()
+    for v, k in [(V - 1, 0), (V // 2, K // 3), (3, K - 1)]:
+        x, pa, m = oracle_slice(wl, psd, np.zeros((N, N)), None, obs, v, k, True, False)
+        gpa, gm = c.convection_da_state(v, k)
+        assert rel(gm, m) < 1e-12
+        assert rel(gpa, pa) < TOL
+        assert rel(got[:, :, v, k], x) < TOL
+    c.upload("psd", got)
+    c.sync()
+    t2 = time.perf_counter()
+    c.assimilate_convection(obs, wl.dt, ME, OE, has_vx_updated=False)
+    c.sync()
+    t3 = time.perf_counter()
+    print("24x25x31x31 convection assimilation (961 slices of 600 states): "
+          "%.3f s with the model build, %.3f s with the cached model" % (t1 - t0, t3 - t2))
+    c.close()

@@ -48,6 +48,46 @@ void launch_radial_solve(const RadialArgs& a, cudaStream_t s);
 void launch_tridag(const double* a, const double* b, const double* c, const double* r, double* u,
                   long n, cudaStream_t s);
 
+// --- convection data assimilation (kfconv.cu) ---------------------------------
+// batched row-major FP64 GEMM: C[s] = Cin[s] + sgn * A[s] diag(dk[s]) op(B[s])
+// (Cin null: no addend; dk null: no scale); batch b works on slice idx[b]
+struct BGemm {
+    const double* A; size_t sA; int lda;
+    const double* B; size_t sB; int ldb;
+    double* C; size_t sC; int ldc;
+    const double* Cin; size_t sCin; int ldcin;
+    double sgn;
+    const double* dk; size_t sdk;
+    int M, N, K;
+    const int* idx;
+};
+void launch_bgemm(const BGemm& g, bool tb, int batch, cudaStream_t s);
+struct KCArgs {
+    Dims d;
+    int s0;  // first (V,K) slice of the chunk (slice = v*K + k)
+    double dt, model_error, obs_error, corr_time;
+    int use_log, growing_q;
+    const double *Pg, *Rg, *VP, *VR, *S;
+    double* psd;
+    const double* obs;
+    int* status;
+};
+void launch_kc_split(const KCArgs& a, int nb, int* nt, cudaStream_t s);
+void launch_kc_model(const KCArgs& a, int nb, const int* nt, double* M1, size_t sM, cudaStream_t s);
+void launch_kc_tdiag(const KCArgs& a, int nb, double* t, size_t st, cudaStream_t s);
+void launch_kc_qdiag(const KCArgs& a, int nb, double* Q, size_t sQ, cudaStream_t s);
+void launch_kc_pa_init(const KCArgs& a, int nb, double* Pa, size_t sPa, cudaStream_t s);
+void launch_kc_obs(const KCArgs& a, int nb, int* m, int* oidx, double* y, double* x, int ldo,
+                   cudaStream_t s);
+void launch_kc_gain(const KCArgs& a, int nb, const double* Pf, size_t sPf, double* G, double* St,
+                    size_t sW, const int* m, const int* oidx, double* y, const double* x, int ldo,
+                    int mm, cudaStream_t s);
+void launch_kc_update(const KCArgs& a, int nb, const double* Kg, size_t sW, const int* m,
+                      const int* oidx, const double* y, const double* x, int ldo, int mm,
+                      const double* Pf, size_t sPf, double* Hf, cudaStream_t s);
+void launch_kc_copy(const double* src, size_t ss, double* dst, size_t sd, size_t n, int nb,
+                    const int* idx, cudaStream_t s);
+
 // --- convection ----------------------------------------------------------------
 struct ConvArgs {
     Dims d;

@@ -74,6 +74,26 @@ class Context:
         a = np.ascontiguousarray(k0, dtype=np.int32).ravel()
         L.check(self.lib.verb_set_local_trim(self.h, a.ctypes.data_as(C.POINTER(C.c_int))), "trim")
 
+    def assimilate_convection(self, obs, dt, model_error, obs_error, use_log=False,
+                              correlation_time=float("inf"), growing_q=False,
+                              has_vx_updated=False, slice_chunk=0) -> None:
+        """Kalman-filter update of every (V,K) slice (convection data
+        assimilation); obs is [P][R][V][K] with NaN where unobserved."""
+        o = _f64(obs)
+        L.check(self.lib.verb_assimilate_convection(
+            self.h, o.ctypes.data_as(L._dp), float(dt), float(model_error), float(obs_error),
+            int(use_log), float(correlation_time), int(growing_q), int(has_vx_updated),
+            int(slice_chunk)), "assimilate_convection")
+
+    def convection_da_state(self, v: int, k: int):
+        """(Pa, model matrix) of slice (v, k) after a convection assimilation."""
+        N = self.shape[0] * self.shape[1]
+        pa = np.empty((N, N))
+        mm = np.empty((N, N))
+        L.check(self.lib.verb_convection_da_state(self.h, v, k, pa.ctypes.data_as(L._dp),
+                                                  mm.ctypes.data_as(L._dp)), "da_state")
+        return pa, mm
+
     def set_convection_arith(self, mode: str = "exact"):
         """"exact": bit-identical to the reference; "fma": multiply-add
         contraction, ~10 % faster, a few ulp per step from "exact"."""
