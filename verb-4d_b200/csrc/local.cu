@@ -433,8 +433,14 @@ __device__ __forceinline__ void cp_wait()
 }
 
 constexpr int SOLVE_WARPS = 4;
-constexpr int FWD_DEPTH = 4;   // L columns in flight per warp
-constexpr int BWD_DEPTH = 2;   // U columns in flight per warp
+#ifndef VERB_FWD_DEPTH
+#define VERB_FWD_DEPTH 4
+#endif
+#ifndef VERB_BWD_DEPTH
+#define VERB_BWD_DEPTH 2
+#endif
+constexpr int FWD_DEPTH = VERB_FWD_DEPTH;  // L columns in flight per warp
+constexpr int BWD_DEPTH = VERB_BWD_DEPTH;  // U columns in flight per warp
 constexpr int FWD_WIN = 128;   // >= kl + 1
 constexpr int BWD_WIN = 256;   // >= kv + 1
 
