@@ -315,6 +315,13 @@ int verb_clamp_positive(verb_ctx* ctx);
  * negative count (src/VERB4D_Solver.cpp:747-1242).  run_* select the phases. */
 int verb_step(verb_ctx* ctx, double dt, double sub_dt, int run_convection, int run_radial,
               int run_local, long long* negative_count);
+/* Replay steps from a CUDA graph: the launches of a steady-state step (no
+ * factorisation, allocation or phase timing) are captured on first use and
+ * replayed while dt, sub_dt, the phase flags and every launch argument stay
+ * the same; uploads of fields other than the PSD, scales, boundary types,
+ * options and forms drop the graph, and the next such step captures it again.
+ * Results are identical to eager steps.  Off by default. */
+int verb_set_step_graph(verb_ctx* ctx, int enable);
 /* Number of PSD points < 0 (src/VERB4D_Solver.cpp:1226-1240). */
 int verb_negative_count(verb_ctx* ctx, long long* count);
 /* min(DVV*DKK - DVK*DVK) over the grid (src/VERB4D_Solver.cpp:747-753). */

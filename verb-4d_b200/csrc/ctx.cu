@@ -120,6 +120,14 @@ struct verb_ctx {
     cudaEvent_t out_ev_snap = nullptr, out_ev_host = nullptr;
     std::thread out_thread;
     int out_status = VERB_OK;
+    // CUDA graph of the steady-state step (captured on first use, replayed
+    // while nothing the step's launches depend on changes)
+    bool use_graph = false;
+    bool graph_valid = false;
+    cudaGraphExec_t step_exec = nullptr;
+    double g_dt = 0, g_sub_dt = 0;
+    int g_flags = 0;
+    long long g_launches = 0;
     // timing
     bool timing = false;
     std::vector<EventPair> ev[PH_N];
@@ -128,6 +136,10 @@ struct verb_ctx {
 };
 
 namespace {
+
+// anything that changes a launch argument of the step (a field other than the
+// PSD, scales, boundary types, options, forms) drops the captured step graph
+inline void graph_invalidate(verb_ctx* c) { c->graph_valid = false; }
 
 int cuda_ok(cudaError_t e)
 {
@@ -1087,6 +1099,7 @@ int verb_destroy(verb_ctx* c)
         cudaFree(p);
     free_krylov(c);
     free_kc(c);
+    if (c->step_exec) cudaGraphExecDestroy(c->step_exec);
     for (void* p : {(void*)c->rfa, (void*)c->rfbet, (void*)c->rfgam, (void*)c->Lf, (void*)c->Uf,
                     (void*)c->lwork, (void*)c->ipiv, (void*)c->conv_scratch,
                     (void*)c->conv_substeps, (void*)c->ticket, (void*)c->red, (void*)c->status,
@@ -1140,6 +1153,7 @@ int verb_device_bytes(const verb_ctx* c, size_t* bytes)
 static int upload_common(verb_ctx* c, int fid, const void* src, cudaMemcpyKind kind)
 {
     if (!c || fid < 0 || fid >= VERB_F_COUNT || !src || c->upd[fid]) return VERB_ERR_ARG;
+    graph_invalidate(c);
     const size_t bytes = npts(c) * sizeof(double);
     int s = ensure_field(c, fid);
     if (s) return s;
@@ -1173,6 +1187,7 @@ int verb_upload_field_device(verb_ctx* c, int fid, const double* dev)
 int verb_set_field_scale(verb_ctx* c, int fid, double scale)
 {
     if (!c || fid < 0 || fid >= VERB_F_COUNT || c->upd[fid]) return VERB_ERR_ARG;
+    graph_invalidate(c);
     if (scale == c->scale[fid]) return VERB_OK;
     const size_t bytes = npts(c) * sizeof(double);
     if (c->f[fid]) {
@@ -1196,6 +1211,7 @@ int verb_set_field_scale(verb_ctx* c, int fid, double scale)
 int verb_upload_bc(verb_ctx* c, int b, const double* host)
 {
     if (!c || b < 0 || b >= VERB_BCF_COUNT || !host) return VERB_ERR_ARG;
+    graph_invalidate(c);
     if (!c->bc[b]) CK(cudaMalloc(&c->bc[b], bc_elems(c, b) * sizeof(double)));
     CK(cudaMemcpyAsync(c->bc[b], host, bc_elems(c, b) * sizeof(double), cudaMemcpyHostToDevice,
                        c->stream));
@@ -1205,6 +1221,7 @@ int verb_upload_bc(verb_ctx* c, int b, const double* host)
 int verb_set_bc_types(verb_ctx* c, const int* types)
 {
     if (!c || !types) return VERB_ERR_ARG;
+    graph_invalidate(c);
     for (int i = 0; i < VERB_BCF_COUNT; i++)
         if (types[i] < 0 || types[i] > 2) return VERB_ERR_BC;
     bool rad = types[VERB_BCF_LL] != c->bct[VERB_BCF_LL] || types[VERB_BCF_LU] != c->bct[VERB_BCF_LU];
@@ -1221,6 +1238,7 @@ int verb_set_options(verb_ctx* c, int radial_sources, int local_sources, int inc
                      int positive_psd)
 {
     if (!c) return VERB_ERR_ARG;
+    graph_invalidate(c);
     c->radial_sources = radial_sources;
     c->local_sources = local_sources;
     if ((include_boundary != 0) != (c->include_boundary != 0)) c->local_dirty = true;
@@ -1234,6 +1252,7 @@ int verb_set_local_precision(verb_ctx* c, int mode, int refinements)
     if (!c || (mode != VERB_PREC_FP64 && mode != VERB_PREC_MIXED) || refinements < 0 ||
         refinements > 16)
         return VERB_ERR_ARG;
+    graph_invalidate(c);
     if (mode != c->local_prec) {
         // release the other form's factors before the next factorisation
         // allocates this one's
@@ -1272,6 +1291,7 @@ int verb_local_refinement(verb_ctx* c, double* rel_correction)
 int verb_invalidate_lu(verb_ctx* c)
 {
     if (!c) return VERB_ERR_ARG;
+    graph_invalidate(c);
     c->local_dirty = true;
     c->radial_dirty = true;
     return VERB_OK;
@@ -1344,6 +1364,7 @@ int verb_convection_da_state(verb_ctx* c, int v, int k, double* Pa_host, double*
 int verb_set_convection_arith(verb_ctx* c, int mode)
 {
     if (!c || (mode != VERB_CONV_EXACT && mode != VERB_CONV_FMA)) return VERB_ERR_ARG;
+    graph_invalidate(c);
     c->conv_arith = mode;
     return VERB_OK;
 }
@@ -1397,18 +1418,13 @@ int verb_tensor_check(verb_ctx* c, double* min_value)
     return tensor_check(c, min_value);
 }
 
-int verb_step(verb_ctx* c, double dt, double sub_dt, int run_convection, int run_radial,
-              int run_local, long long* negative_count)
+// The launches of one step after its host-side checks: phases, clamps and
+// the negative-count kernel (its result is read by the caller).
+int step_body(verb_ctx* c, double dt, double sub_dt, int run_convection, int run_radial,
+              int run_local)
 {
-    if (!c || !(dt > 0)) return VERB_ERR_ARG;
     const Dims& d = c->d;
     int s;
-    if (run_local && d.V >= 3 && d.K >= 3) {
-        double m = 0;
-        s = tensor_check(c, &m);
-        if (s) return s;
-        if (m < 0) return VERB_ERR_TENSOR;
-    }
     if (c->positive_psd && (s = verb_clamp_positive(c))) return s;
     if (run_convection && (3 < d.P || 3 < d.R)) {
         s = conv_run(c, dt);
@@ -1424,13 +1440,88 @@ int verb_step(verb_ctx* c, double dt, double sub_dt, int run_convection, int run
         s = local_run(c, dt, sub_dt);
         if (s) return s;
     }
+    if (c->positive_psd) return verb_clamp_positive(c);
+    return verb_negative_count(c, nullptr);
+}
+
+int verb_set_step_graph(verb_ctx* c, int enable)
+{
+    if (!c) return VERB_ERR_ARG;
+    c->use_graph = enable != 0;
+    c->graph_valid = false;
+    if (!c->use_graph && c->step_exec) {
+        CK(cudaStreamSynchronize(c->stream));
+        cudaGraphExecDestroy(c->step_exec);
+        c->step_exec = nullptr;
+    }
+    return VERB_OK;
+}
+
+int verb_step(verb_ctx* c, double dt, double sub_dt, int run_convection, int run_radial,
+              int run_local, long long* negative_count)
+{
+    if (!c || !(dt > 0)) return VERB_ERR_ARG;
+    const Dims& d = c->d;
+    int s;
+    const bool loc = run_local && d.V >= 3 && d.K >= 3;
+    if (loc) {
+        double m = 0;
+        s = tensor_check(c, &m);
+        if (s) return s;
+        if (m < 0) return VERB_ERR_TENSOR;
+    }
+    // a step that factorises, allocates or is timed runs eagerly; the others
+    // replay the captured graph of the same step (same dt, sub-step, phases)
+    int nsub = (int)(dt / sub_dt);
+    if (nsub < 1) nsub = 1;
+    const bool eager =
+        !c->use_graph || c->timing ||
+        (loc && (c->local_dirty || dt / nsub != c->local_dt || !c->lwork)) ||
+        (run_radial && d.R >= 3 && (c->radial_dirty || dt != c->radial_dt)) ||
+        (run_convection && (3 < d.P || 3 < d.R) && !c->conv_scratch) || !c->red;
+    const int flags = (run_convection ? 1 : 0) | (run_radial ? 2 : 0) | (run_local ? 4 : 0);
+    if (eager) {
+        c->graph_valid = false;
+        s = step_body(c, dt, sub_dt, run_convection, run_radial, run_local);
+        if (s) return s;
+    } else {
+        if (!(c->graph_valid && c->g_dt == dt && c->g_sub_dt == sub_dt && c->g_flags == flags)) {
+            cudaGraph_t g = nullptr;
+            const long long k0 = c->acc.kernel_launches;
+            CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            s = step_body(c, dt, sub_dt, run_convection, run_radial, run_local);
+            const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+            if (s || e != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                return s ? s : cuda_ok(e);
+            }
+            c->g_launches = c->acc.kernel_launches - k0;
+            c->acc.kernel_launches = k0;
+            if (c->step_exec) cudaGraphExecDestroy(c->step_exec);
+            c->step_exec = nullptr;
+            const cudaError_t ei = cudaGraphInstantiate(&c->step_exec, g, 0);
+            cudaGraphDestroy(g);
+            CK(ei);
+            c->graph_valid = true;
+            c->g_dt = dt;
+            c->g_sub_dt = sub_dt;
+            c->g_flags = flags;
+        }
+        CK(cudaGraphLaunch(c->step_exec, c->stream));
+        c->acc.kernel_launches += c->g_launches;
+    }
     c->acc.steps++;
     if (c->positive_psd) {
-        s = verb_clamp_positive(c);
         if (negative_count) *negative_count = 0;
-        return s;
+        return check_launch();
     }
-    return verb_negative_count(c, negative_count);
+    if (negative_count) {
+        unsigned long long k = 0;
+        CK(cudaMemcpyAsync(&k, c->red, sizeof(k), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        *negative_count = (long long)k;
+    }
+    return check_launch();
 }
 
 int verb_sync(verb_ctx* c)
@@ -1800,6 +1891,7 @@ bool pop_component(UpdComponent& k, double t, double** new_base)
 int verb_field_add_component(verb_ctx* c, int fid, const double* host_base, int* comp)
 {
     if (!c || !host_base || !updatable_field(fid)) return VERB_ERR_ARG;
+    graph_invalidate(c);
     if (!c->upd[fid]) c->upd[fid] = new (std::nothrow) UpdField();
     if (!c->upd[fid]) return VERB_ERR_NOMEM;
     UpdField& u = *c->upd[fid];
@@ -1819,6 +1911,7 @@ int verb_field_set_merge(verb_ctx* c, int fid, int merge)
     if (!c || fid < 0 || fid >= VERB_F_COUNT || !c->upd[fid] ||
         (merge != VERB_MERGE_SUM && merge != VERB_MERGE_MEAN))
         return VERB_ERR_ARG;
+    graph_invalidate(c);
     c->upd[fid]->merge = merge;
     c->upd[fid]->built = false;
     return VERB_OK;
@@ -1860,6 +1953,7 @@ int verb_component_queue_limit(verb_ctx* c, int fid, int comp, int axis, int whi
 int verb_update_fields(verb_ctx* c, double current_time, unsigned int* updated_mask)
 {
     if (!c) return VERB_ERR_ARG;
+    graph_invalidate(c);
     unsigned int mask = 0;
     for (int fid = 0; fid < VERB_F_COUNT; fid++) {
         UpdField* u = c->upd[fid];
@@ -1969,6 +2063,7 @@ int verb_write_field_pltb(verb_ctx* c, int fid, const char* path, int async_writ
 int verb_read_field_pltb(verb_ctx* c, int fid, const char* path)
 {
     if (!c || !path || fid < 0 || fid >= VERB_F_COUNT) return VERB_ERR_ARG;
+    graph_invalidate(c);
     FILE* f = fopen(path, "rb");
     if (!f) return VERB_ERR_IO;
     int32_t sz[4];
@@ -2004,6 +2099,7 @@ int verb_append_lst(const char* lst_path, double time, const char* filename)
 int verb_remap_L(verb_ctx* c, const double* new_L_host)
 {
     if (!c || !new_L_host) return VERB_ERR_ARG;
+    graph_invalidate(c);
     for (int fid : {VERB_F_PSD, VERB_F_L}) {
         int s = need_field(c, fid);
         if (s) return s;
@@ -2074,6 +2170,7 @@ int verb_estimate_device_bytes(int P, int R, int V, int K, int precision, int re
 int verb_set_local_trim(verb_ctx* c, const int* k0_host)
 {
     if (!c) return VERB_ERR_ARG;
+    graph_invalidate(c);
     const Dims& d = c->d;
     const size_t nsys = (size_t)d.P * d.R;
     CK(cudaStreamSynchronize(c->stream));

@@ -90,6 +90,7 @@ SIGNATURES = {
                                     C.c_double, C.c_int, C.c_int, C.c_double, C.c_double, _vp]),
     "verb_local_triples": (C.c_int, [_vp, C.c_double, C.c_double, _vp, _vp]),
     "verb_set_convection_arith": (C.c_int, [_vp, C.c_int]),
+    "verb_set_step_graph": (C.c_int, [_vp, C.c_int]),
     "verb_assimilate_convection": (C.c_int, [_vp, _dp, C.c_double, C.c_double, C.c_double, C.c_int,
                                              C.c_double, C.c_int, C.c_int, C.c_int]),
     "verb_convection_da_state": (C.c_int, [_vp, C.c_int, C.c_int, _dp, _dp]),

@@ -94,6 +94,10 @@ class Context:
                                                   mm.ctypes.data_as(L._dp)), "da_state")
         return pa, mm
 
+    def set_step_graph(self, enable: bool = True):
+        """Replay steady-state steps from a captured CUDA graph."""
+        L.check(self.lib.verb_set_step_graph(self.h, int(enable)), "step_graph")
+
     def set_convection_arith(self, mode: str = "exact"):
         """"exact": bit-identical to the reference; "fma": multiply-add
         contraction, ~10 % faster, a few ulp per step from "exact"."""
