@@ -178,6 +178,15 @@ def run_ours(args):
     ctx.sync()
     warm = ctx.timing()
     warm_s = time.perf_counter() - t_w0
+    tune = None
+    if args.autotune and fl["run_local"]:
+        # untimed: pick the local-solve shape for this grid on its own systems
+        ch, tms = ctx.autotune_local_solve(wl.dt, wl.sub_dt)
+        shapes = ctx.solve_variants()
+        tune = {"local_solve_shapes_ms": {f"{w}x{f}x{b}": round(float(t), 3)
+                                          for (w, f, b), t in zip(shapes, tms)},
+                "chosen": "%dx%dx%d (systems per CTA x L columns x U columns in flight)"
+                          % shapes[ch]}
     ctx.set_timing(False)
     ctx.set_timing(True)  # zeroes the counters
     if args.graph:
@@ -386,6 +395,7 @@ def run_ours(args):
                                          "MEASURED_PEAKS.json sm_max_mhz",
                           "fp64_ops_per_face": FP64_OPS_PER_FACE,
                           "face_updates_per_step": int((p_faces + r_faces) * conv_substeps)},
+        "autotune": tune,
         "clocks": clk.summary(),
         "gpu_launches": int(tm["kernel_launches"]),
         "negative_points_end": int(neg),
@@ -592,6 +602,8 @@ def main():
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"],
                     help="local solve: FP64 factors, or FP32 factors with FP64 refinement")
     ap.add_argument("--refine", type=int, default=2, help="refinement steps of the mixed form")
+    ap.add_argument("--autotune", type=int, default=1, choices=[0, 1],
+                    help="time the local-solve shapes before the timed region and use the fastest")
     ap.add_argument("--graph", type=int, default=1, choices=[0, 1],
                     help="replay steady-state steps from a captured CUDA graph (1) or launch "
                          "them eagerly with per-phase events (0)")

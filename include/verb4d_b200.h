@@ -231,6 +231,25 @@ int verb_assimilate_convection(verb_ctx* ctx, const double* obs_host, double dt,
 /* Pa (N x N) and the cached model matrix of slice (v, k); either may be NULL. */
 int verb_convection_da_state(verb_ctx* ctx, int v, int k, double* Pa_host, double* model_host);
 
+/* ---- autotuner ---------------------------------------------------------------
+ * The local solve comes in verb_local_solve_variants() shapes: systems (warps)
+ * per CTA and L / U factor columns in flight per warp.  Deeper factor rings
+ * hide more memory latency per system but leave shared memory for fewer
+ * resident systems, so the best shape depends on the grid and the factor
+ * precision.  verb_autotune_local_solve factorises if needed, forms the first
+ * sub-step's right-hand sides and times every shape on them (best of three,
+ * CUDA events on the context's stream; the PSD is not changed), then uses the
+ * fastest for this context and for later contexts of the same (P, R, V, K,
+ * precision, ragged) in the process.  times_ms (may be NULL) receives one
+ * entry per shape.  All shapes give identical results.  No counterpart in the
+ * reference. */
+int verb_local_solve_variants(int* count);
+int verb_local_solve_variant(int v, int* warps_per_cta, int* l_columns, int* u_columns);
+/* v = -1: the shape tuned for this context's shape in this process (else 0) */
+int verb_set_local_solve_variant(verb_ctx* ctx, int v);
+int verb_autotune_local_solve(verb_ctx* ctx, double dt, double sub_dt, double* times_ms,
+                              int* chosen);
+
 /* Convection arithmetic.  VERB_CONV_EXACT (the default) restates the
  * reference's operations one by one without contraction, so results are
  * bit-identical to it (exp() of loss rates aside).  VERB_CONV_FMA runs the

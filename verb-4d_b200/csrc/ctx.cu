@@ -6,6 +6,9 @@
 #include <cstdio>
 #include <cstring>
 #include <deque>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <new>
 #include <string>
 #include <thread>
@@ -93,6 +96,7 @@ struct verb_ctx {
     unsigned long long* kmax = nullptr;   // [0] max relative residual key, [2..3] update maxima
     bool local_dirty = true;
     double local_dt = -1;
+    int solve_variant = -1;  // local solve shape; -1: the process-wide tuned one, else 0
     const double* dkv_override = nullptr;  // Dyx for the per-slice entry point
     // convection
     double* conv_scratch = nullptr;
@@ -319,6 +323,25 @@ int radial_run(verb_ctx* c, double dt)
     return check_launch();
 }
 
+// Local solve shapes chosen by the autotuner, per (P, R, V, K, factor
+// precision, ragged) in this process, so later contexts of the same shape
+// start with the tuned one.
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int, int, int>, int> g_tuned_solve;
+
+std::tuple<int, int, int, int, int, int> tune_key(const verb_ctx* c)
+{
+    return {c->d.P, c->d.R, c->d.V, c->d.K, c->local_prec, c->trim_k0 ? 1 : 0};
+}
+
+int solve_variant_for(verb_ctx* c)
+{
+    if (c->solve_variant >= 0) return c->solve_variant;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned_solve.find(tune_key(c));
+    return it == g_tuned_solve.end() ? 0 : it->second;
+}
+
 int local_prepare(verb_ctx* c, LocalArgs& a, double dts)
 {
     const Dims& d = c->d;
@@ -385,6 +408,7 @@ int local_prepare(verb_ctx* c, LocalArgs& a, double dts)
     a.ipiv = c->ipiv;
     a.k0 = c->trim_k0;
     a.uoff = c->trim_uoff;
+    a.solve_variant = solve_variant_for(c);
     a.work = c->lwork;
     a.status = c->status;
     return VERB_OK;
@@ -1358,6 +1382,92 @@ int verb_convection_da_state(verb_ctx* c, int v, int k, double* Pa_host, double*
         CK(cudaMemcpyAsync(model_host, c->kc_M + sl * NN, NN * sizeof(double),
                            cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    return VERB_OK;
+}
+
+int verb_local_solve_variants(int* count)
+{
+    if (!count) return VERB_ERR_ARG;
+    *count = local_solve_variants();
+    return VERB_OK;
+}
+
+int verb_local_solve_variant(int v, int* warps_per_cta, int* l_columns, int* u_columns)
+{
+    if (v < 0 || v >= local_solve_variants() || !warps_per_cta || !l_columns || !u_columns)
+        return VERB_ERR_ARG;
+    local_solve_variant_shape(v, warps_per_cta, l_columns, u_columns);
+    return VERB_OK;
+}
+
+int verb_set_local_solve_variant(verb_ctx* c, int v)
+{
+    if (!c || v < -1 || v >= local_solve_variants()) return VERB_ERR_ARG;
+    graph_invalidate(c);
+    c->solve_variant = v;
+    return VERB_OK;
+}
+
+int verb_autotune_local_solve(verb_ctx* c, double dt, double sub_dt, double* times_ms, int* chosen)
+{
+    if (!c || !(dt > 0) || !(sub_dt > 0)) return VERB_ERR_ARG;
+    const Dims& d = c->d;
+    if (d.V < 3 || d.K < 3) return VERB_ERR_ARG;
+    int nsub = (int)(dt / sub_dt);
+    if (nsub < 1) nsub = 1;
+    LocalArgs a{};
+    int s = local_prepare(c, a, dt / nsub);
+    if (s) return s;
+    if (c->local_dirty || dt / nsub != c->local_dt) {
+        s = local_factor(c, a);
+        if (s) return s;
+    }
+    graph_invalidate(c);
+    // the first sub-step's right-hand sides, kept aside: every trial solves
+    // the same systems in place
+    const size_t nu = c->local_unknowns;
+    launch_local_rhs(a, false, c->stream);
+    double* keep = nullptr;
+    CK(cudaMalloc(&keep, nu * sizeof(double)));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int st = cuda_ok(cudaMemcpyAsync(keep, c->lwork, nu * sizeof(double),
+                                     cudaMemcpyDeviceToDevice, c->stream));
+    const int nv = local_solve_variants();
+    int best = 0;
+    float best_ms = 0;
+    for (int v = 0; v < nv && !st; v++) {
+        float vmin = 0;
+        for (int rep = 0; rep < 3 && !st; rep++) {
+            st = cuda_ok(cudaMemcpyAsync(c->lwork, keep, nu * sizeof(double),
+                                         cudaMemcpyDeviceToDevice, c->stream));
+            a.solve_variant = v;
+            cudaEventRecord(e0, c->stream);
+            launch_local_solve(a, c->stream);
+            cudaEventRecord(e1, c->stream);
+            if (!st) st = cuda_ok(cudaEventSynchronize(e1));
+            if (!st) st = check_launch();
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep == 0 || ms < vmin) vmin = ms;
+        }
+        if (times_ms) times_ms[v] = vmin;
+        if (v == 0 || vmin < best_ms) {
+            best_ms = vmin;
+            best = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(keep);
+    if (st) return st;
+    c->solve_variant = best;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tuned_solve[tune_key(c)] = best;
+    }
+    if (chosen) *chosen = best;
     return VERB_OK;
 }
 

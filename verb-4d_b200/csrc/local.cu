@@ -432,28 +432,28 @@ __device__ __forceinline__ void cp_wait()
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-constexpr int SOLVE_WARPS = 4;
-#ifndef VERB_FWD_DEPTH
-#define VERB_FWD_DEPTH 4
-#endif
-#ifndef VERB_BWD_DEPTH
-#define VERB_BWD_DEPTH 2
-#endif
-constexpr int FWD_DEPTH = VERB_FWD_DEPTH;  // L columns in flight per warp
-constexpr int BWD_DEPTH = VERB_BWD_DEPTH;  // U columns in flight per warp
+// Solve variants: warps (systems) per CTA, L and U factor columns in flight
+// per warp.  More columns in flight hide more latency per warp but take
+// shared memory that would otherwise hold more resident warps; the best
+// trade depends on the grid, so the autotuner picks one per context.
+struct SolveShape {
+    int warps, fwd, bwd;
+};
+constexpr SolveShape SOLVE_SHAPES[] = {{4, 4, 2}, {4, 4, 4}, {4, 6, 3}, {2, 4, 2},
+                                       {2, 6, 4}, {8, 4, 2}, {8, 4, 3}, {1, 8, 6}};
+constexpr int N_SOLVE_SHAPES = sizeof(SOLVE_SHAPES) / sizeof(SOLVE_SHAPES[0]);
 constexpr int FWD_WIN = 128;   // >= kl + 1
 constexpr int BWD_WIN = 256;   // >= kv + 1
 
 // ring of factor columns per warp, in doubles (16-byte multiples)
-__host__ __device__ constexpr size_t solve_ring_doubles(int klp, int kvp, int esize)
+__host__ __device__ constexpr size_t solve_ring_doubles(int klp, int kvp, int esize, int fd, int bd)
 {
-    return ((size_t)(FWD_DEPTH * klp > BWD_DEPTH * kvp ? FWD_DEPTH * klp : BWD_DEPTH * kvp) * esize +
-            15) / 16 * 2;
+    return ((size_t)(fd * klp > bd * kvp ? fd * klp : bd * kvp) * esize + 15) / 16 * 2;
 }
 
 // T: storage type of the factors.  The substitutions run in FP64 either way
 // (float factors are widened as they are used).
-template <typename T>
+template <typename T, int SOLVE_WARPS, int FWD_DEPTH, int BWD_DEPTH>
 __global__ void __launch_bounds__(SOLVE_WARPS * 32) local_solve_kernel(LocalArgs a, int nsys)
 {
     extern __shared__ double sm[];
@@ -465,7 +465,7 @@ __global__ void __launch_bounds__(SOLVE_WARPS * 32) local_solve_kernel(LocalArgs
     const bool f32 = sizeof(T) == sizeof(float);
     const int kl = a.kl, kv = a.kv, klp = f32 ? a.klp32 : a.klp, kvp = f32 ? a.kvp32 : a.kvp;
     constexpr int VEC = 16 / sizeof(T);  // elements per 16-byte cp.async
-    const size_t per_warp = BWD_WIN + solve_ring_doubles(klp, kvp, sizeof(T));
+    const size_t per_warp = BWD_WIN + solve_ring_doubles(klp, kvp, sizeof(T), FWD_DEPTH, BWD_DEPTH);
     double* win = sm + (size_t)warp * per_warp;
     T* ring = (T*)(win + BWD_WIN);
     double* w = a.work + u0;
@@ -1032,23 +1032,63 @@ void launch_local_store(const LocalArgs& a, cudaStream_t s)
     local_store_kernel<<<grid, dim3(32, 8), 0, s>>>(a);
 }
 
-void launch_local_solve(const LocalArgs& a, cudaStream_t s)
+namespace {
+
+template <typename T, int W, int FD, int BD>
+void launch_solve_t(const LocalArgs& a, const size_t kl_p, const size_t kv_p, cudaStream_t s)
 {
     const int nsys = a.d.P * a.d.R;
-    const int grid = (nsys + SOLVE_WARPS - 1) / SOLVE_WARPS;
-    if (a.factors32) {
-        const size_t smem = (size_t)SOLVE_WARPS *
-                            (BWD_WIN + solve_ring_doubles(a.klp32, a.kvp32, sizeof(float))) *
-                            sizeof(double);
-        allow_max_dynamic_smem((const void*)local_solve_kernel<float>);
-        local_solve_kernel<float><<<grid, SOLVE_WARPS * 32, smem, s>>>(a, nsys);
-    } else {
-        const size_t smem = (size_t)SOLVE_WARPS *
-                            (BWD_WIN + solve_ring_doubles(a.klp, a.kvp, sizeof(double))) *
-                            sizeof(double);
-        allow_max_dynamic_smem((const void*)local_solve_kernel<double>);
-        local_solve_kernel<double><<<grid, SOLVE_WARPS * 32, smem, s>>>(a, nsys);
+    const int grid = (nsys + W - 1) / W;
+    const size_t smem =
+        (size_t)W * (BWD_WIN + solve_ring_doubles((int)kl_p, (int)kv_p, sizeof(T), FD, BD)) *
+        sizeof(double);
+    allow_max_dynamic_smem((const void*)local_solve_kernel<T, W, FD, BD>);
+    local_solve_kernel<T, W, FD, BD><<<grid, W * 32, smem, s>>>(a, nsys);
+}
+
+template <typename T>
+void launch_solve_v(const LocalArgs& a, int v, size_t klp, size_t kvp, cudaStream_t s)
+{
+    switch (v) {
+#define VERB_SOLVE_CASE(i)                                                                   \
+    case i:                                                                                  \
+        launch_solve_t<T, SOLVE_SHAPES[i].warps, SOLVE_SHAPES[i].fwd, SOLVE_SHAPES[i].bwd>( \
+            a, klp, kvp, s);                                                                 \
+        break;
+        VERB_SOLVE_CASE(1)
+        VERB_SOLVE_CASE(2)
+        VERB_SOLVE_CASE(3)
+        VERB_SOLVE_CASE(4)
+        VERB_SOLVE_CASE(5)
+        VERB_SOLVE_CASE(6)
+        VERB_SOLVE_CASE(7)
+#undef VERB_SOLVE_CASE
+        default:
+            launch_solve_t<T, SOLVE_SHAPES[0].warps, SOLVE_SHAPES[0].fwd, SOLVE_SHAPES[0].bwd>(
+                a, klp, kvp, s);
     }
+}
+
+}  // namespace
+
+static_assert(N_SOLVE_SHAPES == 8, "launch_solve_v lists every shape");
+
+int local_solve_variants() { return N_SOLVE_SHAPES; }
+
+void local_solve_variant_shape(int v, int* warps, int* fwd, int* bwd)
+{
+    const SolveShape& sh = SOLVE_SHAPES[v >= 0 && v < N_SOLVE_SHAPES ? v : 0];
+    *warps = sh.warps;
+    *fwd = sh.fwd;
+    *bwd = sh.bwd;
+}
+
+void launch_local_solve(const LocalArgs& a, cudaStream_t s)
+{
+    if (a.factors32)
+        launch_solve_v<float>(a, a.solve_variant, a.klp32, a.kvp32, s);
+    else
+        launch_solve_v<double>(a, a.solve_variant, a.klp, a.kvp, s);
 }
 
 }  // namespace verb

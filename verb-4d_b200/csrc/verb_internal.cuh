@@ -135,6 +135,8 @@ struct LocalArgs {
     // ConstantValue 0 boundary.  nullptr: every system is the full V*K grid.
     const int* k0;
     const long long* uoff;
+    // local solve shape (local_solve_variant_shape), chosen by the autotuner
+    int solve_variant;
     // optional per-system selection: only systems with (sel[sys] & sel_mask)
     // != 0 are processed
     const unsigned char* sel;
@@ -148,6 +150,8 @@ size_t local_factor_smem(int V);
 void launch_local_factor(const LocalArgs& a, cudaStream_t s);
 void launch_local_rhs(const LocalArgs& a, bool from_work, cudaStream_t s);
 void launch_local_solve(const LocalArgs& a, cudaStream_t s);
+int local_solve_variants();
+void local_solve_variant_shape(int v, int* warps, int* fwd, int* bwd);
 void launch_local_store(const LocalArgs& a, cudaStream_t s);
 // r = b - A x for every system (A assembled on the fly in the reference's order)
 void launch_local_residual(const LocalArgs& a, const double* b, const double* x, double* r,

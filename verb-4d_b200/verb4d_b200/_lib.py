@@ -91,6 +91,12 @@ SIGNATURES = {
     "verb_local_triples": (C.c_int, [_vp, C.c_double, C.c_double, _vp, _vp]),
     "verb_set_convection_arith": (C.c_int, [_vp, C.c_int]),
     "verb_set_step_graph": (C.c_int, [_vp, C.c_int]),
+    "verb_local_solve_variants": (C.c_int, [C.POINTER(C.c_int)]),
+    "verb_local_solve_variant": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                           C.POINTER(C.c_int)]),
+    "verb_set_local_solve_variant": (C.c_int, [_vp, C.c_int]),
+    "verb_autotune_local_solve": (C.c_int, [_vp, C.c_double, C.c_double, _dp,
+                                            C.POINTER(C.c_int)]),
     "verb_assimilate_convection": (C.c_int, [_vp, _dp, C.c_double, C.c_double, C.c_double, C.c_int,
                                              C.c_double, C.c_int, C.c_int, C.c_int]),
     "verb_convection_da_state": (C.c_int, [_vp, C.c_int, C.c_int, _dp, _dp]),

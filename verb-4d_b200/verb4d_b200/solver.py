@@ -94,6 +94,33 @@ class Context:
                                                   mm.ctypes.data_as(L._dp)), "da_state")
         return pa, mm
 
+    def solve_variants(self) -> list:
+        """(warps per CTA, L columns in flight, U columns in flight) of every
+        local-solve shape."""
+        n = C.c_int()
+        L.check(self.lib.verb_local_solve_variants(C.byref(n)), "variants")
+        out = []
+        for v in range(n.value):
+            w, f, b = C.c_int(), C.c_int(), C.c_int()
+            L.check(self.lib.verb_local_solve_variant(v, C.byref(w), C.byref(f), C.byref(b)),
+                    "variant")
+            out.append((w.value, f.value, b.value))
+        return out
+
+    def set_local_solve_variant(self, v: int = -1):
+        L.check(self.lib.verb_set_local_solve_variant(self.h, int(v)), "solve_variant")
+
+    def autotune_local_solve(self, dt: float, sub_dt: float):
+        """Time every local-solve shape on this context's systems and keep the
+        fastest; returns (chosen index, times in ms)."""
+        shapes = self.solve_variants()
+        t = np.zeros(len(shapes))
+        ch = C.c_int()
+        L.check(self.lib.verb_autotune_local_solve(self.h, float(dt), float(sub_dt),
+                                                   t.ctypes.data_as(L._dp), C.byref(ch)),
+                "autotune")
+        return ch.value, t
+
     def set_step_graph(self, enable: bool = True):
         """Replay steady-state steps from a captured CUDA graph."""
         L.check(self.lib.verb_set_step_graph(self.h, int(enable)), "step_graph")
