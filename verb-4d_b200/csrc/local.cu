@@ -439,8 +439,8 @@ __device__ __forceinline__ void cp_wait()
 struct SolveShape {
     int warps, fwd, bwd;
 };
-constexpr SolveShape SOLVE_SHAPES[] = {{4, 4, 2}, {4, 4, 4}, {4, 6, 3}, {2, 4, 2},
-                                       {2, 6, 4}, {8, 4, 2}, {8, 4, 3}, {1, 8, 6}};
+constexpr SolveShape SOLVE_SHAPES[] = {{4, 4, 2}, {4, 6, 3}, {2, 6, 4},  {2, 8, 6}, {1, 8, 6},
+                                       {1, 12, 8}, {1, 12, 10}, {1, 16, 12}, {1, 24, 16}};
 constexpr int N_SOLVE_SHAPES = sizeof(SOLVE_SHAPES) / sizeof(SOLVE_SHAPES[0]);
 constexpr int FWD_WIN = 128;   // >= kl + 1
 constexpr int BWD_WIN = 256;   // >= kv + 1
@@ -1062,6 +1062,7 @@ void launch_solve_v(const LocalArgs& a, int v, size_t klp, size_t kvp, cudaStrea
         VERB_SOLVE_CASE(5)
         VERB_SOLVE_CASE(6)
         VERB_SOLVE_CASE(7)
+        VERB_SOLVE_CASE(8)
 #undef VERB_SOLVE_CASE
         default:
             launch_solve_t<T, SOLVE_SHAPES[0].warps, SOLVE_SHAPES[0].fwd, SOLVE_SHAPES[0].bwd>(
@@ -1071,7 +1072,7 @@ void launch_solve_v(const LocalArgs& a, int v, size_t klp, size_t kvp, cudaStrea
 
 }  // namespace
 
-static_assert(N_SOLVE_SHAPES == 8, "launch_solve_v lists every shape");
+static_assert(N_SOLVE_SHAPES == 9, "launch_solve_v lists every shape");
 
 int local_solve_variants() { return N_SOLVE_SHAPES; }
 
