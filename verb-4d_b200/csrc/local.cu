@@ -302,16 +302,24 @@ __global__ void __launch_bounds__(FACT_THREADS) local_factor_kernel(LocalArgs a)
             const int ncol = ju - j;
             const int cg = tid & 127;        // column lane
             const int rg = tid >> 7;         // row group 0..3
+            // window slots advance with a wrap instead of a modulo per element
+            // (RW = kl + 1 >= 4, so one subtraction suffices)
+            const int r0 = (j + 1 + rg) % RW;
+            int cs = (j + 1 + cg) % CW;
             for (int cc = cg; cc < ncol; cc += 128) {
-                const int cs = (j + 1 + cc) % CW;
                 const double yv = W[rsj * CW + cs];
                 if (yv != 0.0) {
                     const double tmp = -yv;
+                    int r = r0;
                     for (int i = 1 + rg; i <= km; i += 4) {
-                        double* w = &W[((j + i) % RW) * CW + cs];
+                        double* w = &W[r * CW + cs];
                         *w = *w + mult[i] * tmp;  // xGER: A(i,k) + x(i)*temp
+                        r += 4;
+                        if (r >= RW) r -= RW;
                     }
                 }
+                cs += 128;
+                while (cs >= CW) cs -= CW;
             }
         }
         __syncthreads();
