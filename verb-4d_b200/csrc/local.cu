@@ -175,7 +175,12 @@ __device__ __forceinline__ bool skip_system(const LocalArgs& a, int sys)
 }
 
 constexpr int FACT_THREADS = 512;
-constexpr int STAGE_ROWS = 128;
+constexpr int FACT_COLS = 7;  // columns per lane in the rank-1 update: kv + 1 <= 224 (V <= 111)
+// Assembled rows are staged in a ring of STAGE_ROWS rows, a whole ring at a
+// time (one row per thread), when the window's next entering row reaches a
+// multiple of STAGE_ROWS.  256 rows (18 KB) still fit beside the window at
+// V = 111.
+constexpr int STAGE_ROWS = 256;
 
 // The factorisation always runs in FP64 (pivots and multipliers as LAPACK's);
 // T is the storage type of the factors: double, or float for the
@@ -208,7 +213,7 @@ __global__ void __launch_bounds__(FACT_THREADS) local_factor_kernel(LocalArgs a)
     const int tid = threadIdx.x;
 
     auto stage_rows = [&](int q0) {
-        for (int q = q0 + tid; q < q0 + 32 && q < n; q += blockDim.x) {
+        for (int q = q0 + tid; q < q0 + STAGE_ROWS && q < n; q += blockDim.x) {
             double r[9];
             const int st = assemble_row(v, types, a.dt, q, r);
             if (st) set_error(a.status, st);
@@ -227,7 +232,7 @@ __global__ void __launch_bounds__(FACT_THREADS) local_factor_kernel(LocalArgs a)
     };
 
     for (int i = tid; i < RW * CW; i += blockDim.x) W[i] = 0.0;
-    for (int q0 = 0; q0 < STAGE_ROWS; q0 += 32) stage_rows(q0);
+    stage_rows(0);
     __syncthreads();
     // rows 0..kl into the window (columns 0..kv)
     for (int i = tid; i < RW * CW; i += blockDim.x) {
@@ -299,33 +304,39 @@ __global__ void __launch_bounds__(FACT_THREADS) local_factor_kernel(LocalArgs a)
         for (int c = j + tid; c <= ju && c <= j + kv; c += blockDim.x)
             Uf[(size_t)c * kvp + (kv - (c - j))] = (T)W[rsj * CW + (c % CW)];
         if (nz && km > 0 && ju > j) {
-            const int ncol = ju - j;
-            const int cg = tid & 127;        // column lane
-            const int rg = tid >> 7;         // row group 0..3
-            // window slots advance with a wrap instead of a modulo per element
-            // (RW = kl + 1 >= 4, so one subtraction suffices)
-            const int r0 = (j + 1 + rg) % RW;
-            int cs = (j + 1 + cg) % CW;
-            for (int cc = cg; cc < ncol; cc += 128) {
-                const double yv = W[rsj * CW + cs];
-                if (yv != 0.0) {
-                    const double tmp = -yv;
-                    int r = r0;
-                    for (int i = 1 + rg; i <= km; i += 4) {
-                        double* w = &W[r * CW + cs];
-                        *w = *w + mult[i] * tmp;  // xGER: A(i,k) + x(i)*temp
-                        r += 4;
-                        if (r >= RW) r -= RW;
-                    }
-                }
-                cs += 128;
+            // warp w updates rows w+1, w+1+nw, ...; lane l columns j+1+l+32k.
+            // The pivot row's values (negated, as xGER's temp) stay in
+            // registers; window slots advance by wrap, not modulo.
+            const int ncol = ju - j;  // <= kv <= 32 * FACT_COLS
+            const int lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+            double ty[FACT_COLS];
+            int csl[FACT_COLS];
+            int cs = (j + 1 + lane) % CW;
+#pragma unroll
+            for (int k = 0; k < FACT_COLS; k++) {
+                csl[k] = cs;
+                ty[k] = (lane + 32 * k < ncol) ? -W[rsj * CW + cs] : 0.0;
+                cs += 32;
                 while (cs >= CW) cs -= CW;
+            }
+            int r = (j + 1 + wid) % RW;
+            for (int i = 1 + wid; i <= km; i += nw) {
+                const double m = mult[i];
+                double* Wr = W + (size_t)r * CW;
+#pragma unroll
+                for (int k = 0; k < FACT_COLS; k++)
+                    if (ty[k] != 0.0) {
+                        double* w = Wr + csl[k];
+                        *w = *w + m * ty[k];  // xGER: A(i,k) + x(i)*temp, temp = -y(k)
+                    }
+                r += nw;
+                while (r >= RW) r -= RW;
             }
         }
         __syncthreads();
         // [D] slide: row slot j <- original row j+kl+1, column slot j <- column j+kv+1
         const int q = j + kl + 1;
-        if (q < n && (q & 31) == 0 && q >= STAGE_ROWS) {
+        if (q < n && (q & (STAGE_ROWS - 1)) == 0 && q >= STAGE_ROWS) {
             stage_rows(q);
             __syncthreads();
         }
