@@ -51,6 +51,25 @@ def rank_info():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
+def max_over_ranks(value, device=None):
+    """The largest of every rank's value (a time: the job ends with its
+    slowest replica); the value itself in a single process."""
+    import torch
+    import torch.distributed as dist
+
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(sim_hours_per_rank, seconds_max, world):
+    """Whole-job sim-hours/s of `world` independent replicas that each
+    simulate `sim_hours_per_rank`, timed by the slowest one."""
+    return world * sim_hours_per_rank / seconds_max
+
+
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons during the timed region."""
 
@@ -282,12 +301,9 @@ def run_ours(args):
     else:
         ctx.close()
         del solver, ctx
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dev)
     sim_h = args.steps * wl.dt * 24.0
-    value = world * sim_h / (ms / 1e3)
+    value = replica_throughput(sim_h, ms / 1e3, world)
 
     # ---------------- end to end through the public API with host buffers (e2e)
     e2e = None
@@ -342,11 +358,8 @@ def run_ours(args):
         torch.cuda.synchronize(dev)
         e2e_s = time.perf_counter() - t0
         s2.ctx.close()
-        if world > 1:
-            t = torch.tensor([e2e_s], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        e2e = {"value": world * sim_h / e2e_s, "unit": "sim-hours/s",
+        e2e_s = max_over_ranks(e2e_s, dev)
+        e2e = {"value": replica_throughput(sim_h, e2e_s, world), "unit": "sim-hours/s",
                "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
                "includes": "host upload of every input field, one-time LU/Thomas factorisations, "
                            "hourly velocity uploads, per-step negative count and hourly PSD reads",
