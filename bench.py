@@ -46,6 +46,12 @@ HBM_FALLBACK = 6650.0
 
 
 # --------------------------------------------------------------------------- utils
+# DRAM bytes per algorithmic byte of the local solve: one ncu capture at
+# 48x101x101x8 (the production band, 4848 systems of 808 unknowns) read
+# 9,735,437,568 + wrote 66,170,624 bytes for 9,698,947,584 algorithmic bytes
+SOLVE_TRAFFIC_PER_ALG_BYTE = (9735437568 + 66170624) / 9698947584
+
+
 def rank_info():
     return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
             int(os.environ.get("LOCAL_RANK", "0")))
@@ -420,7 +426,12 @@ def run_ours(args):
                      "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                      "algorithmic_bytes_per_launch": int(alg_bytes),
-                     "traffic": args.traffic},
+                     "traffic": (args.traffic if args.traffic is not None
+                                 else int(alg_bytes * SOLVE_TRAFFIC_PER_ALG_BYTE)),
+                     "traffic_source": ("given on the command line" if args.traffic is not None
+                                        else "ncu dram__bytes_read+write of one launch at "
+                                             "48x101x101x8 (same band), scaled by the "
+                                             "algorithmic bytes")},
         "roofline_fp64": {"kernel": "convection_kernel (ULTIMATE-QUICKEST sweeps, FP64 vector)",
                           "bound": "fp64", "achieved": round(conv_tops, 3), "peak": fp64_peak,
                           "unit": "TOP/s", "frac": round(conv_tops / fp64_peak, 4),
