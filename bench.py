@@ -429,9 +429,9 @@ def run_ours(args):
                      "traffic": (args.traffic if args.traffic is not None
                                  else int(alg_bytes * SOLVE_TRAFFIC_PER_ALG_BYTE)),
                      "traffic_source": ("given on the command line" if args.traffic is not None
-                                        else "ncu dram__bytes_read+write of one launch at "
-                                             "48x101x101x8 (same band), scaled by the "
-                                             "algorithmic bytes")},
+                                        else "algorithmic bytes x 1.0106, the DRAM/algorithmic "
+                                             "ratio of one ncu-captured launch at 48x101x101x8 "
+                                             "(the 48x101x101x91 band, kl = 102)")},
         "roofline_fp64": {"kernel": "convection_kernel (ULTIMATE-QUICKEST sweeps, FP64 vector)",
                           "bound": "fp64", "achieved": round(conv_tops, 3), "peak": fp64_peak,
                           "unit": "TOP/s", "frac": round(conv_tops / fp64_peak, 4),
