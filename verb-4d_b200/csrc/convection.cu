@@ -28,7 +28,7 @@
 // runs about 10 % faster and differs from the reference by a few units in the
 // last place per step (launch_convection_fma); it also takes the Courant
 // factors as products with rounded reciprocals instead of exactly rounded
-// quotients.
+// quotients, and runs nine warps per CTA instead of eight.
 #include "verb_internal.cuh"
 
 #ifdef VERB_BUILD_CONV_FMA
@@ -432,7 +432,14 @@ __device__ __forceinline__ double block_max(double v, double* red)
 // per-slice planes G, exp(Loss dt), S dt and the face Courant tables live in a
 // per-CTA scratch region that stays resident in L2.
 
+// Warps per CTA (two CTAs per SM).  The contracted build needs fewer
+// registers (113 fit), so nine warps per CTA fit beside the exact build's
+// eight in the same shared memory and register file.
+#ifdef VERB_BUILD_CONV_FMA
+constexpr int C3_WARPS = 9;
+#else
 constexpr int C3_WARPS = 8;
+#endif
 constexpr int C3_THREADS = C3_WARPS * 32;
 constexpr int TMAX = 16;  // cells per lane: lines of up to 32*TMAX points
 
@@ -1154,12 +1161,28 @@ using namespace VERB_CONV_NS;
 
 #ifdef VERB_BUILD_CONV_FMA
 
+size_t conv_smem_bytes_fma(int P, int R)
+{
+    return ((size_t)conv_wall_offset(P, R) + (size_t)C3_WARPS * conv_wstride(P, R)) * sizeof(double);
+}
+
+int conv_check_fma(int P, int R)
+{
+    if ((P >= 3 && sweep_cfg(P, R - 1).lpl == 0) || (R >= 3 && sweep_cfg(R, P).lpl == 0))
+        return VERB_ERR_SIZE;
+    int dev = 0, maxsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (conv_smem_bytes_fma(P, R) > (size_t)maxsm) return VERB_ERR_SIZE;
+    return VERB_OK;
+}
+
 int conv_ctas_fma(int P, int R)
 {
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const size_t smem = conv_smem_bytes(P, R);
+    const size_t smem = conv_smem_bytes_fma(P, R);
     allow_max_dynamic_smem((const void*)convection_kernel);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, convection_kernel, C3_THREADS, smem);
     if (per < 1) per = 1;
@@ -1168,7 +1191,7 @@ int conv_ctas_fma(int P, int R)
 
 void launch_convection_fma(const ConvArgs& a, int nctas, cudaStream_t s)
 {
-    const size_t smem = conv_smem_bytes(a.d.P, a.d.R);
+    const size_t smem = conv_smem_bytes_fma(a.d.P, a.d.R);
     allow_max_dynamic_smem((const void*)convection_kernel);
     convection_kernel<<<nctas, C3_THREADS, smem, s>>>(a);
 }

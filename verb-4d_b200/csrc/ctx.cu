@@ -960,7 +960,7 @@ int conv_run(verb_ctx* c, double dt)
         int s = need_bc(c, b);
         if (s) return s;
     }
-    if (int s = conv_check(d.P, d.R)) return s;
+    if (int s = (c->conv_arith == VERB_CONV_FMA ? conv_check_fma : conv_check)(d.P, d.R)) return s;
     if (!c->conv_nctas) c->conv_nctas = std::max(conv_ctas(d.P, d.R), conv_ctas_fma(d.P, d.R));
     CK(alloc((void**)&c->conv_scratch,
              (size_t)c->conv_nctas * conv_scratch_doubles(d.P, d.R) * sizeof(double)));

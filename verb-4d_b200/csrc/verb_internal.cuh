@@ -108,6 +108,8 @@ size_t conv_scratch_doubles(int P, int R);
 void launch_convection(const ConvArgs& a, int nctas, cudaStream_t s);
 // the same kernel compiled with multiply-add contraction (convection.cu)
 int conv_ctas_fma(int P, int R);
+int conv_check_fma(int P, int R);
+size_t conv_smem_bytes_fma(int P, int R);
 void launch_convection_fma(const ConvArgs& a, int nctas, cudaStream_t s);
 void launch_convection_line(double* psd, const double* x, int n, double lbc, double ubc, int lbc_t,
                             int ubc_t, const double* ux, double dt, int* status, cudaStream_t s);
