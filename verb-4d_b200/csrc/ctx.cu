@@ -1,166 +1,9 @@
 // C ABI: context lifetime, uploads, cache invalidation, phase dispatch, timing,
 // and the per-slice entry points.  See include/verb4d_b200.h.
-#include <cuda_runtime.h>
+#include "ctx_internal.cuh"
 
-#include <cmath>
-#include <cstdio>
-#include <cstring>
-#include <deque>
-#include <map>
-#include <mutex>
-#include <tuple>
-#include <new>
-#include <string>
-#include <thread>
-#include <algorithm>
-#include <utility>
-#include <vector>
+namespace vctx {
 
-#include "verb_internal.cuh"
-
-using namespace verb;
-
-namespace {
-
-enum Phase { PH_CONV = 0, PH_RAD, PH_RADF, PH_LOCAL, PH_LOCF, PH_LOCS, PH_RED, PH_KF, PH_N };
-
-struct EventPair {
-    cudaEvent_t a, b;
-};
-
-}  // namespace
-
-// One component of an updatable field (src/UpdatableMatrix.h:60-90): base
-// array, queued replacement arrays, scale and limit queues.
-struct UpdComponent {
-    double* base = nullptr;
-    std::deque<std::pair<double, double*>> data_q;           // (time, device array)
-    std::deque<std::pair<double, double>> scale_q;
-    std::deque<std::pair<double, double>> limit_q[4][2];     // [axis][from, to]
-    double scale = 1.0;                                       // latest_scale_coefficient
-    double lim[4][2] = {{-1e99, 1e99}, {-1e99, 1e99}, {-1e99, 1e99}, {-1e99, 1e99}};
-    double last_update_time = -1;
-};
-struct UpdField {
-    std::vector<UpdComponent> comps;
-    int merge = VERB_MERGE_SUM;
-    bool built = false;
-};
-
-struct verb_ctx {
-    Dims d{};
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    double* f[VERB_F_COUNT] = {};
-    double* fbase[VERB_F_COUNT] = {};   // unscaled copy when a scale != 1 is set
-    double scale[VERB_F_COUNT];
-    bool uploaded[VERB_F_COUNT] = {};
-    double* bc[VERB_BCF_COUNT] = {};
-    int bct[VERB_BCF_COUNT];
-    int radial_sources = 0, local_sources = 1, include_boundary = 1, positive_psd = 0;
-    // radial Thomas factors
-    double *rfa = nullptr, *rfbet = nullptr, *rfgam = nullptr;
-    bool radial_dirty = true;
-    double radial_dt = -1;
-    // local LU factors
-    double *Lf = nullptr, *Uf = nullptr, *lwork = nullptr;
-    int32_t* ipiv = nullptr;
-    int kl = 0, kv = 0, klp = 0, kvp = 0;
-    // mixed-precision form: FP32 factors, FP64 refinement (rhs copy, residual)
-    int local_prec = VERB_PREC_FP64, refine_iters = 0;
-    float *Lf32 = nullptr, *Uf32 = nullptr;
-    int klp32 = 0, kvp32 = 0;
-    double *lrhs = nullptr, *lres = nullptr;
-    unsigned long long* refine_red = nullptr;  // max |last correction|, max |x|
-    // ragged (trimmed) local systems: first pitch-angle index per (P,R)
-    // system and the first unknown of each system
-    int* trim_k0 = nullptr;
-    long long* trim_uoff = nullptr;
-    size_t local_unknowns = 0;  // unknowns of all systems (trimmed or full)
-    // convection data assimilation: per (V,K) slice the model matrix cache
-    // and Pa (N x N, N = P*R); chunk work space (4 N x N per slice), vectors
-    // (t, x, y) and integer lists
-    double *kc_M = nullptr, *kc_Pa = nullptr, *kc_W = nullptr, *kc_vec = nullptr;
-    int* kc_int = nullptr;
-    bool kc_valid = false;
-    int kc_chunk = 0;
-    // Krylov form: FP32 diagonals and BiCGSTAB vectors, FP64 b / x / r / d,
-    // CNN features and output, per-system scale, iterations, pending flags
-    float *kA9 = nullptr, *kscr = nullptr, *kfeat = nullptr, *kout = nullptr;
-    double *kb = nullptr, *kx = nullptr, *kr = nullptr, *kd = nullptr, *kscale = nullptr;
-    double* kprev = nullptr;              // previous relative residual per system
-    int* kiters = nullptr;
-    unsigned char* kpend = nullptr;
-    unsigned int* kcount = nullptr;       // [0] pending systems, [1] given up
-    unsigned long long* kmax = nullptr;   // [0] max relative residual key, [2..3] update maxima
-    bool local_dirty = true;
-    double local_dt = -1;
-    int solve_variant = -1;  // local solve shape; -1: the process-wide tuned one, else 0
-    const double* dkv_override = nullptr;  // Dyx for the per-slice entry point
-    // convection
-    double* conv_scratch = nullptr;
-    int* conv_substeps = nullptr;
-    int* ticket = nullptr;
-    int conv_nctas = 0;
-    int conv_arith = VERB_CONV_EXACT;
-    // reductions / status
-    unsigned long long* red = nullptr;  // [0] negatives, [1] tensor min key
-    int* status = nullptr;
-    bool tensor_dirty = true;
-    double tensor_min = 0;
-    // Kalman filter
-    double *Pa = nullptr, *kfwork = nullptr, *obs = nullptr;
-    size_t kfwork_bytes = 0;
-    int* kfticket = nullptr;
-    int pa_p_index = -2;  // the p_index Pa was sized for (-2: not yet)
-    // updatable fields (nullptr: plain uploaded field)
-    UpdField* upd[VERB_F_COUNT] = {};
-    // asynchronous output: device snapshot -> pinned host copy on a copy
-    // stream -> file written by a host thread
-    double* out_snap = nullptr;
-    double* out_host = nullptr;
-    cudaStream_t out_stream = nullptr;
-    cudaEvent_t out_ev_snap = nullptr, out_ev_host = nullptr;
-    std::thread out_thread;
-    int out_status = VERB_OK;
-    // CUDA graph of the steady-state step (captured on first use, replayed
-    // while nothing the step's launches depend on changes)
-    bool use_graph = false;
-    bool graph_valid = false;
-    cudaGraphExec_t step_exec = nullptr;
-    double g_dt = 0, g_sub_dt = 0;
-    int g_flags = 0;
-    long long g_launches = 0;
-    // timing
-    bool timing = false;
-    std::vector<EventPair> ev[PH_N];
-    std::vector<EventPair> pool;
-    verb_timing acc{};
-};
-
-namespace {
-
-// anything that changes a launch argument of the step (a field other than the
-// PSD, scales, boundary types, options, forms) drops the captured step graph
-inline void graph_invalidate(verb_ctx* c) { c->graph_valid = false; }
-
-int cuda_ok(cudaError_t e)
-{
-    if (e == cudaSuccess) return VERB_OK;
-    if (e == cudaErrorMemoryAllocation) return VERB_ERR_NOMEM;
-    return VERB_ERR_CUDA;
-}
-
-int cuda_ok(int s) { return s; }
-
-#define CK(x)                                 \
-    do {                                      \
-        int _s = cuda_ok(x);                  \
-        if (_s != VERB_OK) return _s;         \
-    } while (0)
-
-size_t npts(const verb_ctx* c) { return c->d.npts(); }
 
 size_t bc_elems(const verb_ctx* c, int b)
 {
@@ -245,27 +88,7 @@ EventPair get_pair(verb_ctx* c)
     return p;
 }
 
-struct PhaseTimer {
-    verb_ctx* c;
-    int ph;
-    EventPair p{};
-    PhaseTimer(verb_ctx* c_, int ph_) : c(c_), ph(ph_)
-    {
-        if (c->timing) {
-            p = get_pair(c);
-            cudaEventRecord(p.a, c->stream);
-        }
-    }
-    ~PhaseTimer()
-    {
-        if (c->timing) {
-            cudaEventRecord(p.b, c->stream);
-            c->ev[ph].push_back(p);
-        }
-    }
-};
 
-int check_launch() { return cuda_ok(cudaGetLastError()); }
 
 int radial_run(verb_ctx* c, double dt)
 {
@@ -502,447 +325,6 @@ int local_run(verb_ctx* c, double dt, double sub_dt)
     return check_launch();
 }
 
-void free_krylov(verb_ctx* c)
-{
-    for (void** p : {(void**)&c->kA9, (void**)&c->kscr, (void**)&c->kfeat, (void**)&c->kout,
-                     (void**)&c->kb, (void**)&c->kx, (void**)&c->kr, (void**)&c->kd,
-                     (void**)&c->kscale, (void**)&c->kiters, (void**)&c->kpend,
-                     (void**)&c->kcount, (void**)&c->kmax, (void**)&c->kprev}) {
-        cudaFree(*p);
-        *p = nullptr;
-    }
-}
-
-int krylov_buffers(verb_ctx* c, bool features)
-{
-    const size_t nu = c->local_unknowns;
-    const size_t ns = (size_t)c->d.P * c->d.R;
-    CK(alloc((void**)&c->kb, nu * sizeof(double)));
-    CK(alloc((void**)&c->kscale, ns * sizeof(double)));
-    if (!c->kpend) {
-        // systems the residual check skips keep pend = 0
-        CK(alloc((void**)&c->kpend, ns));
-        CK(cudaMemsetAsync(c->kpend, 0, ns, c->stream));
-    }
-    CK(alloc((void**)&c->kcount, 2 * sizeof(unsigned int)));
-    CK(alloc((void**)&c->kmax, 4 * sizeof(unsigned long long)));
-    if (features) {
-        if (!c->kfeat) {
-            // skipped systems keep zero features: the network reads them too
-            CK(alloc((void**)&c->kfeat, nu * 4 * sizeof(float)));
-            CK(cudaMemsetAsync(c->kfeat, 0, nu * 4 * sizeof(float), c->stream));
-        }
-        CK(alloc((void**)&c->kout, nu * sizeof(float)));
-    }
-    return VERB_OK;
-}
-
-// The local step with the Krylov solve (see verb_local_krylov).
-int krylov_run(verb_ctx* c, double dt, double sub_dt, int guess, verb_cnn* cnn, int smooth,
-               double omega, int max_outer, int inner_maxit, double inner_tol, double resid_tol,
-               verb_krylov_stats* stats)
-{
-    const Dims& d = c->d;
-    if (stats) *stats = verb_krylov_stats{};
-    if (d.V < 3 || d.K < 3) return VERB_OK;
-    const int nsys = d.P * d.R;
-    if (cnn) {
-        int ci, co, H, W, mb;
-        CK(cnn_shape(cnn, &ci, &co, &H, &W, &mb));
-        if (ci != 4 || co != 1 || H != d.K || W != d.V || mb < nsys || c->trim_k0)
-            return VERB_ERR_ARG;
-    }
-    int nsub = (int)(dt / sub_dt);
-    if (nsub < 1) nsub = 1;
-    const double dts = dt / nsub;
-    LocalArgs a{};
-    int s = local_prepare(c, a, dts);
-    if (s) return s;
-    PhaseTimer t(c, PH_LOCAL);
-    const size_t nu = c->local_unknowns;
-    CK(krylov_buffers(c, cnn != nullptr));
-    for (double** p : {&c->kx, &c->kr, &c->kd}) CK(alloc((void**)p, nu * sizeof(double)));
-    CK(alloc((void**)&c->kA9, nu * 9 * sizeof(float)));
-    CK(alloc((void**)&c->kscr, nu * 6 * sizeof(float)));
-    CK(alloc((void**)&c->kiters, nsys * sizeof(int)));
-    CK(alloc((void**)&c->kprev, nsys * sizeof(double)));
-    // the FP32 matrices depend on the coefficients and the sub-step only;
-    // they are rebuilt every call (one pass over the coefficient fields)
-    launch_local_assemble32(a, c->kA9, c->stream);
-    c->acc.kernel_launches++;
-    verb_krylov_stats st{};
-    double guess_max = 0, res_max = 0;
-    for (int k = 0; k < nsub; k++) {
-        // the state the sub-step starts from, in the unknown order: the PSD
-        // on the first sub-step, the previous sub-step's solution (kx) after
-        double* fstate = c->kx;
-        if (k == 0 && guess != VERB_GUESS_ZERO) {
-            fstate = c->kd;
-            launch_gather_state(a, fstate, c->stream);
-            c->acc.kernel_launches++;
-        }
-        launch_local_rhs(a, k > 0, c->stream);
-        CK(cudaMemcpyAsync(c->kb, c->lwork, nu * sizeof(double), cudaMemcpyDeviceToDevice,
-                           c->stream));
-        c->acc.kernel_launches++;
-        if (guess == VERB_GUESS_ZERO) {
-            CK(cudaMemsetAsync(c->kx, 0, nu * sizeof(double), c->stream));
-        } else if (guess == VERB_GUESS_PREV) {
-            launch_warm_start(a, fstate, nullptr, c->kscale, c->kx, c->stream);
-            c->acc.kernel_launches++;
-        } else {
-            launch_local_features(a, fstate, c->kfeat, c->kscale, c->stream);
-            CK(cnn_forward_on(cnn, c->kfeat, c->kout, nsys, c->stream));
-            launch_warm_start(a, fstate, c->kout, c->kscale, c->kx, c->stream);
-            c->acc.kernel_launches += 2 + 4;  // features, warm start, 4 conv layers
-        }
-        // smoothing sweeps damp the guess's high-frequency error, which the
-        // stiff rows amplify in the residual
-        for (int sw = 0; sw < smooth; sw++) {
-            launch_local_residual(a, c->kb, c->kx, c->kr, c->stream);
-            launch_jacobi_update(a, c->kA9, c->kr, c->kx, omega, c->stream);
-            c->acc.kernel_launches += 2;
-        }
-        // outer passes: check, then correct the pending systems; a pass
-        // that leaves a system's FP64 residual above a tenth of its previous
-        // value sends the system to the LU
-        unsigned int cnt[2] = {0, 0};
-        int pass = 0;
-        CK(cudaMemsetAsync(c->kprev, 0, nsys * sizeof(double), c->stream));
-        CK(cudaMemsetAsync(c->kiters, 0, nsys * sizeof(int), c->stream));
-        for (;; pass++) {
-            CK(cudaMemsetAsync(c->kcount, 0, 2 * sizeof(unsigned int), c->stream));
-            CK(cudaMemsetAsync(c->kmax, 0, sizeof(unsigned long long), c->stream));
-            launch_residual_check(a, c->kb, c->kx, resid_tol, 0.1, c->kprev, c->kpend, c->kcount,
-                                  c->kmax, c->stream);
-            c->acc.kernel_launches++;
-            unsigned long long key;
-            CK(cudaMemcpyAsync(cnt, c->kcount, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
-            CK(cudaMemcpyAsync(&key, c->kmax, sizeof(key), cudaMemcpyDeviceToHost, c->stream));
-            CK(cudaStreamSynchronize(c->stream));
-            const double rel = dkey_inv(key);
-            if (pass == 0) guess_max = fmax(guess_max, rel);
-            if (cnt[0] == 0 || pass == max_outer) {
-                res_max = fmax(res_max, rel);
-                break;
-            }
-            LocalArgs ap = a;
-            ap.sel = c->kpend;
-            ap.sel_mask = 1;
-            launch_local_residual(ap, c->kb, c->kx, c->kr, c->stream);
-            // the FP64 check decides convergence: no inner flag is kept
-            launch_bicgstab(ap, c->kA9, c->kr, c->kd, c->kscr, inner_maxit, (float)inner_tol,
-                            c->kiters, nullptr, c->stream);
-            launch_local_update(ap, c->kx, c->kd, c->kmax + 2, c->stream);
-            c->acc.kernel_launches += 3;
-        }
-        st.outer_passes += pass;
-        st.systems += nsys;
-        const unsigned int nfall = cnt[0] + cnt[1];
-        if (stats) {
-            std::vector<int> it(nsys);
-            std::vector<unsigned char> pe(nsys);
-            CK(cudaMemcpyAsync(it.data(), c->kiters, nsys * sizeof(int), cudaMemcpyDeviceToHost,
-                               c->stream));
-            CK(cudaMemcpyAsync(pe.data(), c->kpend, nsys, cudaMemcpyDeviceToHost, c->stream));
-            CK(cudaStreamSynchronize(c->stream));
-            for (int q = 0; q < nsys; q++) {
-                st.inner_iterations += it[q];
-                if (!pe[q]) st.solved_iterations += it[q];
-            }
-        }
-        if (nfall) {
-            // LU for the systems still above the tolerance: the rhs is in
-            // lwork; factor (those systems only) and solve in place, then
-            // take their solutions into x
-            LocalArgs ap = a;
-            ap.sel = c->kpend;
-            ap.sel_mask = 3;
-            s = alloc_factors(c, ap);
-            if (s) return s;
-            const size_t nuf = c->local_unknowns;
-            if (ap.factors32)
-                CK(cudaMemsetAsync(c->Uf32, 0, nuf * c->kvp32 * sizeof(float), c->stream));
-            else
-                CK(cudaMemsetAsync(c->Uf, 0, nuf * c->kvp * sizeof(double), c->stream));
-            launch_local_factor(ap, c->stream);
-            launch_local_solve(ap, c->stream);
-            launch_masked_copy(ap, c->kx, c->lwork, c->stream);
-            c->acc.kernel_launches += 3;
-            c->local_dirty = true;  // the factors of the other systems are stale
-            st.fallbacks += nfall;
-        }
-        CK(cudaMemcpyAsync(c->lwork, c->kx, nu * sizeof(double), cudaMemcpyDeviceToDevice,
-                           c->stream));
-    }
-    launch_local_store(a, c->stream);
-    c->acc.kernel_launches++;
-    s = check_launch();
-    if (s) return s;
-    if (stats) {
-        st.max_rel_residual = res_max;
-        st.guess_rel_residual = guess_max;
-        *stats = st;
-    }
-    return VERB_OK;
-}
-
-// A local LU step that also emits the CNN's training triples (see
-// verb_local_triples).
-int triples_run(verb_ctx* c, double dt, double sub_dt, float* feat, float* target)
-{
-    const Dims& d = c->d;
-    if (d.V < 3 || d.K < 3 || c->trim_k0) return VERB_ERR_ARG;
-    int nsub = (int)(dt / sub_dt);
-    if (nsub < 1) nsub = 1;
-    const double dts = dt / nsub;
-    LocalArgs a{};
-    int s = local_prepare(c, a, dts);
-    if (s) return s;
-    if (c->local_dirty || dts != c->local_dt) {
-        s = local_factor(c, a);
-        if (s) return s;
-    }
-    const size_t nu = c->local_unknowns;
-    CK(krylov_buffers(c, false));
-    for (int k = 0; k < nsub; k++) {
-        const bool last = k == nsub - 1;
-        if (last) {
-            // the state this sub-step starts from (kb, unknown order)
-            if (k == 0)
-                launch_gather_state(a, c->kb, c->stream);
-            else
-                CK(cudaMemcpyAsync(c->kb, c->lwork, nu * sizeof(double),
-                                   cudaMemcpyDeviceToDevice, c->stream));
-            launch_local_features(a, c->kb, feat, c->kscale, c->stream);
-        }
-        launch_local_rhs(a, k > 0, c->stream);
-        launch_local_solve(a, c->stream);
-        if (last) launch_local_targets(a, c->kb, c->lwork, c->kscale, target, c->stream);
-        c->acc.kernel_launches += last ? 5 : 2;
-    }
-    launch_local_store(a, c->stream);
-    c->acc.kernel_launches++;
-    return check_launch();
-}
-
-// ---- convection data assimilation ------------------------------------------
-
-void free_kc(verb_ctx* c)
-{
-    for (void** p : {(void**)&c->kc_M, (void**)&c->kc_Pa, (void**)&c->kc_W, (void**)&c->kc_vec,
-                     (void**)&c->kc_int})
-    {
-        cudaFree(*p);
-        *p = nullptr;
-    }
-    c->kc_valid = false;
-    c->kc_chunk = 0;
-}
-
-// out[b] = base[b]^e[b] for the slices of a chunk (binary exponentiation;
-// products of powers of one matrix commute, so the order of the factors
-// only changes rounding).  cur and sq hold the running square, tmp the
-// product; idx_dev is scratch for the per-bit slice lists.
-int kc_pow(verb_ctx* c, int nb, const double* base, size_t sbase, const std::vector<int>& e,
-           double* out, size_t sout, double* cur, double* sq, double* tmp, size_t sW, int* idx_dev)
-{
-    const int N = c->d.P * c->d.R;
-    const size_t NN = (size_t)N * N;
-    launch_kc_copy(base, sbase, cur, sW, NN, nb, nullptr, c->stream);
-    int emax = 0;
-    for (int v : e) emax = std::max(emax, v);
-    std::vector<char> started(nb, 0);
-    std::vector<int> sel;
-    auto gemm = [&](const double* A, size_t sA, const double* B, size_t sB, double* C, size_t sC,
-                    int batch, const int* idx) {
-        BGemm g{};
-        g.A = A; g.sA = sA; g.lda = N;
-        g.B = B; g.sB = sB; g.ldb = N;
-        g.C = C; g.sC = sC; g.ldc = N;
-        g.M = N; g.N = N; g.K = N;
-        g.sgn = 1.0;
-        g.idx = idx;
-        launch_bgemm(g, false, batch, c->stream);
-        c->acc.kernel_launches++;
-    };
-    for (int bit = 0; (1 << bit) <= emax; bit++) {
-        std::vector<int> first, mult;
-        for (int b = 0; b < nb; b++)
-            if (e[b] >> bit & 1) (started[b] ? mult : first).push_back(b);
-        if (!first.empty()) {
-            CK(cudaMemcpyAsync(idx_dev, first.data(), first.size() * sizeof(int),
-                               cudaMemcpyHostToDevice, c->stream));
-            launch_kc_copy(cur, sW, out, sout, NN, (int)first.size(), idx_dev, c->stream);
-            for (int b : first) started[b] = 1;
-        }
-        if (!mult.empty()) {
-            int* id2 = idx_dev + nb;
-            CK(cudaMemcpyAsync(id2, mult.data(), mult.size() * sizeof(int), cudaMemcpyHostToDevice,
-                               c->stream));
-            gemm(out, sout, cur, sW, tmp, sW, (int)mult.size(), id2);
-            launch_kc_copy(tmp, sW, out, sout, NN, (int)mult.size(), id2, c->stream);
-        }
-        if ((2 << bit) <= emax) {
-            gemm(cur, sW, cur, sW, sq, sW, nb, nullptr);
-            std::swap(cur, sq);
-        }
-        // the host lists are reused by the next bit: let the copies finish
-        CK(cudaStreamSynchronize(c->stream));
-    }
-    return VERB_OK;
-}
-
-int kc_run(verb_ctx* c, const double* obs_host, double dt, double model_error, double obs_error,
-           int use_log, double corr_time, int growing_q, int has_vx_updated, int chunk)
-{
-    const Dims& d = c->d;
-    for (int fid : {VERB_F_PSD, VERB_F_P, VERB_F_R, VERB_F_VP, VERB_F_VR}) {
-        int s = need_field(c, fid);
-        if (s) return s;
-    }
-    if (d.P < 3 || d.R < 3) return VERB_ERR_GRID;
-    const int N = d.P * d.R;
-    const size_t NN = (size_t)N * N;
-    const int nsl = d.V * d.K;
-    // persistent: the model matrix cache and Pa of every slice
-    if (!c->kc_M) {
-        CK(alloc((void**)&c->kc_M, (size_t)nsl * NN * sizeof(double)));
-        CK(alloc((void**)&c->kc_Pa, (size_t)nsl * NN * sizeof(double)));
-        CK(cudaMemsetAsync(c->kc_Pa, 0, (size_t)nsl * NN * sizeof(double), c->stream));
-        c->kc_valid = false;
-    }
-    int B = chunk > 0 ? chunk : (int)std::max<size_t>(1, ((size_t)4 << 30) / (4 * NN * sizeof(double)));
-    B = std::min(B, nsl);
-    if (c->kc_chunk != B) {
-        for (void** p : {(void**)&c->kc_W, (void**)&c->kc_vec, (void**)&c->kc_int}) {
-            cudaFree(*p);
-            *p = nullptr;
-        }
-        c->kc_chunk = B;
-    }
-    CK(alloc((void**)&c->kc_W, (size_t)B * 4 * NN * sizeof(double)));
-    CK(alloc((void**)&c->kc_vec, (size_t)B * 3 * N * sizeof(double)));   // t, x, y
-    CK(alloc((void**)&c->kc_int, ((size_t)B * (N + 4)) * sizeof(int)));  // oidx, m, nt, 2 lists
-    CK(alloc((void**)&c->obs, npts(c) * sizeof(double)));
-    CK(cudaMemcpyAsync(c->obs, obs_host, npts(c) * sizeof(double), cudaMemcpyHostToDevice,
-                       c->stream));
-    double* W0 = c->kc_W;
-    double* W1 = W0 + (size_t)B * NN;
-    double* W2 = W1 + (size_t)B * NN;
-    double* W3 = W2 + (size_t)B * NN;
-    double* tv = c->kc_vec;
-    double* xv = tv + (size_t)B * N;
-    double* yv = xv + (size_t)B * N;
-    int* oidx = c->kc_int;
-    int* mdev = oidx + (size_t)B * N;
-    int* ntdev = mdev + B;
-    int* lists = ntdev + B;  // 2 * B
-    const bool rebuild = has_vx_updated || !c->kc_valid;
-    const int e1d = (int)std::ceil(3. / 24 / dt);
-    KCArgs a{};
-    a.d = d;
-    a.dt = dt;
-    a.model_error = model_error;
-    a.obs_error = obs_error;
-    a.corr_time = corr_time;
-    a.use_log = use_log;
-    a.growing_q = growing_q;
-    a.Pg = c->f[VERB_F_P];
-    a.Rg = c->f[VERB_F_R];
-    a.VP = c->f[VERB_F_VP];
-    a.VR = c->f[VERB_F_VR];
-    a.S = c->f[VERB_F_SOURCES];
-    a.psd = c->f[VERB_F_PSD];
-    a.obs = c->obs;
-    a.status = c->status;
-    for (int s0 = 0; s0 < nsl; s0 += B) {
-        const int nb = std::min(B, nsl - s0);
-        a.s0 = s0;
-        double* Mc = c->kc_M + (size_t)s0 * NN;
-        double* Pa = c->kc_Pa + (size_t)s0 * NN;
-        if (rebuild) {
-            std::vector<int> nt(nb);
-            launch_kc_split(a, nb, ntdev, c->stream);
-            CK(cudaMemcpyAsync(nt.data(), ntdev, nb * sizeof(int), cudaMemcpyDeviceToHost,
-                               c->stream));
-            launch_kc_model(a, nb, ntdev, W0, NN, c->stream);
-            CK(cudaStreamSynchronize(c->stream));
-            c->acc.kernel_launches += 2;
-            CK(kc_pow(c, nb, W0, NN, nt, Mc, NN, W1, W2, W3, NN, lists));
-        }
-        // M1d = M^ceil(3/24/dt) into W1 (W0 and W2 as scratch; W3 the product)
-        {
-            std::vector<int> e(nb, e1d);
-            CK(kc_pow(c, nb, Mc, NN, e, W3, NN, W0, W2, W1, NN, lists));
-        }
-        // Q = M1d diag(t) M1d^T (+ diagonal terms) into W2
-        launch_kc_tdiag(a, nb, tv, N, c->stream);
-        {
-            BGemm g{};
-            g.A = W3; g.sA = NN; g.lda = N;
-            g.B = W3; g.sB = NN; g.ldb = N;
-            g.C = W2; g.sC = NN; g.ldc = N;
-            g.dk = tv; g.sdk = N;
-            g.M = N; g.N = N; g.K = N;
-            g.sgn = 1.0;
-            launch_bgemm(g, true, nb, c->stream);
-        }
-        launch_kc_qdiag(a, nb, W2, NN, c->stream);
-        launch_kc_pa_init(a, nb, c->kc_Pa, NN, c->stream);
-        // Pf = (M Pa) M^T + Q into W3 (W0 = M Pa)
-        {
-            BGemm g{};
-            g.A = Mc; g.sA = NN; g.lda = N;
-            g.B = Pa; g.sB = NN; g.ldb = N;
-            g.C = W0; g.sC = NN; g.ldc = N;
-            g.M = N; g.N = N; g.K = N;
-            g.sgn = 1.0;
-            launch_bgemm(g, false, nb, c->stream);
-            BGemm h{};
-            h.A = W0; h.sA = NN; h.lda = N;
-            h.B = Mc; h.sB = NN; h.ldb = N;
-            h.C = W3; h.sC = NN; h.ldc = N;
-            h.Cin = W2; h.sCin = NN; h.ldcin = N;
-            h.M = N; h.N = N; h.K = N;
-            h.sgn = 1.0;
-            launch_bgemm(h, true, nb, c->stream);
-        }
-        // observation space, gain, update
-        launch_kc_obs(a, nb, mdev, oidx, yv, xv, N, c->stream);
-        std::vector<int> m(nb);
-        CK(cudaMemcpyAsync(m.data(), mdev, nb * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-        CK(cudaStreamSynchronize(c->stream));
-        int mm = 0;
-        for (int v : m) mm = std::max(mm, v);
-        c->acc.kernel_launches += 8;
-        if (mm == 0) {
-            // no observation in the chunk: x unchanged, Pa = Pf
-            launch_kc_copy(W3, NN, Pa, NN, NN, nb, nullptr, c->stream);
-            continue;
-        }
-        launch_kc_gain(a, nb, W3, NN, W0, W1, NN, mdev, oidx, yv, xv, N, mm, c->stream);
-        launch_kc_update(a, nb, W0, NN, mdev, oidx, yv, xv, N, mm, W3, NN, W2, c->stream);
-        {
-            BGemm g{};
-            g.A = W0; g.sA = NN; g.lda = mm;
-            g.B = W2; g.sB = NN; g.ldb = N;
-            g.C = Pa; g.sC = NN; g.ldc = N;
-            g.Cin = W3; g.sCin = NN; g.ldcin = N;
-            g.M = N; g.N = N; g.K = mm;
-            g.sgn = -1.0;
-            launch_bgemm(g, false, nb, c->stream);
-        }
-        c->acc.kernel_launches += 4;
-    }
-    c->kc_valid = true;
-    CK(check_launch());
-    int st = VERB_OK;
-    CK(cudaMemcpyAsync(&st, c->status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    return st;
-}
-
 int conv_run(verb_ctx* c, double dt)
 {
     const Dims& d = c->d;
@@ -1038,7 +420,7 @@ int harvest_timing(verb_ctx* c)
     return VERB_OK;
 }
 
-}  // namespace
+}  // namespace vctx
 
 // ============================================================================ C ABI
 
@@ -1359,32 +741,6 @@ int verb_local(verb_ctx* c, double dt, double sub_dt)
     return local_run(c, dt, sub_dt);
 }
 
-int verb_assimilate_convection(verb_ctx* c, const double* obs_host, double dt, double model_error,
-                               double obs_error, int use_log, double correlation_time,
-                               int growing_q, int has_vx_updated, int slice_chunk)
-{
-    if (!c || !obs_host || !(dt > 0) || !(dt <= 0.125) || !(model_error > 0) ||
-        !(obs_error > 0) || !(correlation_time > 0) || slice_chunk < 0)
-        return VERB_ERR_ARG;
-    return kc_run(c, obs_host, dt, model_error, obs_error, use_log, correlation_time, growing_q,
-                  has_vx_updated, slice_chunk);
-}
-
-int verb_convection_da_state(verb_ctx* c, int v, int k, double* Pa_host, double* model_host)
-{
-    if (!c || v < 0 || v >= c->d.V || k < 0 || k >= c->d.K || !c->kc_Pa) return VERB_ERR_ARG;
-    const size_t NN = (size_t)c->d.P * c->d.R * c->d.P * c->d.R;
-    const size_t sl = (size_t)v * c->d.K + k;
-    if (Pa_host)
-        CK(cudaMemcpyAsync(Pa_host, c->kc_Pa + sl * NN, NN * sizeof(double), cudaMemcpyDeviceToHost,
-                           c->stream));
-    if (model_host)
-        CK(cudaMemcpyAsync(model_host, c->kc_M + sl * NN, NN * sizeof(double),
-                           cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    return VERB_OK;
-}
-
 int verb_local_solve_variants(int* count)
 {
     if (!count) return VERB_ERR_ARG;
@@ -1477,24 +833,6 @@ int verb_set_convection_arith(verb_ctx* c, int mode)
     graph_invalidate(c);
     c->conv_arith = mode;
     return VERB_OK;
-}
-
-int verb_local_krylov(verb_ctx* c, double dt, double sub_dt, int guess, verb_cnn* cnn,
-                      int smooth, double omega, int max_outer, int inner_maxit, double inner_tol,
-                      double resid_tol, verb_krylov_stats* stats)
-{
-    if (!c || !(dt > 0) || !(sub_dt > 0) || guess < VERB_GUESS_ZERO || guess > VERB_GUESS_CNN ||
-        (guess == VERB_GUESS_CNN) != (cnn != nullptr) || smooth < 0 || !(omega > 0) ||
-        !(omega < 2) || max_outer < 0 || inner_maxit < 1 || !(inner_tol > 0) || !(resid_tol > 0))
-        return VERB_ERR_ARG;
-    return krylov_run(c, dt, sub_dt, guess, cnn, smooth, omega, max_outer, inner_maxit, inner_tol,
-                      resid_tol, stats);
-}
-
-int verb_local_triples(verb_ctx* c, double dt, double sub_dt, float* feat_dev, float* target_dev)
-{
-    if (!c || !(dt > 0) || !(sub_dt > 0) || !feat_dev || !target_dev) return VERB_ERR_ARG;
-    return triples_run(c, dt, sub_dt, feat_dev, target_dev);
 }
 
 int verb_clamp_positive(verb_ctx* c)
