@@ -253,8 +253,10 @@ int verb_autotune_local_solve(verb_ctx* ctx, double dt, double sub_dt, double* t
 /* Convection arithmetic.  VERB_CONV_EXACT (the default) restates the
  * reference's operations one by one without contraction, so results are
  * bit-identical to it (exp() of loss rates aside).  VERB_CONV_FMA runs the
- * same kernel compiled with multiply-add contraction: about 10 % faster, and
- * within a few units in the last place of the exact form per step. */
+ * same kernel compiled with multiply-add contraction (and nine warps per
+ * block): about 18 % faster, and within a few units in the last place of the
+ * exact form per step.  Convection_2D (src/Convection_2D.cpp:36-169) has one
+ * arithmetic; the switch has no counterpart in the reference. */
 #define VERB_CONV_EXACT 0
 #define VERB_CONV_FMA 1
 int verb_set_convection_arith(verb_ctx* ctx, int mode);
@@ -339,7 +341,9 @@ int verb_step(verb_ctx* ctx, double dt, double sub_dt, int run_convection, int r
  * replayed while dt, sub_dt, the phase flags and every launch argument stay
  * the same; uploads of fields other than the PSD, scales, boundary types,
  * options and forms drop the graph, and the next such step captures it again.
- * Results are identical to eager steps.  Off by default. */
+ * Results are identical to eager steps.  Off by default.  No counterpart in
+ * the reference (its time loop, src/VERB4D_Solver.cpp:747-1282, runs on the
+ * host). */
 int verb_set_step_graph(verb_ctx* ctx, int enable);
 /* Number of PSD points < 0 (src/VERB4D_Solver.cpp:1226-1240). */
 int verb_negative_count(verb_ctx* ctx, long long* count);
