@@ -14,7 +14,9 @@ its own LU, so agreement is to rounding: 1e-10 for states and covariances,
 and takes Pa = Pf (the reference's dummy observation row makes the linear
 form's innovation matrix singular, so it exits, and gives log(0) in the log
 form, so it throws on the NaN state).  At
-24 x 25 x 31 x 31 (961 slices of 600 states) sampled slices are checked.
+24 x 25 x 31 x 31 (961 slices of 600 states) sampled slices are checked, and with
+40x velocities the per-slice split counts (9 to 1107 split steps) exercise the
+batched exponentiation with a different product set per slice.
 """
 import math
 
@@ -151,3 +153,38 @@ def test_cfg1_sampled_slices(gpu):
     print("24x25x31x31 convection assimilation (961 slices of 600 states): "
           "%.3f s with the model build, %.3f s with the cached model" % (t1 - t0, t3 - t2))
     c.close()
+
+
+def test_per_slice_split_counts(gpu):
+    # 40x the drift velocities: the Courant split count of the model matrix
+    # differs from slice to slice (tens to hundreds of split steps), so the
+    # batched binary exponentiation takes a different set of products per
+    # slice
+    wl = W.make_workload(W.GridSpec(8, 11, 4, 3), seed=63, sources=True)
+    wl.fields["VP"] = wl.fields["VP"] * 40.0
+    wl.fields["VR"] = wl.fields["VR"] * 40.0
+    P, R, V, K = wl.spec.shape
+    N = P * R
+    f = wl.fields
+    nts = set()
+    for v in range(V):
+        for k in range(K):
+            nts.add(KC.split_courant(1.0, wl.dt, f["VP"][:, :, v, k], f["VR"][:, :, v, k],
+                                     f["Pg"][1, 0, v, k] - f["Pg"][0, 0, v, k],
+                                     f["Rg"][0, 1, v, k] - f["Rg"][0, 0, v, k])[0])
+    assert len(nts) > 1
+    obs = make_obs(wl, 90, 0.15)
+    c = load_ctx(wl)
+    c.assimilate_convection(obs, wl.dt, ME, OE, has_vx_updated=True, slice_chunk=5)
+    got = c.download()
+    new = f["psd"].copy()
+    for v in range(V):
+        for k in range(K):
+            x, pa, m = oracle_slice(wl, f["psd"], np.zeros((N, N)), None, obs, v, k, True, False)
+            new[:, :, v, k] = x
+            gpa, gm = c.convection_da_state(v, k)
+            assert rel(gm, m) < 1e-12, (v, k)
+            assert rel(gpa, pa) < TOL, (v, k)
+    assert rel(got, new) < TOL
+    c.close()
+    print("split counts per slice:", sorted(nts))
