@@ -68,3 +68,33 @@ def test_ragged_mixed_within_tolerance(gpu):
     assert mem["mixed"] < mem["fp64"]
     d = np.abs(res["mixed"] - res["fp64"]).max() / np.abs(res["fp64"]).max()
     assert d < 1e-8
+
+
+def test_ragged_every_solve_shape_and_graph(gpu):
+    # every local-solve shape of the autotuner gives the same trimmed step,
+    # and steps replayed from the captured graph equal eager ones
+    wl, k0 = trimmed_workload()
+    outs = []
+    c = load_ctx(wl)
+    nshapes = len(c.solve_variants())
+    c.close()
+    for v in range(nshapes):
+        c = load_ctx(wl)
+        c.set_local_trim(k0)
+        c.set_local_solve_variant(v)
+        c.local(wl.dt, wl.sub_dt)
+        c.sync()
+        outs.append(c.download())
+        c.close()
+    for v in range(1, nshapes):
+        assert np.array_equal(outs[v], outs[0]), v
+    res = []
+    for graph in (False, True):
+        c = load_ctx(wl)
+        c.set_local_trim(k0)
+        c.set_step_graph(graph)
+        negs = [c.step(wl.dt, wl.sub_dt, 1, 1, 1, count_negatives=True) for _ in range(4)]
+        c.sync()
+        res.append((c.download(), negs))
+        c.close()
+    assert np.array_equal(res[0][0], res[1][0]) and res[0][1] == res[1][1]
