@@ -272,7 +272,8 @@ int verb_set_convection_arith(verb_ctx* ctx, int mode);
  * A d = r to inner_tol in FP32 (at most inner_maxit iterations) and adds d.
  * A system is done when max|b - A x| / max|b| <= resid_tol; systems still
  * above it after max_outer passes, or whose residual a pass did not reduce
- * at least tenfold, are solved by the banded LU (factorised
+ * at least tenfold, are solved by the banded LU (in the mixed form: FP32
+ * factors and the form's FP64 refinement steps) (factorised
  * for those systems only; the factors are allocated on first use) so the
  * step is always accurate to the residual tolerance or exact.  The features
  * are [sys][4][K][V] FP32: (log10 D_VV - m)/2, (log10 D_KK - m)/2 with

@@ -148,3 +148,18 @@ def test_learned_warm_start(gpu):
         print(guess, "iterations per Krylov-solved system %.1f" % (st["solved_iterations"] / ns),
               "fallbacks", st["fallbacks"], "guess residual %.3g" % st["guess_rel_residual"])
     net.close()
+
+
+def test_krylov_mixed_fallback_refined(gpu):
+    # with FP32 factors the LU fallback takes the mixed form's FP64 refinement
+    wl = W.make_workload(W.CONFIGS["cfg1"], seed=24, sources=True, losses=True)
+    ref = lu_step(wl)
+    for max_outer in (0, 10):
+        c = split_ctx(wl)
+        c.set_local_precision("mixed", 10)
+        st = c.local_krylov(wl.dt, wl.sub_dt, guess="prev", max_outer=max_outer)
+        c.sync()
+        got = c.download()
+        c.close()
+        assert st["fallbacks"] > 0
+        assert rel(got, ref) < TOL, max_outer

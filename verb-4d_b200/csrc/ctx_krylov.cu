@@ -171,8 +171,18 @@ int krylov_run(verb_ctx* c, double dt, double sub_dt, int guess, verb_cnn* cnn, 
                 CK(cudaMemsetAsync(c->Uf, 0, nuf * c->kvp * sizeof(double), c->stream));
             launch_local_factor(ap, c->stream);
             launch_local_solve(ap, c->stream);
+            c->acc.kernel_launches += 2;
+            // the mixed form's FP64 refinement (FP32 factors), as in the LU step
+            for (int it = 0; it < c->refine_iters; it++) {
+                launch_local_residual(ap, c->kb, c->lwork, c->lres, c->stream);
+                LocalArgs ar = ap;
+                ar.work = c->lres;
+                launch_local_solve(ar, c->stream);
+                launch_local_update(ap, c->lwork, c->lres, c->refine_red, c->stream);
+                c->acc.kernel_launches += 3;
+            }
             launch_masked_copy(ap, c->kx, c->lwork, c->stream);
-            c->acc.kernel_launches += 3;
+            c->acc.kernel_launches++;
             c->local_dirty = true;  // the factors of the other systems are stale
             st.fallbacks += nfall;
         }
