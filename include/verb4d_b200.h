@@ -297,7 +297,7 @@ typedef struct {
 int verb_local_krylov(verb_ctx* ctx, double dt, double sub_dt, int guess, verb_cnn* cnn,
                       int smooth, double omega, int max_outer, int inner_maxit, double inner_tol,
                       double resid_tol, verb_krylov_stats* stats);
-/* One local step by the LU (as verb_local, without refinement) that also
+/* One local step by the LU (as verb_local, with its refinement steps) that also
  * writes, for the last sub-step, the CNN features of every system
  * (feat_dev, [P*R][4][K][V] floats) and the training target
  * (target_dev, [P*R][K][V] floats, (x - f) / max|f|).  Untrimmed systems only;

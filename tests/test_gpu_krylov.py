@@ -163,3 +163,28 @@ def test_krylov_mixed_fallback_refined(gpu):
         c.close()
         assert st["fallbacks"] > 0
         assert rel(got, ref) < TOL, max_outer
+
+
+def test_triples_step_is_the_lu_step(gpu):
+    # the state after verb_local_triples is the LU step's, in the FP64 form
+    # and in the mixed form with refinement
+    import torch
+
+    wl = W.make_workload(W.CONFIGS["cfg1"], seed=25, sources=True, losses=True)
+    P, R, V, K = wl.spec.shape
+    for form in (("fp64", 0), ("mixed", 10)):
+        c = split_ctx(wl)
+        c.set_local_precision(*form)
+        c.local(wl.dt, wl.sub_dt)
+        c.sync()
+        want = c.download()
+        c.close()
+        c = split_ctx(wl)
+        c.set_local_precision(*form)
+        feat = torch.zeros((P * R, 4, K, V), dtype=torch.float32, device="cuda")
+        targ = torch.zeros((P * R, 1, K, V), dtype=torch.float32, device="cuda")
+        c.local_triples(wl.dt, wl.sub_dt, feat.data_ptr(), targ.data_ptr())
+        c.sync()
+        got = c.download()
+        c.close()
+        assert np.array_equal(got, want), form

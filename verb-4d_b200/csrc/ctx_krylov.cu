@@ -231,7 +231,20 @@ int triples_run(verb_ctx* c, double dt, double sub_dt, float* feat, float* targe
             launch_local_features(a, c->kb, feat, c->kscale, c->stream);
         }
         launch_local_rhs(a, k > 0, c->stream);
+        if (c->refine_iters > 0)
+            CK(cudaMemcpyAsync(c->lrhs, c->lwork, nu * sizeof(double), cudaMemcpyDeviceToDevice,
+                               c->stream));
         launch_local_solve(a, c->stream);
+        // the solution the LU step itself would take: with refinement
+        // configured, its FP64 refinement steps too
+        for (int it = 0; it < c->refine_iters; it++) {
+            launch_local_residual(a, c->lrhs, c->lwork, c->lres, c->stream);
+            LocalArgs ar = a;
+            ar.work = c->lres;
+            launch_local_solve(ar, c->stream);
+            launch_local_update(a, c->lwork, c->lres, c->refine_red, c->stream);
+            c->acc.kernel_launches += 3;
+        }
         if (last) launch_local_targets(a, c->kb, c->lwork, c->kscale, target, c->stream);
         c->acc.kernel_launches += last ? 5 : 2;
     }
