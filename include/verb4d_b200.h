@@ -51,7 +51,8 @@ typedef enum {
     VERB_ERR_CFL = 3,     /* Courant number > 1 (src/Convection_1D_ULTIMATE_QUICKEST6.cpp:48-52) */
     VERB_ERR_BC = 4,      /* unsupported boundary-condition type for this operator */
     VERB_ERR_TENSOR = 5,  /* min(DVV*DKK - DVK^2) < 0 (src/VERB4D_Solver.cpp:747-753) */
-    VERB_ERR_NAN = 6,     /* NaN after the Kalman update (src/DataAssimilation.cpp:62-67) */
+    VERB_ERR_NAN = 6,     /* NaN after the Kalman update (src/DataAssimilation.cpp:62-67),
+                             or a NaN in the PSD after a step (no counterpart) */
     VERB_ERR_CUDA = 7,    /* CUDA runtime error */
     VERB_ERR_NOMEM = 8,   /* device allocation failed / would not fit */
     VERB_ERR_GRID = 9,    /* convection line shorter than 11 points (QUICKEST6.cpp:56-59) */
@@ -350,6 +351,13 @@ int verb_set_step_graph(verb_ctx* ctx, int enable);
 int verb_negative_count(verb_ctx* ctx, long long* count);
 /* min(DVV*DKK - DVK*DVK) over the grid (src/VERB4D_Solver.cpp:747-753). */
 int verb_tensor_check(verb_ctx* ctx, double* min_value);
+/* max |field| of n <= 8 fields (verb_field codes) in one pass over the grid:
+ * the per-step log of src/VERB4D_Solver.cpp:636-675 (VP, VR, DLL, DVV, DVK,
+ * DKK after their update; DLL with its scale factor applied), with
+ * Matrix4D::maxabs's semantics (src/Matrix.cpp:5908-5915: NaN values are
+ * skipped, -inf for an empty grid).  Every listed field must have been
+ * uploaded. */
+int verb_field_maxabs(verb_ctx* ctx, int n, const int* fields, double* out);
 /* Wait for the context stream; returns the first device-side error. */
 int verb_sync(verb_ctx* ctx);
 int verb_set_timing(verb_ctx* ctx, int enable);
@@ -410,13 +418,19 @@ int verb_convection_2d(double* psd, const double* P, const double* R, int nP, in
  * caller's DEVICE memory, for callers that cannot allocate device memory (a
  * host application or plugin that owns every allocation, or a path where an
  * allocation is not allowed).  It calls no allocator: the kernel's scratch is
- * a fixed array of VERB_NOALLOC_MAX_POINTS doubles (plus a few status words)
- * that the library reserves on every device that loads it, until exit.
+ * a fixed array in the library's device code of 5 doubles per point of
+ * VERB_NOALLOC_MAX_POINTS points (320 KiB) plus a few status words, held on
+ * every device that loads that code until exit.  CUDA loads device code
+ * lazily, so the first call on a device loads it (the array and the kernel
+ * take their device memory then, and the device may synchronise) and looks
+ * up the array's address: make that first call outside any region where
+ * allocation is not allowed, and before any stream capture.
  * nP*nR > VERB_NOALLOC_MAX_POINTS returns VERB_ERR_SIZE.  All calls share that
- * array, so calls that overlap on the GPU race: serialise them.  The first
- * call on a device looks up the array's address; make it before any stream
- * capture.  `stream` is a cudaStream_t (NULL = default stream); the call
- * returns after the slice is done, with the device-side status. */
+ * array, so calls that overlap on the GPU race: serialise them.  `stream` is
+ * a cudaStream_t (NULL = default stream); the call returns after the slice is
+ * done, with the device-side status (e.g. VERB_ERR_CFL, the slice then left
+ * unchanged) or VERB_ERR_CUDA for a failure of its own launch; an error left
+ * pending by the caller's earlier CUDA work is not reported or cleared. */
 #define VERB_NOALLOC_MAX_POINTS 8192
 int verb_convection_2d_noalloc(double* psd, const double* P, const double* R, int nP, int nR,
                                const double* pl, const double* pu, const double* rl,

@@ -32,7 +32,10 @@ _ip = C.POINTER(C.c_int)
 
 def build(with_ref: bool | None = None) -> None:
     """Compile the restatement, and the reference libraries when the reference tree exists."""
-    ref_dir = os.environ.get("VERB_REFERENCE", "/root/reference")
+    # the reference tree: $VERB_REFERENCE, else a checkout named `reference`
+    # beside this repository
+    ref_dir = os.environ.get("VERB_REFERENCE",
+                             os.path.abspath(os.path.join(HERE, "..", "..", "reference")))
     if with_ref is None:
         with_ref = os.path.isdir(os.path.join(ref_dir, "src"))
     target = "ref" if with_ref else "all"

@@ -34,15 +34,16 @@ def slice_case(spec, seed, iV, iK, vp_scale):
                 S=sl(f["S"]), loss=np.zeros_like(sl(f["psd"])), G=sl(f["G_conv"]), dt=wl.dt)
 
 
-def run_noalloc(lib, c, torch):
+def run_noalloc(lib, c, torch, stream=None):
     dev = torch.device("cuda", 0)
-    t = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev)
-         for k, v in c.items() if k != "dt"}
+    t = {k: torch.from_numpy(np.array(v)).to(dev) for k, v in c.items() if k != "dt"}
+    torch.cuda.synchronize()
     nP, nR = c["psd"].shape
     p = lambda k: C.c_void_p(t[k].data_ptr())  # noqa: E731
+    handle = C.c_void_p(stream.cuda_stream) if stream is not None else None
     st = lib.verb_convection_2d_noalloc(p("psd"), p("P"), p("R"), nP, nR, p("pl"), p("pu"), p("rl"),
                                         p("ru"), 0, 0, 1, 1, p("VP"), p("VR"), p("S"), p("loss"),
-                                        p("G"), c["dt"], None)
+                                        p("G"), c["dt"], handle)
     torch.cuda.synchronize()
     return st, t["psd"].cpu().numpy()
 
@@ -74,3 +75,29 @@ def test_noalloc_rejects_oversized_slices(gpu):
     st, got = run_noalloc(lib, c, torch)
     assert st == 11  # VERB_ERR_SIZE
     assert np.array_equal(got, c["psd"])  # nothing was touched
+
+
+def test_noalloc_on_a_caller_stream(gpu):
+    """The caller's own (non-default) stream: the same result bit for bit."""
+    import torch
+
+    lib = L.load()
+    c = slice_case(W.CONFIGS["cfg1"], 11, 20, 12, 1.0)
+    stream = torch.cuda.Stream()
+    st, got = run_noalloc(lib, c, torch, stream)
+    assert st == L.VERB_OK
+    assert np.array_equal(got, run_allocating(c))
+
+
+def test_noalloc_reports_a_courant_failure(gpu):
+    """A duplicated MLT coordinate makes the grid spacing zero, so the
+    sub-step count is infinite: the slice is skipped and VERB_ERR_CFL is
+    returned (the reference exits, QUICKEST6.cpp:48-52)."""
+    import torch
+
+    lib = L.load()
+    c = slice_case(W.CONFIGS["cfg1"], 12, 20, 12, 1.0)
+    c["P"][1, :] = c["P"][0, :]
+    st, got = run_noalloc(lib, c, torch)
+    assert st == 3  # VERB_ERR_CFL
+    assert np.array_equal(got, c["psd"])

@@ -437,7 +437,7 @@ const char* verb_status_string(int s)
         case VERB_ERR_CFL: return "Courant number > 1";
         case VERB_ERR_BC: return "unsupported boundary condition type";
         case VERB_ERR_TENSOR: return "DVV*DKK - DVK^2 < 0";
-        case VERB_ERR_NAN: return "NaN after the Kalman update";
+        case VERB_ERR_NAN: return "NaN in the PSD (after a step or the Kalman update)";
         case VERB_ERR_CUDA: return "CUDA error";
         case VERB_ERR_NOMEM: return "out of device memory";
         case VERB_ERR_GRID: return "convection grid shorter than 11 points";
@@ -501,7 +501,8 @@ int verb_destroy(verb_ctx* c)
     }
     for (int i = 0; i < VERB_BCF_COUNT; i++) cudaFree(c->bc[i]);
     for (void* p : {(void*)c->Lf32, (void*)c->Uf32, (void*)c->lrhs, (void*)c->lres,
-                    (void*)c->refine_red, (void*)c->trim_k0, (void*)c->trim_uoff})
+                    (void*)c->refine_red, (void*)c->trim_k0, (void*)c->trim_uoff,
+                    (void*)c->maxabs_red})
         cudaFree(p);
     free_krylov(c);
     free_kc(c);
@@ -848,7 +849,7 @@ int verb_negative_count(verb_ctx* c, long long* count)
     if (!c || !c->f[VERB_F_PSD]) return VERB_ERR_ARG;
     {
         PhaseTimer t(c, PH_RED);
-        launch_negative_count(c->f[VERB_F_PSD], npts(c), c->red, c->stream);
+        launch_negative_count(c->f[VERB_F_PSD], npts(c), c->red, c->status, c->stream);
         c->acc.kernel_launches++;
     }
     if (count) {
@@ -864,6 +865,29 @@ int verb_tensor_check(verb_ctx* c, double* min_value)
 {
     if (!c) return VERB_ERR_ARG;
     return tensor_check(c, min_value);
+}
+
+int verb_field_maxabs(verb_ctx* c, int n, const int* fields, double* out)
+{
+    if (!c || n < 1 || n > MAXABS_FIELDS || !fields || !out) return VERB_ERR_ARG;
+    MaxabsArgs a{};
+    for (int i = 0; i < n; i++) {
+        if (fields[i] < 0 || fields[i] >= VERB_F_COUNT || !c->f[fields[i]]) return VERB_ERR_ARG;
+        a.x[i] = c->f[fields[i]];
+    }
+    a.nf = n;
+    CK(alloc((void**)&c->maxabs_red, MAXABS_FIELDS * sizeof(unsigned long long)));
+    a.out = c->maxabs_red;
+    {
+        PhaseTimer t(c, PH_RED);
+        launch_maxabs(a, npts(c), c->stream);
+        c->acc.kernel_launches++;
+    }
+    unsigned long long k[MAXABS_FIELDS];
+    CK(cudaMemcpyAsync(k, c->maxabs_red, sizeof(k), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < n; i++) out[i] = dkey_inv(k[i]);
+    return check_launch();
 }
 
 // The launches of one step after its host-side checks: phases, clamps and

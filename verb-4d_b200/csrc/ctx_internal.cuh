@@ -112,6 +112,7 @@ struct verb_ctx {
     int conv_arith = VERB_CONV_EXACT;
     // reductions / status
     unsigned long long* red = nullptr;  // [0] negatives, [1] tensor min key
+    unsigned long long* maxabs_red = nullptr;  // [MAXABS_FIELDS] max |field| keys
     int* status = nullptr;
     bool tensor_dirty = true;
     double tensor_min = 0;

@@ -178,6 +178,10 @@ int krylov_run(verb_ctx* c, double dt, double sub_dt, int guess, verb_cnn* cnn, 
                 LocalArgs ar = ap;
                 ar.work = c->lres;
                 launch_local_solve(ar, c->stream);
+                // the statistic reports the last correction of this call
+                if (it == c->refine_iters - 1)
+                    CK(cudaMemsetAsync(c->refine_red, 0, 2 * sizeof(unsigned long long),
+                                       c->stream));
                 launch_local_update(ap, c->lwork, c->lres, c->refine_red, c->stream);
                 c->acc.kernel_launches += 3;
             }
@@ -242,6 +246,8 @@ int triples_run(verb_ctx* c, double dt, double sub_dt, float* feat, float* targe
             LocalArgs ar = a;
             ar.work = c->lres;
             launch_local_solve(ar, c->stream);
+            if (last && it == c->refine_iters - 1)
+                CK(cudaMemsetAsync(c->refine_red, 0, 2 * sizeof(unsigned long long), c->stream));
             launch_local_update(a, c->lwork, c->lres, c->refine_red, c->stream);
             c->acc.kernel_launches += 3;
         }

@@ -210,6 +210,11 @@ __global__ void __launch_bounds__(KF_THREADS) kf_kernel(KFArgs a)
         for (int i = threadIdx.x; i < n; i += blockDim.x) Pf[(size_t)i * n + i] += a.model_error;
         __syncthreads();
         if (m == 0) {
+            // no observation: x += 0 (the reference's dummy row), and the
+            // NaN check still applies (src/DataAssimilation.cpp:62-67)
+            bool bad = false;
+            for (int i = threadIdx.x; i < n; i += blockDim.x) bad = bad || isnan(x[i]);
+            if (__syncthreads_or(bad) && threadIdx.x == 0) set_error(a.status, VERB_ERR_NAN);
             for (size_t e = threadIdx.x; e < RR; e += blockDim.x) Pa[e] = Pf[e];
             __syncthreads();
             continue;

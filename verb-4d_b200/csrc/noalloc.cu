@@ -8,8 +8,12 @@
 // entry point runs the same convection kernel as verb_convection_2d, with the
 // kernel's scratch (the slice's face Courant tables and its G, exp(Loss*dt)
 // and Sources*dt planes, the work ticket, the sub-step count and the status
-// word) placed in a fixed array that the library reserves in device memory
-// when it is loaded.
+// word) placed in a fixed array of device memory that belongs to the
+// library's device code.  CUDA loads that code on a device lazily (the default
+// since CUDA 12.2): the first call on a device loads it, which is when the
+// array and the kernel take their device memory and the device may
+// synchronise.  A caller that must not allocate makes one warm-up call on each
+// device before it enters the region where allocation is not allowed.
 //
 // Limits and sharing:
 //  * P_size * R_size must not exceed VERB_NOALLOC_MAX_POINTS (8192 points,
@@ -23,6 +27,10 @@
 //  * The first call on a device looks up the array's device address (once per
 //    device, with that device current).  Make that first call before any
 //    stream capture begins.
+//  * Errors: the call reports the device-side status of its slice
+//    (VERB_ERR_CFL, ...) and an error of its own launch.  An error that the
+//    caller's earlier CUDA work left pending in the runtime is neither
+//    reported nor cleared here.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -107,8 +115,15 @@ extern "C" int verb_convection_2d_noalloc(double* psd, const double* P, const do
     a.ticket = words;
     a.substeps = words + 1;
     a.status = words + 2;
+    // an error the caller's earlier work left pending stays pending: only a
+    // change of the runtime's last error after the launch is this call's own
+    const cudaError_t before = cudaPeekAtLastError();
     verb::launch_convection(a, 1, st);
-    if (cudaGetLastError() != cudaSuccess) return VERB_ERR_CUDA;
+    const cudaError_t after = cudaPeekAtLastError();
+    if (after != cudaSuccess && after != before) {
+        cudaGetLastError();
+        return VERB_ERR_CUDA;
+    }
     int dev_status = 0;
     if (cudaMemcpyAsync(&dev_status, words + 2, sizeof(int), cudaMemcpyDeviceToHost, st) !=
             cudaSuccess ||

@@ -200,7 +200,15 @@ void launch_masked_copy(const LocalArgs& a, double* x, const double* y, cudaStre
 // unknowns of all systems (V*K*P*R, or the sum over trimmed systems)
 
 // --- reductions / elementwise ---------------------------------------------------
-void launch_negative_count(const double* psd, size_t n, unsigned long long* out, cudaStream_t s);
+void launch_negative_count(const double* psd, size_t n, unsigned long long* out, int* status,
+                           cudaStream_t s);
+constexpr int MAXABS_FIELDS = 8;
+struct MaxabsArgs {
+    const double* x[MAXABS_FIELDS];
+    int nf;
+    unsigned long long* out;  // [MAXABS_FIELDS] dkey of max |x| per field
+};
+void launch_maxabs(const MaxabsArgs& a, size_t n, cudaStream_t s);
 void launch_tensor_min(const double* dvv, const double* dkk, const double* dvk, size_t n,
                        unsigned long long* out_ordered, cudaStream_t s);
 void launch_clamp_positive(double* psd, size_t n, cudaStream_t s);

@@ -126,6 +126,7 @@ SIGNATURES = {
     "verb_step": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, _llp]),
     "verb_negative_count": (C.c_int, [_vp, _llp]),
     "verb_tensor_check": (C.c_int, [_vp, _dp]),
+    "verb_field_maxabs": (C.c_int, [_vp, C.c_int, _ip, _dp]),
     "verb_sync": (C.c_int, [_vp]),
     "verb_set_timing": (C.c_int, [_vp, C.c_int]),
     "verb_get_timing": (C.c_int, [_vp, C.POINTER(Timing)]),

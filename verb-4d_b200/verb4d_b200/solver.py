@@ -248,6 +248,19 @@ class Context:
         L.check(self.lib.verb_tensor_check(self.h, C.byref(v)), "tensor check")
         return v.value
 
+    def maxabs(self, names) -> dict:
+        """max |field| of each named field in one pass (the reference's per-step
+        log of VP, VR, DLL, DVV, DVK, DKK; NaN values skipped)."""
+        ids = (C.c_int * len(names))(*[L.FIELD_IDS[n] for n in names])
+        out = np.zeros(len(names))
+        L.check(self.lib.verb_field_maxabs(self.h, len(names), ids, out.ctypes.data_as(L._dp)),
+                "maxabs")
+        return dict(zip(names, out.tolist()))
+
+    def status(self) -> int:
+        """The device-side status word after waiting for the stream (0: OK)."""
+        return int(self.lib.verb_sync(self.h))
+
     def sync(self) -> None:
         L.check(self.lib.verb_sync(self.h), "device status")
 
