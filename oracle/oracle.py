@@ -22,6 +22,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libverbref.so")
 REF_LU_SO = os.path.join(HERE, "_ref", "libverbref_lu.so")
+# the C++ drop-in layer (reference signatures over the CUDA library) with the
+# same harness entry points under a drop_ prefix
+DROPIN_SO = os.path.join(HERE, "_ref", "libverbdropin.so")
 
 BC_PERIODIC, BC_VALUE, BC_DERIV = 0, 1, 2
 
@@ -50,11 +53,26 @@ def _f64(a):
     return np.ascontiguousarray(a, dtype=np.float64)
 
 
+class _Renamed:
+    """A loaded library whose entry points named prefix_<x> answer to ref_<x>."""
+
+    def __init__(self, lib, prefix: str):
+        self._lib = lib
+        self._prefix = prefix
+
+    def __getattr__(self, name: str):
+        if name.startswith("ref_"):
+            name = self._prefix + name[4:]
+        return getattr(self._lib, name)
+
+
 class _Lib:
-    def __init__(self, path: str):
+    def __init__(self, path: str, prefix: str | None = None):
         if not os.path.exists(path):
             raise FileNotFoundError(path)
         self.lib = C.CDLL(path)
+        if prefix:
+            self.lib = _Renamed(self.lib, prefix)
         self.path = path
 
     def has(self, name: str) -> bool:
@@ -299,6 +317,15 @@ def reference(lu_caching: bool = False) -> _Lib:
     if path not in _cache:
         _cache[path] = _Lib(path)
     return _cache[path]
+
+
+def dropin() -> _Lib:
+    """The C++ drop-in layer built against the reference's headers
+    (oracle/_ref/libverbdropin.so): the same per-slice entry points as
+    reference(), running on the GPU through libverb4d_b200.so."""
+    if DROPIN_SO not in _cache:
+        _cache[DROPIN_SO] = _Lib(DROPIN_SO, prefix="drop_")
+    return _cache[DROPIN_SO]
 
 
 def have_reference() -> bool:

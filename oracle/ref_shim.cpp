@@ -26,6 +26,7 @@
 #include "Matrix.h"
 #include "MatrixSolver.h"
 #include "MonotCubicInterpolator.hpp"
+#include "UpdatableMatrix.h"
 
 namespace {
 
@@ -324,6 +325,36 @@ int ref_radial_lines(orc_state* s, double dt, const int* pvk, int nlist, int nth
         const size_t b = ((size_t)iP * V + iV) * K + iK;
         Diffusion_1D(f, lg, R, s->Ll[b], s->Lu[b], bct(s->Ll_t), bct(s->Lu_t), dl, gr, sr, ls, dt);
         for (int iR = 0; iR < R; iR++) s->psd[(((size_t)iP * R + iR) * V + iV) * K + iK] = f[iR];
+    }
+    return 0;
+}
+
+// src/UpdatableMatrix.cpp:857-961 with :308-600 and :602-846: an
+// UpdatableListMatrix<Matrix4D<double>> read from the .tab file `tab` (one
+// component per line: a .pltb data file or a .lst list of (time, .pltb file),
+// then optionally a scale (a number or a .lst list of (time, value)) and
+// from/to limits per axis), merged by SUM (mean = 0) or MEAN, and updated at
+// times[0..nt).  out receives the field after every update ([nt][P][R][V][K])
+// and updated[t] the update's return value.  q1..q4 are the four grids.
+int ref_updatable_list(const char* tab, int mean, int P, int R, int V, int K, const double* q1,
+                       const double* q2, const double* q3, const double* q4, const double* times,
+                       int nt, double* out, int* updated)
+{
+    const size_t n = (size_t)P * R * V * K;
+    auto grid = [&](const double* q) {
+        Matrix4D<double> m((size_t)P, (size_t)R, (size_t)V, (size_t)K);
+        std::memcpy(&m[0][0][0][0], q, sizeof(double) * n);
+        return m;
+    };
+    const Matrix4D<double> Q1 = grid(q1), Q2 = grid(q2), Q3 = grid(q3), Q4 = grid(q4);
+    using L = UpdatableListMatrix<Matrix4D<double>>;
+    L field(mean ? L::MERGE_TYPE::MEAN : L::MERGE_TYPE::SUM);
+    field.AllocateMemory((size_t)P, (size_t)R, (size_t)V, (size_t)K);
+    field = 0.0;
+    if (!field.readFromIniFile(tab, Q1, Q2, Q3, Q4)) return 1;
+    for (int t = 0; t < nt; t++) {
+        updated[t] = field.update(times[t], Q1, Q2, Q3, Q4) ? 1 : 0;
+        std::memcpy(out + (size_t)t * n, &field[0][0][0][0], sizeof(double) * n);
     }
     return 0;
 }
