@@ -169,12 +169,13 @@ def run_ours(args):
                for h, (vp, vr) in vel_host.items()}
     torch.cuda.synchronize(dev)
 
-    def make_solver(form):
+    def make_solver(form, conv=None, trim=None, refine=None):
         sv = Solver(wl, stream=stream.cuda_stream, velocity_provider=None)
         sv.load()
-        sv.ctx.set_local_precision(form, args.refine if form == "mixed" else 0)
-        sv.ctx.set_convection_arith(args.conv)
-        if args.trim:
+        ref = (args.refine if form == "mixed" else 0) if refine is None else refine
+        sv.ctx.set_local_precision(form, ref)
+        sv.ctx.set_convection_arith(conv or args.conv)
+        if args.trim if trim is None else trim:
             sv.ctx.set_local_trim(W.loss_cone_k0(wl))
         return sv
 
@@ -209,10 +210,11 @@ def run_ours(args):
         # untimed: pick the local-solve shape for this grid on its own systems
         ch, tms = ctx.autotune_local_solve(wl.dt, wl.sub_dt)
         shapes = ctx.solve_variants()
-        tune = {"local_solve_shapes_ms": {f"{w}x{f}x{b}": round(float(t), 3)
-                                          for (w, f, b), t in zip(shapes, tms)},
-                "chosen": "%dx%dx%d (systems per CTA x L columns x U columns in flight)"
-                          % shapes[ch]}
+        key = lambda sh: "%dx%dx%d%s" % (sh[0], sh[1], sh[2], "r" if sh[3] else "")  # noqa: E731
+        tune = {"local_solve_shapes_ms": {key(sh): round(float(t), 3)
+                                          for sh, t in zip(shapes, tms)},
+                "chosen": key(shapes[ch]) + " (systems per CTA x L columns x U columns in "
+                                            "flight; r: right-hand-side window in registers)"}
     ctx.set_timing(False)
     ctx.set_timing(True)  # zeroes the counters
     if args.graph:
@@ -310,6 +312,15 @@ def run_ours(args):
     ms = max_over_ranks(ms, dev)
     sim_h = args.steps * wl.dt * 24.0
     value = replica_throughput(sim_h, ms / 1e3, world)
+
+    # ---------------- the forms side by side (same box, same inputs): the
+    # plain FP64 form (the reference's arithmetic), the benchmarked form and
+    # the mixed-precision forms; per form the time per step over
+    # --form-steps graph-replayed steps and the one-step error against the
+    # plain form from the same initial state
+    forms = None
+    if not args.no_forms:
+        forms = measure_forms(args, wl, make_solver, update_dev, stream, dev)
 
     # ---------------- end to end through the public API with host buffers (e2e)
     e2e = None
@@ -409,16 +420,13 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.form == "fp64" else "f64 (local LU factors stored f32)",
         "data": "synthetic (seeded)",
-        "config": {"workload": f"VERB-4D operator-split step {args.config} "
-                               f"(P,R,V,K)={spec.shape}, dt=5 min, hourly Kp in [1,6]",
-                   "P_mlt": P, "R_L": R, "V_energy": V, "K_alpha": K, "dt_min": 5,
-                   "parallelism": f"replicas{world}",
-                   "local_systems": "loss-cone trimmed (ragged)" if args.trim else "full",
-                   "step_launch": "CUDA graph replay" if args.graph else "eager launches",
-                   "convection_arith": ("fma: multiply-add contraction, within 1e-12 of the "
-                                        "reference per step" if args.conv == "fma" else
-                                        "exact: bit-identical to the reference"),
-                   "l2": "inputs larger than L2 (110 GB of LU factors streamed per step)"},
+        "config": workload_config(args, spec, world),
+        "impl": {"local_systems": "loss-cone trimmed (ragged)" if args.trim else "full",
+                 "local_precision": args.form,
+                 "step_launch": "CUDA graph replay" if args.graph else "eager launches",
+                 "convection_arith": ("fma: multiply-add contraction, within 1e-12 of the "
+                                      "reference per step" if args.conv == "fma" else
+                                      "exact: bit-identical to the reference")},
         "phases_ms_per_step": {"convection": round(conv_ms, 3),
                                "radial": round(tph["radial_ms"] / nph, 3),
                                "local_solve": round(tph["local_solve_ms"] / nph, 3),
@@ -458,6 +466,8 @@ def run_ours(args):
         out["e2e"] = e2e
     if form_info:
         out["form"] = form_info
+    if forms:
+        out["forms"] = forms
     if world == 1 and rank == 0 and not args.no_cpu_baseline:
         cb = reference_estimate(wl, budget_s=args.cpu_budget)
         out["cpu_baseline"] = {"value": round(cb["value"], 8), "unit": "sim-hours/s",
@@ -467,6 +477,84 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def timed_hours(args, dt):
+    """Simulated hours (of the Kp series) that the timed steps
+    warmup+1 .. warmup+steps fall in."""
+    return sorted({int(np.floor(it * dt * 24 + 1e-9))
+                   for it in range(args.warmup + 1, args.warmup + args.steps + 1)})
+
+
+def workload_config(args, spec, world):
+    """The workload both arms run (identical in their JSON lines)."""
+    from verb4d_b200 import workload as W
+
+    return {"workload": f"VERB-4D operator-split step {args.config} (P,R,V,K)={spec.shape}, "
+                        f"dt=5 min, hourly Kp in [1,6] (seed {args.seed})",
+            "P_mlt": spec.P, "R_L": spec.R, "V_energy": spec.V, "K_alpha": spec.K, "dt_min": 5,
+            "kp_hours_timed": timed_hours(args, W.DT_5MIN),
+            "parallelism": f"replicas{world}",
+            "l2": "inputs larger than L2 (110 GB of LU factors streamed per step)"}
+
+
+# --------------------------------------------------------------------------- forms
+FORMS = {
+    # name: (local precision, FP64 refinement steps, convection arithmetic, ragged systems)
+    "plain_fp64": ("fp64", 0, "exact", False),
+    "fp64_fma": ("fp64", 0, "fma", False),
+    "mixed_fma": ("mixed", 2, "fma", False),
+    "mixed_fma_trim": ("mixed", 2, "fma", True),
+}
+
+
+def measure_forms(args, wl, make_solver, update_dev, stream, dev):
+    """Time every form of FORMS for args.form_steps steps after 3 warm-up
+    steps (the first of which factorises and gives the one-step PSD), one
+    context at a time (each FP64 context holds 110 GB of factors)."""
+    import torch
+
+    fl = wl.flags
+    out = {}
+    psd_plain = None
+    for name, (prec, refine, conv, trim) in FORMS.items():
+        sv = make_solver(prec, conv=conv, trim=trim, refine=refine)
+        sv.hour = -1
+        psd1 = None
+        for it in range(1, 4):
+            update_dev(it, sv)
+            sv.ctx.step(wl.dt, wl.sub_dt, fl["run_convection"], fl["run_radial"], fl["run_local"])
+            if it == 1:
+                psd1 = sv.ctx.download()
+        sv.ctx.sync()
+        sv.ctx.set_step_graph(True)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for it in range(4, 4 + args.form_steps):
+            update_dev(it, sv)
+            sv.ctx.step(wl.dt, wl.sub_dt, fl["run_convection"], fl["run_radial"], fl["run_local"])
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        sv.ctx.sync()
+        msf = e0.elapsed_time(e1) / args.form_steps
+        sv.ctx.close()
+        del sv
+        if psd_plain is None:
+            psd_plain = psd1
+        err = float(np.abs(psd1 - psd_plain).max() / np.abs(psd_plain).max())
+        out[name] = {"ms_per_step": round(msf, 3), "local_precision": prec,
+                     "refinements": refine, "convection_arith": conv,
+                     "local_systems": "loss-cone trimmed" if trim else "full",
+                     "max_rel_err_one_step_vs_plain_fp64": err}
+    plain = out["plain_fp64"]["ms_per_step"]
+    for v in out.values():
+        v["speedup_vs_plain_fp64"] = round(plain / v["ms_per_step"], 3)
+    return {"forms": out, "steps_timed": args.form_steps,
+            "error": "norm-wise max|psd - psd_plain| / max|psd_plain| after one step from the "
+                     "same initial state; tolerance 1e-8",
+            "timing": "CUDA events, graph-replayed steps after 3 warm-up steps, one context "
+                      "at a time"}
 
 
 # --------------------------------------------------------------------------- ensemble
@@ -554,25 +642,59 @@ class ReferenceSampler:
                                    self.ipiv.ctypes.data_as(ctypes.POINTER(ctypes.c_long)),
                                    ctypes.c_int(recompute), ctypes.c_int(self.cores))
 
+    def set_hour(self, h):
+        """Inputs of simulated hour h of the run: the hourly drift velocities
+        and the D_LL scale of that hour's Kp (as the timed GPU steps see them)."""
+        from verb4d_b200 import workload as W
+
+        wl = self.wl
+        h = min(int(h), len(wl.kp) - 1)
+        if h == getattr(self, "hour", None):
+            return
+        self.hour = h
+        vp, vr = W.drift_velocities(wl.spec, float(wl.kp[h]))
+        self.state.keep["VP"][...] = vp
+        self.state.keep["VR"][...] = vr
+        self.state.keep["DLL"][...] = wl.fields["DLL_base"] * wl.dll_scale(h)
+        w2 = copy.copy(wl)
+        w2.fields = dict(wl.fields, VP=vp, VR=vr)
+        self.ns = W.convection_substeps(w2)
+
     def sample_step(self, conv_slices=None):
         """Seconds for one full step on all host cores, from one bounded sample."""
         wl = self.wl
         P, R, V, K = wl.spec.shape
         ip = ctypes.POINTER(ctypes.c_int)
-        nconv = conv_slices or self.cores
-        vk = np.array([divmod(int(i), K) for i in self.rng.choice(V * K, size=nconv, replace=False)],
-                      dtype=np.int32)
+        nconv = min(conv_slices or self.cores, self.cores)
+        # convection: a group of slices with (nearly) equal sub-step counts, one
+        # per thread, around a point of the sorted counts drawn with
+        # probability proportional to the sub-steps (where the step's work
+        # is).  Each thread then carries the same work, so the wall time is the
+        # per-thread time of ns_max sub-steps with all threads busy, and a full
+        # step (dynamic scheduling over all slices, as the reference's loop)
+        # is that per-sub-step time times the total sub-steps over the threads.
+        flat = self.ns.ravel()
+        order = np.argsort(flat, kind="stable")
+        cum = np.cumsum(flat[order], dtype=np.float64)
+        c = int(np.searchsorted(cum, self.rng.uniform(0.0, cum[-1]), side="right"))
+        c = min(c, len(order) - 1)
+        lo = max(0, min(c - nconv // 2, len(order) - nconv))
+        pick = order[lo:lo + nconv]
+        vk = np.array([divmod(int(i), K) for i in pick], dtype=np.int32)
         t0 = time.perf_counter()
         self.lib.ref_conv_slices(ctypes.byref(self.state.st), ctypes.c_double(wl.dt),
                                  vk.ctypes.data_as(ip), ctypes.c_int(nconv), ctypes.c_int(self.cores))
         t_c = time.perf_counter() - t0
-        sub = int(sum(self.ns[v, k] for v, k in vk))
-        # slices run concurrently: the wall time of a batch of `cores` slices is set by the
-        # heaviest one, so scale by work (sub-steps) per thread rather than by batch count
-        t_conv = t_c * self.ns.sum() / max(sub, 1)
-        nl = 256 * self.cores
-        pvk = np.stack([self.rng.integers(0, P, nl), self.rng.integers(0, V, nl),
-                        self.rng.integers(0, K, nl)], axis=1).astype(np.int32)
+        sub = int(flat[pick].sum())
+        ns_max = int(flat[pick].max())
+        t_conv = t_c / ns_max * float(self.ns.sum()) / self.cores
+        # radial: whole runs of K (the fastest index) at random (P, V), in the
+        # order the reference's collapse(3) loop visits lines, so that the
+        # sampled lines share cache lines as the full loop's do
+        nblk = max(1, (256 * self.cores + K - 1) // K)
+        blk = [(int(self.rng.integers(P)), int(self.rng.integers(V))) for _ in range(nblk)]
+        pvk = np.array([(p, v, k) for p, v in blk for k in range(K)], dtype=np.int32)
+        nl = len(pvk)
         t0 = time.perf_counter()
         self.lib.ref_radial_lines(ctypes.byref(self.state.st), ctypes.c_double(wl.dt),
                                   pvk.ctypes.data_as(ip), ctypes.c_int(nl), ctypes.c_int(self.cores))
@@ -582,6 +704,8 @@ class ReferenceSampler:
         t_local = (time.perf_counter() - t0) * (P * R) / (len(self.pr) // 2)
         t_fac = self.t_factor_step / 288.0
         self.samples += 1
+        self.last_phases = {"convection": t_conv, "radial": t_rad, "local": t_local,
+                            "factor_per_step": t_fac}
         self.last = (f"reference routines from source in the reference's OpenMP phase loops "
                      f"(oracle/_ref), {self.cores} threads; per sample: {nconv} convection slices "
                      f"({sub} of {int(self.ns.sum())} slice-substeps), {nl} radial lines, "
@@ -616,15 +740,21 @@ def run_reference(args):
     from verb4d_b200 import workload as W
 
     spec = W.CONFIGS[args.config]
-    wl = W.make_workload(spec, seed=args.seed, kp=W.kp_series(args.seed, 24))
+    hours = int(np.ceil((args.warmup + args.steps + 1) * W.DT_5MIN * 24)) + 1
+    # the Kp series of the GPU arm (rank 0's seed): the same inputs hour by hour
+    wl = W.make_workload(spec, seed=args.seed, kp=W.kp_series(args.seed, max(hours, 24)))
     rs = ReferenceSampler(wl)
-    # each bench step is one bounded sample of a full step; a few convection
-    # slices per step keeps the whole --steps/--warmup run within minutes
+    # each bench step is one bounded sample of a full step of the same hour
+    # as the GPU arm's step; a few convection slices per step keeps the
+    # whole --steps/--warmup run within minutes
     nconv = max(1, min(rs.cores, int(8 * rs.cores * 4 / max(args.steps + args.warmup, 1))))
-    for _ in range(args.warmup):
+    hour = lambda it: int(np.floor(it * wl.dt * 24 + 1e-9))  # noqa: E731
+    for it in range(1, args.warmup + 1):
+        rs.set_hour(hour(it))
         rs.sample_step(nconv)
     t_total = 0.0
-    for _ in range(args.steps):
+    for it in range(args.warmup + 1, args.warmup + args.steps + 1):
+        rs.set_hour(hour(it))
         t_total += rs.sample_step(nconv)
     rs.close()
     sim_h = args.steps * wl.dt * 24.0
@@ -634,8 +764,8 @@ def run_reference(args):
            "warmup": args.warmup, "ms_per_step": round(t_total / args.steps * 1e3, 1),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (seeded)", "impl": "reference",
-           "config": {"workload": f"VERB-4D operator-split step {args.config} (P,R,V,K)={spec.shape}, "
-                                  f"dt=5 min", "parallelism": f"host threads {rs.cores}"},
+           "config": workload_config(args, spec, world),
+           "impl": {"host_threads": rs.cores},
            "cpu_baseline": {"value": value, "unit": "sim-hours/s", "cores": rs.cores,
                             "kind": "reference", "sample": rs.last},
            "e2e": {"value": value, "unit": "sim-hours/s", "h2d_bytes_per_step": 0,
@@ -668,6 +798,9 @@ def main():
     ap.add_argument("--members", type=int, default=64)
     ap.add_argument("--ens-steps", type=int, default=12)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip timing the plain / mixed forms beside the main run")
+    ap.add_argument("--form-steps", type=int, default=5)
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--traffic", type=float, default=None,
                     help="dram bytes per local-solve launch from an ncu capture")

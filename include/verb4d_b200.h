@@ -246,6 +246,11 @@ int verb_convection_da_state(verb_ctx* ctx, int v, int k, double* Pa_host, doubl
  * reference. */
 int verb_local_solve_variants(int* count);
 int verb_local_solve_variant(int v, int* warps_per_cta, int* l_columns, int* u_columns);
+/* 1 when shape v keeps the right-hand-side window of the substitutions in
+ * registers (the factor columns still stream through shared memory), 0 when
+ * the window lives in shared memory.  Bands wider than the register window
+ * holds (V > 126) fall back to the shared-memory window. */
+int verb_local_solve_variant_window(int v, int* in_registers);
 /* v = -1: the shape tuned for this context's shape in this process (else 0) */
 int verb_set_local_solve_variant(verb_ctx* ctx, int v);
 int verb_autotune_local_solve(verb_ctx* ctx, double dt, double sub_dt, double* times_ms,
@@ -418,8 +423,8 @@ int verb_convection_2d(double* psd, const double* P, const double* R, int nP, in
  * caller's DEVICE memory, for callers that cannot allocate device memory (a
  * host application or plugin that owns every allocation, or a path where an
  * allocation is not allowed).  It calls no allocator: the kernel's scratch is
- * a fixed array in the library's device code of 5 doubles per point of
- * VERB_NOALLOC_MAX_POINTS points (320 KiB) plus a few status words, held on
+ * a fixed array in the library's device code of 7 doubles per point of
+ * VERB_NOALLOC_MAX_POINTS points (448 KiB) plus a few status words, held on
  * every device that loads that code until exit.  CUDA loads device code
  * lazily, so the first call on a device loads it (the array and the kernel
  * take their device memory then, and the device may synchronise) and looks

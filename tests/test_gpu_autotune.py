@@ -17,12 +17,12 @@ def test_shapes_identical_and_tuning_side_effect_free(gpu, form):
     c = load_ctx(wl)
     c.set_local_precision(form, 0)
     shapes = c.solve_variants()
-    assert len(shapes) >= 2 and shapes[0] == (4, 4, 2)
+    assert len(shapes) >= 2 and shapes[0] == (4, 4, 2, 0)
     before = c.download()
     chosen, times = c.autotune_local_solve(wl.dt, wl.sub_dt)
     assert np.array_equal(c.download(), before)
     assert np.all(times > 0) and times[chosen] == times.min()
-    print(form, "local solve shapes (warps/CTA, L cols, U cols) -> ms:",
+    print(form, "local solve shapes (warps/CTA, L cols, U cols, window in registers) -> ms:",
           {str(s): round(float(t), 4) for s, t in zip(shapes, times)}, "chosen", shapes[chosen])
     c.local(wl.dt, wl.sub_dt)
     c.sync()

@@ -757,6 +757,14 @@ int verb_local_solve_variant(int v, int* warps_per_cta, int* l_columns, int* u_c
     return VERB_OK;
 }
 
+int verb_local_solve_variant_window(int v, int* in_registers)
+{
+    if (v < 0 || v >= local_solve_variants() || !in_registers) return VERB_ERR_ARG;
+    int w = 0, f = 0, b = 0;
+    local_solve_variant_shape(v, &w, &f, &b, in_registers);
+    return VERB_OK;
+}
+
 int verb_set_local_solve_variant(verb_ctx* c, int v)
 {
     if (!c || v < -1 || v >= local_solve_variants()) return VERB_ERR_ARG;

@@ -455,11 +455,15 @@ __device__ __forceinline__ void cp_wait()
 // per warp.  More columns in flight hide more latency per warp but take
 // shared memory that would otherwise hold more resident warps; the best
 // trade depends on the grid, so the autotuner picks one per context.
+// The second group keeps the right-hand-side window in registers instead of
+// shared memory (local_solve_rw_kernel).
 struct SolveShape {
-    int warps, fwd, bwd;
+    int warps, fwd, bwd, rw;
 };
-constexpr SolveShape SOLVE_SHAPES[] = {{4, 4, 2}, {4, 6, 3}, {2, 6, 4},  {2, 8, 6}, {1, 8, 6},
-                                       {1, 12, 8}, {1, 12, 10}, {1, 16, 12}, {1, 24, 16}};
+constexpr SolveShape SOLVE_SHAPES[] = {
+    {4, 4, 2, 0},  {4, 6, 3, 0},  {2, 6, 4, 0},  {2, 8, 6, 0},  {1, 8, 6, 0},  {1, 12, 8, 0},
+    {1, 12, 10, 0}, {1, 16, 12, 0}, {1, 24, 16, 0},
+    {4, 4, 3, 1},  {4, 6, 4, 1},  {2, 8, 6, 1},  {2, 12, 8, 1}, {1, 12, 8, 1}, {1, 16, 12, 1}};
 constexpr int N_SOLVE_SHAPES = sizeof(SOLVE_SHAPES) / sizeof(SOLVE_SHAPES[0]);
 constexpr int FWD_WIN = 128;   // >= kl + 1
 constexpr int BWD_WIN = 256;   // >= kv + 1
@@ -583,6 +587,166 @@ __global__ void __launch_bounds__(SOLVE_WARPS * 32) local_solve_kernel(LocalArgs
             w[j] = bj;
             if (j - BWD_WIN >= 0) cp_async8(&win[j & (BWD_WIN - 1)], &w[j - BWD_WIN]);
         }
+        issue_U(j - BWD_DEPTH);
+        cp_commit();
+    }
+    cp_wait<0>();
+}
+
+// The same solve with the right-hand-side window in registers.  Forward
+// (xGBTRS with interleaved row interchanges), at column j the window holds
+// positions j .. j+32FS-1: lane i's slot m holds position
+// j + ((i - j) & 31) + 32m, so the updates of column j (positions
+// j+1 .. j+lm) touch every lane's slots in place, the pivot row l is read from
+// lane l & 31, slot (l - j) >> 5, and only lane j & 31 shifts its slots down
+// (position j leaves, position j + 32FS enters) when the column is done.
+// Backward (xTBSV), at column j the window holds j .. j-32BS+1 the same way
+// downwards.  The factor columns still stream through a per-warp cp.async
+// ring in shared memory (read with rotated, conflict-free accesses), and the
+// right-hand-side entries that enter the window are staged with them.  The
+// operations and their order are those of local_solve_kernel, so the result is
+// bit-identical; what changes is that the window no longer costs shared-memory
+// loads and stores per column, which the old kernel's column chain waited on.
+template <typename T, int SOLVE_WARPS, int FWD_DEPTH, int BWD_DEPTH, int FS, int BS>
+__global__ void __launch_bounds__(SOLVE_WARPS * 32) local_solve_rw_kernel(LocalArgs a, int nsys)
+{
+    extern __shared__ double sm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int sys = blockIdx.x * SOLVE_WARPS + warp;
+    if (sys >= nsys || skip_system(a, sys)) return;
+    const int n = a.d.V * (a.d.K - sys_k0(a, sys));
+    const size_t u0 = sys_uoff(a, sys);
+    const bool f32 = sizeof(T) == sizeof(float);
+    const int kl = a.kl, kv = a.kv, klp = f32 ? a.klp32 : a.klp, kvp = f32 ? a.kvp32 : a.kvp;
+    constexpr int VEC = 16 / sizeof(T);
+    constexpr int FWIN = 32 * FS, BWIN = 32 * BS;
+    constexpr int STAGE = (FWD_DEPTH > BWD_DEPTH ? FWD_DEPTH : BWD_DEPTH) + 1 & ~1;
+    const size_t per_warp = STAGE + solve_ring_doubles(klp, kvp, sizeof(T), FWD_DEPTH, BWD_DEPTH);
+    double* stage = sm + (size_t)warp * per_warp;  // entering right-hand-side entries
+    T* ring = (T*)(stage + STAGE);
+    double* w = a.work + u0;
+    const T* Lf = (f32 ? (const T*)a.Lf32 : (const T*)a.Lf) + u0 * klp;
+    const T* Uf = (f32 ? (const T*)a.Uf32 : (const T*)a.Uf) + u0 * kvp;
+    const int32_t* ip = a.ipiv + u0;
+
+    // ---------------- forward: L with interleaved row interchanges (xGBTRS) --------
+    double s[FS > BS ? FS : BS];
+#pragma unroll
+    for (int m = 0; m < FS; m++) {
+        const int p = lane + 32 * m;
+        s[m] = p < n ? w[p] : 0.0;
+    }
+    // column col's multipliers, and b[col + FWIN] (which enters the window
+    // when column col is done)
+    auto issue_L = [&](int col) {
+        if (col < n - 1) {
+            T* dst = ring + (col % FWD_DEPTH) * klp;
+            const T* src = Lf + (size_t)col * klp;
+            for (int c = lane; c < klp / VEC; c += 32) cp_async16(dst + VEC * c, src + VEC * c);
+            if (lane == 0) {
+                double* st = &stage[col % FWD_DEPTH];
+                if (col + FWIN < n) cp_async8(st, &w[col + FWIN]);
+                else *st = 0.0;
+            }
+        }
+    };
+    for (int c = 0; c < FWD_DEPTH; c++) {
+        issue_L(c);
+        cp_commit();
+    }
+    int pv_cur = (lane < n) ? ip[lane] : 0;
+    int pv_next = (32 + lane < n) ? ip[32 + lane] : 0;
+    for (int j = 0; j < n - 1; j++) {
+        if ((j & 31) == 0 && j > 0) {
+            pv_cur = pv_next;
+            const int nx = j + 32 + lane;
+            pv_next = (nx < n) ? ip[nx] : 0;
+        }
+        cp_wait<FWD_DEPTH - 1>();
+        __syncwarp();
+        const int lm = min(kl, n - 1 - j);
+        const int l = __shfl_sync(0xffffffffu, pv_cur, j & 31);
+        const int sl = (l - j) >> 5;  // slot of position l in lane l & 31
+        double v = s[0];
+#pragma unroll
+        for (int m = 1; m < FS; m++) v = (sl == m) ? s[m] : v;
+        const double bl = __shfl_sync(0xffffffffu, v, l & 31);
+        const double bj_old = __shfl_sync(0xffffffffu, s[0], j & 31);
+        const double bj = (l != j) ? bl : bj_old;
+        if (l != j && lane == (l & 31)) {
+#pragma unroll
+            for (int m = 0; m < FS; m++)
+                if (sl == m) s[m] = bj_old;
+        }
+        if (bj != 0.0) {
+            const T* Lc = ring + (j % FWD_DEPTH) * klp;
+            const double tmp = -bj;
+            const int o = (lane - j) & 31;
+#pragma unroll
+            for (int m = 0; m < FS; m++) {
+                const int e = o + 32 * m - 1;  // position j + 1 + e
+                if (e >= 0 && e < lm) s[m] = s[m] + (double)Lc[e] * tmp;  // xGER in xGBTRS
+            }
+        }
+        if (lane == (j & 31)) {
+            w[j] = bj;
+#pragma unroll
+            for (int m = 0; m + 1 < FS; m++) s[m] = s[m + 1];
+            s[FS - 1] = stage[j % FWD_DEPTH];
+        }
+        __syncwarp();
+        issue_L(j + FWD_DEPTH);
+        cp_commit();
+    }
+    cp_wait<0>();
+    __syncwarp();
+    if (lane == ((n - 1) & 31)) w[n - 1] = s[0];
+    __syncwarp();
+
+    // ---------------- backward: U, column oriented (xTBSV 'U','N','N') ------------
+#pragma unroll
+    for (int m = 0; m < BS; m++) {
+        const int p = (n - 1) - ((n - 1 - lane) & 31) - 32 * m;
+        s[m] = p >= 0 ? w[p] : 0.0;
+    }
+    auto issue_U = [&](int col) {
+        if (col >= 0) {
+            T* dst = ring + ((n - 1 - col) % BWD_DEPTH) * kvp;
+            const T* src = Uf + (size_t)col * kvp;
+            for (int c = lane; c < kvp / VEC; c += 32) cp_async16(dst + VEC * c, src + VEC * c);
+            if (lane == 0) {
+                double* st = &stage[(n - 1 - col) % BWD_DEPTH];
+                if (col - BWIN >= 0) cp_async8(st, &w[col - BWIN]);
+                else *st = 0.0;
+            }
+        }
+    };
+    for (int c = 0; c < BWD_DEPTH; c++) {
+        issue_U(n - 1 - c);
+        cp_commit();
+    }
+    for (int j = n - 1; j >= 0; j--) {
+        cp_wait<BWD_DEPTH - 1>();
+        __syncwarp();
+        const T* Uc = ring + ((n - 1 - j) % BWD_DEPTH) * kvp;
+        double bj = __shfl_sync(0xffffffffu, s[0], j & 31);
+        if (bj != 0.0) {
+            bj = bj / (double)Uc[kv];
+            const int o = (j - lane) & 31;
+#pragma unroll
+            for (int m = 0; m < BS; m++) {
+                const int d = o + 32 * m;  // position j - d
+                if (d >= 1 && d <= kv && d <= j)
+                    s[m] = s[m] - bj * (double)Uc[kv - d];  // xTBSV: X(I) - TEMP*A(L+I,J)
+            }
+        }
+        if (lane == (j & 31)) {
+            w[j] = bj;
+#pragma unroll
+            for (int m = 0; m + 1 < BS; m++) s[m] = s[m + 1];
+            s[BS - 1] = stage[(n - 1 - j) % BWD_DEPTH];
+        }
+        __syncwarp();
         issue_U(j - BWD_DEPTH);
         cp_commit();
     }
@@ -1053,11 +1217,35 @@ void launch_local_store(const LocalArgs& a, cudaStream_t s)
 
 namespace {
 
-template <typename T, int W, int FD, int BD>
+template <typename T, int W, int FD, int BD, int RW>
 void launch_solve_t(const LocalArgs& a, const size_t kl_p, const size_t kv_p, cudaStream_t s)
 {
     const int nsys = a.d.P * a.d.R;
     const int grid = (nsys + W - 1) / W;
+    if (RW) {
+        // slots of the register window: 32 FS > kl, 32 BS > kv
+        const int fs = (a.kl + 1 + 31) / 32, bs = (a.kv + 1 + 31) / 32;
+        constexpr int STAGE = (FD > BD ? FD : BD) + 1 & ~1;
+        const size_t smem =
+            (size_t)W * (STAGE + solve_ring_doubles((int)kl_p, (int)kv_p, sizeof(T), FD, BD)) *
+            sizeof(double);
+#define VERB_RW(F, B)                                                                         \
+    if (fs <= F && bs <= B) {                                                                 \
+        allow_max_dynamic_smem((const void*)local_solve_rw_kernel<T, W, FD, BD, F, B>);       \
+        local_solve_rw_kernel<T, W, FD, BD, F, B><<<grid, W * 32, smem, s>>>(a, nsys);        \
+        return;                                                                               \
+    }
+        VERB_RW(1, 1)
+        VERB_RW(1, 2)
+        VERB_RW(2, 3)
+        VERB_RW(2, 4)
+        VERB_RW(3, 5)
+        VERB_RW(3, 6)
+        VERB_RW(4, 7)
+        VERB_RW(4, 8)
+#undef VERB_RW
+        // wider bands than the register window holds: the shared-memory window
+    }
     const size_t smem =
         (size_t)W * (BWD_WIN + solve_ring_doubles((int)kl_p, (int)kv_p, sizeof(T), FD, BD)) *
         sizeof(double);
@@ -1069,10 +1257,10 @@ template <typename T>
 void launch_solve_v(const LocalArgs& a, int v, size_t klp, size_t kvp, cudaStream_t s)
 {
     switch (v) {
-#define VERB_SOLVE_CASE(i)                                                                   \
-    case i:                                                                                  \
-        launch_solve_t<T, SOLVE_SHAPES[i].warps, SOLVE_SHAPES[i].fwd, SOLVE_SHAPES[i].bwd>( \
-            a, klp, kvp, s);                                                                 \
+#define VERB_SOLVE_CASE(i)                                                                \
+    case i:                                                                               \
+        launch_solve_t<T, SOLVE_SHAPES[i].warps, SOLVE_SHAPES[i].fwd, SOLVE_SHAPES[i].bwd, \
+                       SOLVE_SHAPES[i].rw>(a, klp, kvp, s);                               \
         break;
         VERB_SOLVE_CASE(1)
         VERB_SOLVE_CASE(2)
@@ -1082,25 +1270,32 @@ void launch_solve_v(const LocalArgs& a, int v, size_t klp, size_t kvp, cudaStrea
         VERB_SOLVE_CASE(6)
         VERB_SOLVE_CASE(7)
         VERB_SOLVE_CASE(8)
+        VERB_SOLVE_CASE(9)
+        VERB_SOLVE_CASE(10)
+        VERB_SOLVE_CASE(11)
+        VERB_SOLVE_CASE(12)
+        VERB_SOLVE_CASE(13)
+        VERB_SOLVE_CASE(14)
 #undef VERB_SOLVE_CASE
         default:
-            launch_solve_t<T, SOLVE_SHAPES[0].warps, SOLVE_SHAPES[0].fwd, SOLVE_SHAPES[0].bwd>(
-                a, klp, kvp, s);
+            launch_solve_t<T, SOLVE_SHAPES[0].warps, SOLVE_SHAPES[0].fwd, SOLVE_SHAPES[0].bwd,
+                           SOLVE_SHAPES[0].rw>(a, klp, kvp, s);
     }
 }
 
 }  // namespace
 
-static_assert(N_SOLVE_SHAPES == 9, "launch_solve_v lists every shape");
+static_assert(N_SOLVE_SHAPES == 15, "launch_solve_v lists every shape");
 
 int local_solve_variants() { return N_SOLVE_SHAPES; }
 
-void local_solve_variant_shape(int v, int* warps, int* fwd, int* bwd)
+void local_solve_variant_shape(int v, int* warps, int* fwd, int* bwd, int* rw)
 {
     const SolveShape& sh = SOLVE_SHAPES[v >= 0 && v < N_SOLVE_SHAPES ? v : 0];
     *warps = sh.warps;
     *fwd = sh.fwd;
     *bwd = sh.bwd;
+    if (rw) *rw = sh.rw;
 }
 
 void launch_local_solve(const LocalArgs& a, cudaStream_t s)

@@ -153,7 +153,7 @@ void launch_local_factor(const LocalArgs& a, cudaStream_t s);
 void launch_local_rhs(const LocalArgs& a, bool from_work, cudaStream_t s);
 void launch_local_solve(const LocalArgs& a, cudaStream_t s);
 int local_solve_variants();
-void local_solve_variant_shape(int v, int* warps, int* fwd, int* bwd);
+void local_solve_variant_shape(int v, int* warps, int* fwd, int* bwd, int* rw = nullptr);
 void launch_local_store(const LocalArgs& a, cudaStream_t s);
 // r = b - A x for every system (A assembled on the fly in the reference's order)
 void launch_local_residual(const LocalArgs& a, const double* b, const double* x, double* r,

@@ -94,6 +94,7 @@ SIGNATURES = {
     "verb_local_solve_variants": (C.c_int, [C.POINTER(C.c_int)]),
     "verb_local_solve_variant": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                            C.POINTER(C.c_int)]),
+    "verb_local_solve_variant_window": (C.c_int, [C.c_int, C.POINTER(C.c_int)]),
     "verb_set_local_solve_variant": (C.c_int, [_vp, C.c_int]),
     "verb_autotune_local_solve": (C.c_int, [_vp, C.c_double, C.c_double, _dp,
                                             C.POINTER(C.c_int)]),

@@ -95,16 +95,17 @@ class Context:
         return pa, mm
 
     def solve_variants(self) -> list:
-        """(warps per CTA, L columns in flight, U columns in flight) of every
-        local-solve shape."""
+        """(warps per CTA, L columns in flight, U columns in flight, window in
+        registers) of every local-solve shape."""
         n = C.c_int()
         L.check(self.lib.verb_local_solve_variants(C.byref(n)), "variants")
         out = []
         for v in range(n.value):
-            w, f, b = C.c_int(), C.c_int(), C.c_int()
+            w, f, b, r = C.c_int(), C.c_int(), C.c_int(), C.c_int()
             L.check(self.lib.verb_local_solve_variant(v, C.byref(w), C.byref(f), C.byref(b)),
                     "variant")
-            out.append((w.value, f.value, b.value))
+            L.check(self.lib.verb_local_solve_variant_window(v, C.byref(r)), "variant window")
+            out.append((w.value, f.value, b.value, r.value))
         return out
 
     def set_local_solve_variant(self, v: int = -1):
