@@ -210,6 +210,12 @@ int verb_cnn_forward(verb_cnn* cnn, const float* in_dev, float* out_dev, int bat
 /* MSE loss against target_dev, backward pass, Adam step (lr <= 0: gradients only) */
 int verb_cnn_train_step(verb_cnn* cnn, const float* in_dev, const float* target_dev, int batch,
                         float lr, float* loss_host);
+/* Backward pass and Adam step (lr <= 0: gradients only) for an output
+ * gradient the caller computed (grad_out_dev, the network output's shape),
+ * through the activations of the last verb_cnn_forward, which must have run
+ * on in_dev with the same batch. */
+int verb_cnn_backward_step(verb_cnn* cnn, const float* in_dev, const float* grad_out_dev, int batch,
+                           float lr);
 
 /* ---- convection data assimilation ------------------------------------------
  * runKalmanFilterConvection2D (src/DataAssimilationConvection.cpp:124-253)
@@ -303,6 +309,25 @@ typedef struct {
 int verb_local_krylov(verb_ctx* ctx, double dt, double sub_dt, int guess, verb_cnn* cnn,
                       int smooth, double omega, int max_outer, int inner_maxit, double inner_tol,
                       double resid_tol, verb_krylov_stats* stats);
+/* Learned preconditioner of the Krylov form (no counterpart in the reference):
+ * a CNN with 9 input channels and 25 output channels on the K x V grid of a
+ * local system predicts, for every unknown i, the 25 coefficients C[o](i) of
+ * a sparse approximate inverse on its 5 x 5 neighbourhood o,
+ *   M v (i) = sum_o (delta(o = 0) + C[o](i)) v(i + o) / diag(i + o),
+ * which replaces the Jacobi preconditioner of the BiCGSTAB in
+ * verb_local_krylov (C = 0 is Jacobi).  Its inputs are the system's matrix:
+ * log10(|diag| dt) and the eight off-diagonal entries of each row over the
+ * diagonal, [sys][9][K][V] (verb_local_precond_inputs, which also returns the
+ * FP32 diagonals [sys][9][V*K]).  verb_precond_loss_grad gives its training
+ * signal: for nprobe probe vectors z per system ([sys][nprobe][V*K]) the loss
+ * mean |A M z - z|^2 and its gradient with respect to C ([sys][25][V*K]), to
+ * pass to verb_cnn_backward_step.  net = NULL restores Jacobi.  The context
+ * keeps the pointer: the network must outlive its use. */
+int verb_set_krylov_preconditioner(verb_ctx* ctx, verb_cnn* net);
+int verb_local_precond_inputs(verb_ctx* ctx, double dt, double sub_dt, float* feat_dev,
+                              float* A9_dev);
+int verb_precond_loss_grad(const float* A9_dev, const float* C_dev, const float* Z_dev, int nsys,
+                           int V, int K, int nprobe, float* gC_dev, float* loss_host, void* stream);
 /* One local step by the LU (as verb_local, with its refinement steps) that also
  * writes, for the last sub-step, the CNN features of every system
  * (feat_dev, [P*R][4][K][V] floats) and the training target

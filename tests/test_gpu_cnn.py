@@ -1,7 +1,9 @@
-"""The warm-start CNN's CUDA kernels against the CPU restatement
-(oracle/cnn_ref.py): forward pass and the gradients of one training step
-(FP32 device sums against float64 ones, checked norm-wise at 1e-4), and a few
-Adam steps that reduce the loss of a fixed batch."""
+"""The warm-start CNN's CUDA kernels (tensor-core implicit GEMMs with TF32
+operands) against the CPU restatement (oracle/cnn_ref.py, which rounds the
+same operands to TF32): forward pass and the gradients of one training step
+(FP32 device sums against float64 ones, checked norm-wise at 1e-5 / 1e-4),
+at a size that spans several GEMM tiles and K chunks, and a few Adam steps
+that reduce the loss of a fixed batch."""
 import numpy as np
 import pytest
 
@@ -12,11 +14,11 @@ pytestmark = pytest.mark.gpu
 CH = (4, 8, 8, 1)
 
 
-def test_forward_and_gradients_match_cpu(gpu):
+@pytest.mark.parametrize("B,H,W,CH", [(3, 9, 7, CH), (5, 31, 31, (4, 32, 32, 32, 1))])
+def test_forward_and_gradients_match_cpu(gpu, B, H, W, CH):
     import torch
 
     rng = np.random.default_rng(0)
-    B, H, W = 3, 9, 7
     net = CNN(H, W, B, channels=CH, seed=1)
     p = net.params()
     x = rng.standard_normal((B, 4, H, W)).astype(np.float32)

@@ -6,11 +6,9 @@
 //
 // Tensors are NCHW FP32 ([batch][channel][H][W], W fastest).  A layer's
 // weights are [Cout][Cin][3][3] (FP32 master copy, FP16 copy used by the
-// forward and backward passes) plus an FP32 bias [Cout].  One thread computes
-// one output value (forward, input gradient) or one weight gradient; the
-// batch sizes here (hundreds of 31x31 or 101x91 images, 32 channels) keep
-// every SM busy with plain FP32 FMA work, which is far from the tensor-core
-// regime (the whole network is ~2e8 multiply-adds per batch).
+// forward and backward passes) plus an FP32 bias [Cout].  The convolutions
+// run on the tensor cores as implicit GEMMs (TF32 operands, FP32
+// accumulation; conv3x3_mma_kernel).
 #include <cuda_fp16.h>
 
 #include <algorithm>
@@ -23,120 +21,192 @@ namespace verb {
 
 namespace {
 
-__global__ void conv3x3_fwd_kernel(const float* __restrict__ in, const __half* __restrict__ w,
-                                   const float* __restrict__ bias, float* __restrict__ out, int B,
-                                   int Cin, int Cout, int H, int W, int relu)
+// The three convolution passes as implicit GEMMs on the tensor cores
+// (mma.sync m16n8k8, TF32 operands, FP32 accumulation).  With k = (ci, tap),
+// tap = 3 (dy+1) + (dx+1), and n = (b, y, x) a pixel of the batch:
+//   forward        out[co][n]  = bias[co] + sum_k w[co][k] in[ci][n + tap]
+//                  (M = Cout, K = 9 Cin, N = B H W; ReLU in the epilogue)
+//   input grad     gin[ci][n]  = sum_(co,tap) w[co][ci][tap] gout[co][n - tap]
+//                  (M = Cin, K = 9 Cout; masked where the input's ReLU was 0)
+//   weight grad    gw[co][k]   = sum_n gout[co][n] in[ci][n + tap]
+//                  (M = Cout, N = 9 Cin, K = B H W split across CTAs,
+//                  partial sums added atomically)
+// where an index outside the image reads zero (zero padding).  The FP16
+// weights are exact in TF32; activations and gradients are rounded to TF32
+// (cvt.rna) as they enter the MMA.  A warp computes a 16 x 32 tile (four
+// m16n8 accumulators) and fetches its fragments straight from global memory
+// (L1/L2 resident at these sizes).
+struct ConvGeom {
+    int B, Cin, Cout, H, W;
+};
+
+__device__ __forceinline__ uint32_t to_tf32(float x)
 {
-    const size_t total = (size_t)B * Cout * H * W;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-         i += (size_t)gridDim.x * blockDim.x) {
-        const int x = (int)(i % W);
-        const int y = (int)((i / W) % H);
-        const int co = (int)((i / ((size_t)W * H)) % Cout);
-        const int b = (int)(i / ((size_t)W * H * Cout));
-        float acc = bias[co];
-        const float* ib = in + (size_t)b * Cin * H * W;
-        const __half* wc = w + (size_t)co * Cin * 9;
-        for (int ci = 0; ci < Cin; ci++) {
-            const float* ic = ib + (size_t)ci * H * W;
-            const __half* wk = wc + ci * 9;
-#pragma unroll
-            for (int dy = -1; dy <= 1; dy++) {
-                const int yy = y + dy;
-                if (yy < 0 || yy >= H) continue;
-#pragma unroll
-                for (int dx = -1; dx <= 1; dx++) {
-                    const int xx = x + dx;
-                    if (xx < 0 || xx >= W) continue;
-                    acc = fmaf(__half2float(wk[(dy + 1) * 3 + (dx + 1)]), ic[yy * W + xx], acc);
-                }
-            }
-        }
-        out[i] = (relu && acc < 0.f) ? 0.f : acc;
-    }
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
 }
 
-// gradient wrt the layer input: full correlation with the flipped kernel;
-// `act` is the input activation when the input went through a ReLU (its
-// gradient is masked where the activation is 0), nullptr for the first layer
-__global__ void conv3x3_bwd_input_kernel(const float* __restrict__ gout, const __half* __restrict__ w,
-                                         const float* __restrict__ act, float* __restrict__ gin,
-                                         int B, int Cin, int Cout, int H, int W)
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2])
 {
-    const size_t total = (size_t)B * Cin * H * W;
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
-         i += (size_t)gridDim.x * blockDim.x) {
-        const int x = (int)(i % W);
-        const int y = (int)((i / W) % H);
-        const int ci = (int)((i / ((size_t)W * H)) % Cin);
-        const int b = (int)(i / ((size_t)W * H * Cin));
-        if (act && act[i] <= 0.f) {
-            gin[i] = 0.f;
-            continue;
-        }
-        float acc = 0.f;
-        const float* gb = gout + (size_t)b * Cout * H * W;
-        for (int co = 0; co < Cout; co++) {
-            const float* gc = gb + (size_t)co * H * W;
-            const __half* wk = w + ((size_t)co * Cin + ci) * 9;
-#pragma unroll
-            for (int dy = -1; dy <= 1; dy++) {
-                const int yy = y - dy;  // out(yy) used in(y) through tap dy
-                if (yy < 0 || yy >= H) continue;
-#pragma unroll
-                for (int dx = -1; dx <= 1; dx++) {
-                    const int xx = x - dx;
-                    if (xx < 0 || xx >= W) continue;
-                    acc = fmaf(__half2float(wk[(dy + 1) * 3 + (dx + 1)]), gc[yy * W + xx], acc);
-                }
-            }
-        }
-        gin[i] = acc;
-    }
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-// weight and bias gradients: one block per (co, ci, tap) or per co for the bias
-__global__ void conv3x3_bwd_weight_kernel(const float* __restrict__ in, const float* __restrict__ gout,
-                                          float* __restrict__ gw, float* __restrict__ gb, int B,
-                                          int Cin, int Cout, int H, int W)
+enum { CONV_FWD = 0, CONV_BWD_IN = 1, CONV_BWD_W = 2 };
+
+// element (m, k) of the A operand and (k, n) of the B operand of each pass
+template <int MODE>
+__device__ __forceinline__ float conv_a(const ConvGeom& g, const __half* w, const float* gout, int m,
+                                        int k, int M, int K)
+{
+    if (m >= M || k >= K) return 0.f;
+    if (MODE == CONV_FWD) return __half2float(w[(size_t)m * K + k]);  // w[co][ci*9+tap]
+    if (MODE == CONV_BWD_IN) {
+        const int co = k / 9, tap = k - co * 9;
+        return __half2float(w[((size_t)co * g.Cin + m) * 9 + tap]);
+    }
+    const size_t HW = (size_t)g.H * g.W;  // CONV_BWD_W: gout[b][co][p], k = (b, p)
+    const int b = (int)(k / HW);
+    return gout[((size_t)b * g.Cout + m) * HW + (k - b * HW)];
+}
+
+template <int MODE>
+__device__ __forceinline__ float conv_b(const ConvGeom& g, const float* src, int k, int n, int K, int N)
+{
+    if (k >= K || n >= N) return 0.f;
+    const int HW = g.H * g.W;
+    int b, p, c, tap;
+    if (MODE == CONV_BWD_W) {  // k = (b, p), n = (ci, tap): in[b][ci][p + tap]
+        b = k / HW;
+        p = k - b * HW;
+        c = n / 9;
+        tap = n - c * 9;
+    } else {                   // k = (c, tap), n = (b, p)
+        c = k / 9;
+        tap = k - c * 9;
+        b = n / HW;
+        p = n - b * HW;
+    }
+    const int y = p / g.W, x = p - (p / g.W) * g.W;
+    int dy = tap / 3 - 1, dx = tap - (tap / 3) * 3 - 1;
+    if (MODE == CONV_BWD_IN) {  // gout[b][co][p - tap]
+        dy = -dy;
+        dx = -dx;
+    }
+    const int yy = y + dy, xx = x + dx;
+    if (yy < 0 || yy >= g.H || xx < 0 || xx >= g.W) return 0.f;
+    const int C = MODE == CONV_BWD_IN ? g.Cout : g.Cin;
+    return src[(((size_t)b * C + c) * g.H + yy) * g.W + xx];
+}
+
+// One warp: rows m0 .. m0+15, columns n0 .. n0+31, k over [k_begin, k_end).
+// grid: x = column tiles of 128 (4 warps), y = row tiles of 16, z = K chunks
+// (weight gradient only).
+template <int MODE>
+__global__ void __launch_bounds__(128) conv3x3_mma_kernel(ConvGeom g, const float* __restrict__ src,
+                                                          const __half* __restrict__ w,
+                                                          const float* __restrict__ gout,
+                                                          const float* __restrict__ bias,
+                                                          const float* __restrict__ act,
+                                                          float* __restrict__ dst, int relu,
+                                                          int kchunk)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int gi = lane >> 2, ti = lane & 3;
+    const int HWi = g.H * g.W;
+    const int M = MODE == CONV_BWD_IN ? g.Cin : g.Cout;
+    const int K = MODE == CONV_FWD ? 9 * g.Cin : (MODE == CONV_BWD_IN ? 9 * g.Cout : g.B * HWi);
+    const int N = MODE == CONV_BWD_W ? 9 * g.Cin : g.B * HWi;
+    const int m0 = blockIdx.y * 16;
+    const int n0 = (blockIdx.x * 4 + warp) * 32;
+    if (n0 >= N) return;
+    const int kb = MODE == CONV_BWD_W ? blockIdx.z * kchunk : 0;
+    const int ke = MODE == CONV_BWD_W ? min(K, kb + kchunk) : K;
+    const float* bsrc = MODE == CONV_BWD_IN ? gout : src;
+    float acc[4][4] = {};
+    for (int k0 = kb; k0 < ke; k0 += 8) {
+        uint32_t a[4];
+        a[0] = to_tf32(conv_a<MODE>(g, w, gout, m0 + gi, k0 + ti, M, ke));
+        a[1] = to_tf32(conv_a<MODE>(g, w, gout, m0 + gi + 8, k0 + ti, M, ke));
+        a[2] = to_tf32(conv_a<MODE>(g, w, gout, m0 + gi, k0 + ti + 4, M, ke));
+        a[3] = to_tf32(conv_a<MODE>(g, w, gout, m0 + gi + 8, k0 + ti + 4, M, ke));
+#pragma unroll
+        for (int t = 0; t < 4; t++) {
+            const int n = n0 + 8 * t + gi;
+            uint32_t b[2];
+            b[0] = to_tf32(conv_b<MODE>(g, bsrc, k0 + ti, n, ke, N));
+            b[1] = to_tf32(conv_b<MODE>(g, bsrc, k0 + ti + 4, n, ke, N));
+            mma_tf32(acc[t], a, b);
+        }
+    }
+    // accumulator element e of tile t: row m0 + gi + 8 (e >> 1), column n0 + 8t + 2 ti + (e & 1)
+#pragma unroll
+    for (int t = 0; t < 4; t++)
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+            const int m = m0 + gi + 8 * (e >> 1);
+            const int n = n0 + 8 * t + 2 * ti + (e & 1);
+            if (m >= M || n >= N) continue;
+            float v = acc[t][e];
+            if (MODE == CONV_BWD_W) {
+                atomicAdd(&dst[(size_t)m * N + n], v);
+                continue;
+            }
+            const int b = n / HWi, p = n - b * HWi;
+            const size_t o = ((size_t)b * M + m) * HWi + p;
+            if (MODE == CONV_FWD) {
+                v += bias[m];
+                if (relu && v < 0.f) v = 0.f;
+            } else if (act && act[o] <= 0.f) {
+                v = 0.f;
+            }
+            dst[o] = v;
+        }
+}
+
+// bias gradient: one block per output channel, gb[co] = sum over the batch
+__global__ void conv_bias_grad_kernel(const float* __restrict__ gout, float* __restrict__ gb, int B,
+                                      int Cout, int HW)
 {
     __shared__ float red[256];
-    const int nw = Cout * Cin * 9;
-    for (int item = blockIdx.x; item < nw + Cout; item += gridDim.x) {
-        float acc = 0.f;
-        const size_t HW = (size_t)H * W;
-        if (item < nw) {
-            const int tap = item % 9, ci = (item / 9) % Cin, co = item / (9 * Cin);
-            const int dy = tap / 3 - 1, dx = tap % 3 - 1;
-            for (size_t j = threadIdx.x; j < (size_t)B * HW; j += blockDim.x) {
-                const int b = (int)(j / HW);
-                const int p = (int)(j - (size_t)b * HW);
-                const int y = p / W, x = p - (p / W) * W;
-                const int yy = y + dy, xx = x + dx;
-                if (yy < 0 || yy >= H || xx < 0 || xx >= W) continue;
-                acc = fmaf(gout[((size_t)b * Cout + co) * HW + p], in[((size_t)b * Cin + ci) * HW + yy * W + xx],
-                           acc);
-            }
-        } else {
-            const int co = item - nw;
-            for (size_t j = threadIdx.x; j < (size_t)B * HW; j += blockDim.x) {
-                const int b = (int)(j / HW);
-                const int p = (int)(j - (size_t)b * HW);
-                acc += gout[((size_t)b * Cout + co) * HW + p];
-            }
-        }
-        red[threadIdx.x] = acc;
-        __syncthreads();
-        for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-            if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) {
-            if (item < nw) gw[item] = red[0];
-            else gb[item - nw] = red[0];
-        }
+    const int co = blockIdx.x;
+    float acc = 0.f;
+    for (size_t j = threadIdx.x; j < (size_t)B * HW; j += blockDim.x) {
+        const int b = (int)(j / HW);
+        acc += gout[((size_t)b * Cout + co) * HW + (j - (size_t)b * HW)];
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
         __syncthreads();
     }
+    if (threadIdx.x == 0) gb[co] = red[0];
+}
+
+template <int MODE>
+void launch_conv_mma(const ConvGeom& g, const float* src, const __half* w, const float* gout,
+                     const float* bias, const float* act, float* dst, int relu, cudaStream_t s)
+{
+    const int HW = g.H * g.W;
+    const int M = MODE == CONV_BWD_IN ? g.Cin : g.Cout;
+    const int N = MODE == CONV_BWD_W ? 9 * g.Cin : g.B * HW;
+    dim3 grid((N + 127) / 128, (M + 15) / 16, 1);
+    int kchunk = 0;
+    if (MODE == CONV_BWD_W) {
+        // split the pixel reduction so that about 4 CTAs per SM run
+        const long long K = (long long)g.B * HW;
+        const long long want = 148 * 4 / ((long long)grid.x * grid.y) + 1;
+        kchunk = (int)((K + want - 1) / want);
+        kchunk = (kchunk + 7) / 8 * 8;
+        grid.z = (unsigned)((K + kchunk - 1) / kchunk);
+        cudaMemsetAsync(dst, 0, (size_t)M * N * sizeof(float), s);
+    }
+    conv3x3_mma_kernel<MODE><<<grid, 128, 0, s>>>(g, src, w, gout, bias, act, dst, relu, kchunk);
 }
 
 // mean squared error over the batch (sum / count) and its gradient
@@ -313,9 +383,11 @@ void forward(verb_cnn* n, const float* in, int B)
     for (int l = 0; l < n->L; l++) {
         float* y = n->act + n->aoff[l];
         const size_t tot = (size_t)B * n->cout[l] * n->H * n->W;
-        verb::conv3x3_fwd_kernel<<<verb::blocks_for(tot), 256, 0, n->s>>>(
-            x, n->ph + n->woff[l], n->p + n->boff[l], y, B, n->cin[l], n->cout[l], n->H, n->W,
-            l < n->L - 1 ? 1 : 0);
+        (void)tot;
+        const verb::ConvGeom g{B, n->cin[l], n->cout[l], n->H, n->W};
+        verb::launch_conv_mma<verb::CONV_FWD>(g, x, n->ph + n->woff[l], nullptr,
+                                              n->p + n->boff[l], nullptr, y,
+                                              l < n->L - 1 ? 1 : 0, n->s);
         x = y;
     }
 }
@@ -334,6 +406,43 @@ extern "C" int verb_cnn_forward(verb_cnn* n, const float* in_dev, float* out_dev
     return s;
 }
 
+namespace {
+
+// Backward pass from the output gradient in n->grad (first buffer) through
+// the activations of the last forward pass on in_dev, then an Adam step
+// (lr <= 0: gradients only).
+int backward_adam(verb_cnn* n, const float* in_dev, int B, float lr)
+{
+    const size_t HW = (size_t)n->H * n->W;
+    const int Lt = n->L - 1;
+    float* g0 = n->grad;
+    float* g1 = n->grad + n->amax;
+    int s = VERB_OK;
+    for (int l = Lt; l >= 0; l--) {
+        const float* xin = l > 0 ? n->act + n->aoff[l - 1] : in_dev;
+        const verb::ConvGeom g{B, n->cin[l], n->cout[l], n->H, n->W};
+        verb::launch_conv_mma<verb::CONV_BWD_W>(g, xin, nullptr, g0, nullptr, nullptr,
+                                                n->g + n->woff[l], 0, n->s);
+        verb::conv_bias_grad_kernel<<<n->cout[l], 256, 0, n->s>>>(g0, n->g + n->boff[l], B,
+                                                                  n->cout[l], (int)HW);
+        if (l > 0) {
+            verb::launch_conv_mma<verb::CONV_BWD_IN>(g, nullptr, n->ph + n->woff[l], g0, nullptr,
+                                                     n->act + n->aoff[l - 1], g1, 0, n->s);
+            std::swap(g0, g1);
+        }
+    }
+    if (lr > 0) {
+        n->t++;
+        const float b1 = 0.9f, b2 = 0.999f;
+        const float c1 = 1.f - powf(b1, (float)n->t), c2 = 1.f - powf(b2, (float)n->t);
+        verb::adam_kernel<<<verb::blocks_for(n->np), 256, 0, n->s>>>(n->p, n->ph, n->g, n->m, n->v,
+                                                                     n->np, lr, b1, b2, 1e-8f, c1, c2);
+    }
+    return s;
+}
+
+}  // namespace
+
 // One training step on a batch: MSE loss against target (device), backward
 // pass, Adam update with learning rate lr (lr <= 0: gradients only, no
 // update).  loss_host receives the batch loss.
@@ -345,34 +454,29 @@ extern "C" int verb_cnn_train_step(verb_cnn* n, const float* in_dev, const float
     const size_t HW = (size_t)n->H * n->W;
     const int Lt = n->L - 1;
     const size_t nout = (size_t)B * n->cout[Lt] * HW;
-    float* g0 = n->grad;
-    float* g1 = n->grad + n->amax;
     int s = ck(cudaMemsetAsync(n->loss, 0, sizeof(float), n->s));
     if (s) return s;
-    verb::mse_kernel<<<verb::blocks_for(nout), 256, 0, n->s>>>(n->act + n->aoff[Lt], target_dev, g0,
-                                                               nout, n->loss);
-    for (int l = Lt; l >= 0; l--) {
-        const float* xin = l > 0 ? n->act + n->aoff[l - 1] : in_dev;
-        verb::conv3x3_bwd_weight_kernel<<<148 * 8, 256, 0, n->s>>>(
-            xin, g0, n->g + n->woff[l], n->g + n->boff[l], B, n->cin[l], n->cout[l], n->H, n->W);
-        if (l > 0) {
-            const size_t tin = (size_t)B * n->cin[l] * HW;
-            verb::conv3x3_bwd_input_kernel<<<verb::blocks_for(tin), 256, 0, n->s>>>(
-                g0, n->ph + n->woff[l], n->act + n->aoff[l - 1], g1, B, n->cin[l], n->cout[l], n->H,
-                n->W);
-            std::swap(g0, g1);
-        }
-    }
-    if (lr > 0) {
-        n->t++;
-        const float b1 = 0.9f, b2 = 0.999f;
-        const float c1 = 1.f - powf(b1, (float)n->t), c2 = 1.f - powf(b2, (float)n->t);
-        verb::adam_kernel<<<verb::blocks_for(n->np), 256, 0, n->s>>>(n->p, n->ph, n->g, n->m, n->v,
-                                                                     n->np, lr, b1, b2, 1e-8f, c1, c2);
-    }
-    if (loss_host)
+    verb::mse_kernel<<<verb::blocks_for(nout), 256, 0, n->s>>>(n->act + n->aoff[Lt], target_dev,
+                                                               n->grad, nout, n->loss);
+    s = backward_adam(n, in_dev, B, lr);
+    if (!s && loss_host)
         s = ck(cudaMemcpyAsync(loss_host, n->loss, sizeof(float), cudaMemcpyDeviceToHost, n->s));
     if (!s) s = ck(cudaStreamSynchronize(n->s));
+    if (!s) s = ck(cudaGetLastError());
+    return s;
+}
+
+// The backward pass and Adam step for an output gradient computed by the
+// caller (grad_out_dev, the shape of the network's output): the activations
+// are those of the last verb_cnn_forward, which must have run on in_dev.
+extern "C" int verb_cnn_backward_step(verb_cnn* n, const float* in_dev, const float* grad_out_dev,
+                                      int B, float lr)
+{
+    if (!n || !in_dev || !grad_out_dev || B < 1 || B > n->maxb) return VERB_ERR_ARG;
+    const size_t nout = (size_t)B * n->cout[n->L - 1] * n->H * n->W;
+    int s = ck(cudaMemcpyAsync(n->grad, grad_out_dev, nout * sizeof(float), cudaMemcpyDeviceToDevice,
+                               n->s));
+    if (!s) s = backward_adam(n, in_dev, B, lr);
     if (!s) s = ck(cudaGetLastError());
     return s;
 }

@@ -452,8 +452,8 @@ __device__ __forceinline__ double block_max(double v, double* red)
 // registers, so nine warps per CTA fit beside the exact build's eight in the
 // same register file.  Nine warps split the 25 MLT-sweep jobs and the 24
 // L-sweep jobs of a 48 x 101 slice into three rounds each.
-#ifdef VERB_BUILD_CONV_FMA
-constexpr int C3_WARPS = 8;
+#if defined(VERB_CONV_WARPS)
+constexpr int C3_WARPS = VERB_CONV_WARPS;
 #else
 constexpr int C3_WARPS = 8;
 #endif
@@ -643,9 +643,16 @@ __host__ __device__ inline int plane_stride(int R)
 __host__ __device__ inline int plane_doubles(int P, int R) { return (P + 2 * GST) * plane_stride(R); }
 
 // offset (doubles) of the per-line arrays after the plane
+__host__ __device__ inline size_t conv_table_doubles(int P, int R, size_t* off_r);
+
 __host__ __device__ inline int conv_smem_doubles(int P, int R)
 {
-    return plane_doubles(P, R) + 4 * R + 4 * P + 32 + (R + P) + 2;
+    const int base = plane_doubles(P, R) + 4 * R + 4 * P + 32 + (R + P) + 2;
+#ifdef VERB_CONV_CR_SMEM
+    return base + (int)conv_table_doubles(P, R, nullptr);  // Courant tables in shared memory
+#else
+    return base;
+#endif
 }
 
 // per-CTA scratch: the Courant tables of both sweeps ([line][T][lpl]) and
@@ -710,11 +717,18 @@ __device__ __forceinline__ void sweep_job(const SweepRun& s, int job)
     const int nsmax = __reduce_max_sync(FULL, ns);
     const int jl = (n - 1) / T;  // the lane that owns cell n-1
 
-    // Courant numbers of the lane's faces (loaded where they are used: the
-    // table stays in L1, and registers are the scarce resource) and of the
-    // right neighbour's first face
-    const double* const ct = s.crtab + (size_t)li * T * lpl + j;
-    const double crn = __shfl_down_sync(FULL, ct[0], 1, lpl);
+    // Courant numbers of the lane's faces and of the right neighbour's first
+    // face
+    const double* const ct0 = s.crtab + (size_t)li * T * lpl + j;
+#ifdef VERB_CONV_CR_REG
+    double crr[T];
+#pragma unroll
+    for (int t = 0; t < T; t++) crr[t] = ct0[t * lpl];
+#define CT(t) crr[t]
+#else
+#define CT(t) ct0[(t) * lpl]
+#endif
+    const double crn = __shfl_down_sync(FULL, CT(0), 1, lpl);
 
     // ghost cells of E (QUICKEST6.cpp:94-140): ghost gi < 5 is low ghost
     // gi+1, gi >= 5 high ghost gi-4; the lanes of a line take the ten in turn
@@ -762,7 +776,7 @@ __device__ __forceinline__ void sweep_job(const SweepRun& s, int job)
 #pragma unroll
         for (int t = 0; t < T; t++)
             F[t] = face10<DIR>(W[t], W[t + 1], W[t + 2], W[t + 3], W[t + 4], W[t + 5], W[t + 6],
-                               W[t + 7], W[t + 8], W[t + 9], ct[t * lpl]);
+                               W[t + 7], W[t + 8], W[t + 9], CT(t));
         // B: unlimited cells (:245-249); cell 0 of a non-periodic line is
         // rewritten below, so its left flux (zero in the reference) is unused
         double fn = __shfl_down_sync(FULL, F[0], 1, lpl);
@@ -770,8 +784,8 @@ __device__ __forceinline__ void sweep_job(const SweepRun& s, int job)
 #pragma unroll
         for (int t = 0; t < T; t++) {
             const double fr = t + 1 < T ? F[t + 1] : fn;
-            const double cg = t + 1 < T ? ct[(t + 1) * lpl] : crn;
-            C[t] = W[GST + t] - (cg * fr - ct[t * lpl] * F[t]);
+            const double cg = t + 1 < T ? CT(t + 1) : crn;
+            C[t] = W[GST + t] - (cg * fr - CT(t) * F[t]);
         }
         __syncwarp();  // every lane has its window of E
         if (act) {
@@ -792,7 +806,7 @@ __device__ __forceinline__ void sweep_job(const SweepRun& s, int job)
             for (int i = 0; i < T + 7; i++) Uw[i] = X0[min(c0 - 4 + i, xmax) * xs];
 #pragma unroll
             for (int t = 0; t < T; t++)
-                F[t] = limit12<DIR>(F[t], ct[t * lpl], Uw[t], Uw[t + 1], Uw[t + 2], Uw[t + 3], Uw[t + 4],
+                F[t] = limit12<DIR>(F[t], CT(t), Uw[t], Uw[t + 1], Uw[t + 2], Uw[t + 3], Uw[t + 4],
                                     Uw[t + 5], Uw[t + 6], Uw[t + 7], W[t + 3], W[t + 4], W[t + 5],
                                     W[t + 6]);
         }
@@ -801,8 +815,8 @@ __device__ __forceinline__ void sweep_job(const SweepRun& s, int job)
 #pragma unroll
         for (int t = 0; t < T; t++) {
             const double fr = t + 1 < T ? F[t + 1] : fn;
-            const double cg = t + 1 < T ? ct[(t + 1) * lpl] : crn;
-            C[t] = W[GST + t] - (cg * fr - ct[t * lpl] * F[t]);
+            const double cg = t + 1 < T ? CT(t + 1) : crn;
+            C[t] = W[GST + t] - (cg * fr - CT(t) * F[t]);
         }
         __syncwarp();  // every lane has its window of UE
         if (act) {
@@ -828,6 +842,7 @@ __device__ __forceinline__ void sweep_job(const SweepRun& s, int job)
         }
     }
     __syncwarp();  // the warp's next job overwrites what phase D wrote last
+#undef CT
 }
 
 // One job: the body for the sweep's cells per lane and the job's directions
@@ -858,7 +873,10 @@ __device__ __forceinline__ void run_job(const SweepRun& s, int job)
 #undef VERB_JOB3
 }
 
-__global__ void __launch_bounds__(C3_THREADS, 2) convection_kernel(ConvArgs a)
+#ifndef VERB_CONV_MINB
+#define VERB_CONV_MINB 2
+#endif
+__global__ void __launch_bounds__(C3_THREADS, VERB_CONV_MINB) convection_kernel(ConvArgs a)
 {
     extern __shared__ double sm[];
     const Dims d = a.d;
@@ -888,8 +906,12 @@ __global__ void __launch_bounds__(C3_THREADS, 2) convection_kernel(ConvArgs a)
     size_t offR = 0;
     const size_t ntab = conv_table_doubles(P, R, &offR);
     double* crP = a.scratch + (size_t)blockIdx.x * conv_scratch_per_cta(P, R);  // [R-1][TP][lplP]
-    double* crR = crP + offR;                                                  // [P][TR][lplR]
     double* gpl = crP + ntab;  // G of the slice
+#ifdef VERB_CONV_CR_SMEM
+    crP = (double*)(dirR + P) + 1;  // after the int arrays, 8-byte aligned (+1 for odd P+R)
+    crP = (double*)(((size_t)crP + 7) & ~(size_t)7);
+#endif
+    double* crR = crP + offR;                                                  // [P][TR][lplR]
     double* lexp = gpl + PR;   // exp(Loss dt)
     double* spl = lexp + PR;   // Sources dt
     const int nslices = V * K;

@@ -100,6 +100,10 @@ struct verb_ctx {
     unsigned char* kpend = nullptr;
     unsigned int* kcount = nullptr;       // [0] pending systems, [1] given up
     unsigned long long* kmax = nullptr;   // [0] max relative residual key, [2..3] update maxima
+    // learned preconditioner of the Krylov form: the network, its features
+    // [sys][9][n] and coefficients [sys][25][n]
+    verb_cnn* kpc_net = nullptr;
+    float *kpfeat = nullptr, *kpc = nullptr;
     bool local_dirty = true;
     double local_dt = -1;
     int solve_variant = -1;  // local solve shape; -1: the process-wide tuned one, else 0

@@ -11,7 +11,8 @@ void free_krylov(verb_ctx* c)
     for (void** p : {(void**)&c->kA9, (void**)&c->kscr, (void**)&c->kfeat, (void**)&c->kout,
                      (void**)&c->kb, (void**)&c->kx, (void**)&c->kr, (void**)&c->kd,
                      (void**)&c->kscale, (void**)&c->kiters, (void**)&c->kpend,
-                     (void**)&c->kcount, (void**)&c->kmax, (void**)&c->kprev}) {
+                     (void**)&c->kcount, (void**)&c->kmax, (void**)&c->kprev,
+                     (void**)&c->kpfeat, (void**)&c->kpc}) {
         cudaFree(*p);
         *p = nullptr;
     }
@@ -74,6 +75,15 @@ int krylov_run(verb_ctx* c, double dt, double sub_dt, int guess, verb_cnn* cnn, 
     // they are rebuilt every call (one pass over the coefficient fields)
     launch_local_assemble32(a, c->kA9, c->stream);
     c->acc.kernel_launches++;
+    if (c->kpc_net) {
+        // the learned preconditioner's coefficients from the matrix
+        if (c->trim_k0) return VERB_ERR_ARG;
+        CK(alloc((void**)&c->kpfeat, nu * 9 * sizeof(float)));
+        CK(alloc((void**)&c->kpc, nu * 25 * sizeof(float)));
+        launch_precond_features(a, c->kA9, c->kpfeat, c->stream);
+        CK(cnn_forward_on(c->kpc_net, c->kpfeat, c->kpc, nsys, c->stream));
+        c->acc.kernel_launches += 1 + 4;
+    }
     verb_krylov_stats st{};
     double guess_max = 0, res_max = 0;
     for (int k = 0; k < nsub; k++) {
@@ -135,7 +145,8 @@ int krylov_run(verb_ctx* c, double dt, double sub_dt, int guess, verb_cnn* cnn, 
             ap.sel_mask = 1;
             launch_local_residual(ap, c->kb, c->kx, c->kr, c->stream);
             // the FP64 check decides convergence: no inner flag is kept
-            launch_bicgstab(ap, c->kA9, c->kr, c->kd, c->kscr, inner_maxit, (float)inner_tol,
+            launch_bicgstab(ap, c->kA9, c->kpc_net ? c->kpc : nullptr, c->kr, c->kd, c->kscr,
+                            inner_maxit, (float)inner_tol,
                             c->kiters, nullptr, c->stream);
             launch_local_update(ap, c->kx, c->kd, c->kmax + 2, c->stream);
             c->acc.kernel_launches += 3;
@@ -279,6 +290,58 @@ int verb_local_triples(verb_ctx* c, double dt, double sub_dt, float* feat_dev, f
 {
     if (!c || !(dt > 0) || !(sub_dt > 0) || !feat_dev || !target_dev) return VERB_ERR_ARG;
     return triples_run(c, dt, sub_dt, feat_dev, target_dev);
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int verb_set_krylov_preconditioner(verb_ctx* c, verb_cnn* net)
+{
+    if (!c) return VERB_ERR_ARG;
+    if (net) {
+        int ci, co, H, W, mb;
+        CK(cnn_shape(net, &ci, &co, &H, &W, &mb));
+        if (ci != 9 || co != 25 || H != c->d.K || W != c->d.V || mb < c->d.P * c->d.R)
+            return VERB_ERR_ARG;
+    }
+    c->kpc_net = net;
+    return VERB_OK;
+}
+
+int verb_local_precond_inputs(verb_ctx* c, double dt, double sub_dt, float* feat_dev, float* A9_dev)
+{
+    if (!c || !feat_dev || !A9_dev || !(dt > 0) || !(sub_dt > 0)) return VERB_ERR_ARG;
+    const Dims& d = c->d;
+    if (d.V < 3 || d.K < 3 || c->trim_k0) return VERB_ERR_ARG;
+    int nsub = (int)(dt / sub_dt);
+    if (nsub < 1) nsub = 1;
+    LocalArgs a{};
+    int s = local_prepare(c, a, dt / nsub);
+    if (s) return s;
+    launch_local_assemble32(a, A9_dev, c->stream);
+    launch_precond_features(a, A9_dev, feat_dev, c->stream);
+    c->acc.kernel_launches += 2;
+    CK(cudaStreamSynchronize(c->stream));
+    return check_launch();
+}
+
+int verb_precond_loss_grad(const float* A9, const float* C, const float* Z, int nsys, int V, int K,
+                           int nprobe, float* gC, float* loss_host, void* stream)
+{
+    if (!A9 || !C || !Z || !gC || nsys < 1 || V < 1 || K < 1 || nprobe < 1) return VERB_ERR_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    float* loss = nullptr;
+    CK(cudaMallocAsync((void**)&loss, sizeof(float), s));
+    int st = cuda_ok(cudaMemsetAsync(loss, 0, sizeof(float), s));
+    if (!st) st = launch_precond_grad(A9, C, Z, gC, loss, nsys, V, K, nprobe, s);
+    float h = 0.f;
+    if (!st) st = cuda_ok(cudaMemcpyAsync(&h, loss, sizeof(float), cudaMemcpyDeviceToHost, s));
+    cudaFreeAsync(loss, s);
+    if (!st) st = cuda_ok(cudaStreamSynchronize(s));
+    if (!st) st = check_launch();
+    if (loss_host) *loss_host = h;
+    return st;
 }
 
 }  // extern "C"

@@ -267,6 +267,9 @@ __global__ void __launch_bounds__(FACT_THREADS) local_factor_kernel(LocalArgs a)
                 }
             }
             if (tid == 0) {
+                // idamax: a NaN first element is the maximum (nothing compares
+                // greater), elsewhere NaN never is
+                if (colj[0] != colj[0]) bi = 0;
                 s_jp = bi;
                 s_piv = W[((j + bi) % RW) * CW + csj];
                 ip[j] = j + bi;
@@ -854,10 +857,132 @@ __device__ __forceinline__ float mv_row(const float* A, const float* y, int n, i
     return acc;
 }
 
-// One CTA per system.  Right preconditioning with M = diag(A) (Jacobi):
+// ---- learned preconditioner ----------------------------------------------
+// M v (i) = sum over the 5 x 5 neighbourhood o of i of
+//           (delta(o = 0) + C[o](i)) v(i + o) / diag(i + o)
+// on the system's (V, K') grid (no wrap-around at its edges): a sparse
+// approximate inverse whose 25 coefficients per unknown a CNN predicts from
+// the matrix (C = 0 is the Jacobi preconditioner).  C is [sys][25][n], slot
+// o = (dy + 2) * 5 + (dx + 2).
+constexpr int PC_TAPS = 25;
+
+__device__ __forceinline__ float precond_row(const float* C, const float* dg, const float* v, int n,
+                                             int nx, int ny, int i)
+{
+    const int iy = i / nx, ix = i - iy * nx;
+    float acc = 0.f;
+#pragma unroll
+    for (int dy = -2; dy <= 2; dy++) {
+        const int yy = iy + dy;
+        if (yy < 0 || yy >= ny) continue;
+#pragma unroll
+        for (int dx = -2; dx <= 2; dx++) {
+            const int xx = ix + dx;
+            if (xx < 0 || xx >= nx) continue;
+            const int o = (dy + 2) * 5 + (dx + 2);
+            const int j = yy * nx + xx;
+            const float c = C[(size_t)o * n + i] + (o == 12 ? 1.f : 0.f);
+            acc = fmaf(c, v[j] / dg[j], acc);
+        }
+    }
+    return acc;
+}
+
+// features of the learned preconditioner, [sys][9][K'][V]: log10(|diag| dt)
+// and the eight off-diagonal entries of each row over its diagonal
+__global__ void precond_features_kernel(LocalArgs a, const float* A9, float* feat)
+{
+    const int sys = blockIdx.y;
+    if (skip_system(a, sys)) return;
+    const int n = a.d.V * (a.d.K - sys_k0(a, sys));
+    const size_t u0 = sys_uoff(a, sys);
+    const float* A = A9 + u0 * 9;
+    float* f = feat + u0 * 9;
+    const float dt = (float)a.dt;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float d = A[(size_t)4 * n + i];
+        f[i] = log10f(fmaxf(fabsf(d) * dt, 1e-30f));
+        int c = 1;
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            if (k == 4) continue;
+            f[(size_t)c * n + i] = d != 0.f ? A[(size_t)k * n + i] / d : 0.f;
+            c++;
+        }
+    }
+}
+
+// Training signal of the learned preconditioner for nprobe probe vectors z
+// per system: y = M z, e = A y - z, loss += |e|^2 / cnt and
+// gC[o](i) = (2 / cnt) sum_z (A^T e)(i) z(i + o) / diag(i + o), the
+// gradient of the loss with respect to C.  One CTA per system; z, y and e
+// live in shared memory (3 n floats).
+__global__ void precond_grad_kernel(const float* A9, const float* C, const float* Z, float* gC,
+                                    float* loss, int nx, int ny, int nprobe, float inv_cnt)
+{
+    extern __shared__ float psm[];
+    __shared__ float red[32];
+    const int sys = blockIdx.x;
+    const int n = nx * ny;
+    const float* A = A9 + (size_t)sys * 9 * n;
+    const float* dg = A + (size_t)4 * n;
+    const float* Cs = C + (size_t)sys * PC_TAPS * n;
+    float* g = gC + (size_t)sys * PC_TAPS * n;
+    float* z = psm;
+    float* y = z + n;
+    float* e = y + n;
+    for (size_t i = threadIdx.x; i < (size_t)PC_TAPS * n; i += blockDim.x) g[i] = 0.f;
+    float lsum = 0.f;
+    for (int q = 0; q < nprobe; q++) {
+        const float* zq = Z + ((size_t)sys * nprobe + q) * n;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) z[i] = zq[i];
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = precond_row(Cs, dg, z, n, nx, ny, i);
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const float ei = mv_row(A, y, n, nx, i) - z[i];
+            e[i] = ei;
+            lsum = fmaf(ei, ei, lsum);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            // (A^T e)(i): rows r = i - off with A[k](r) multiplying x(r + off)
+            float gy = 0.f;
+#pragma unroll
+            for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+                for (int dx = -1; dx <= 1; dx++) {
+                    const int r = i - (dy * nx + dx);
+                    if (r < 0 || r >= n) continue;
+                    gy = fmaf(A[(size_t)((dy + 1) * 3 + (dx + 1)) * n + r], e[r], gy);
+                }
+            gy *= 2.f * inv_cnt;
+            const int iy = i / nx, ix = i - iy * nx;
+#pragma unroll
+            for (int dy = -2; dy <= 2; dy++) {
+                const int yy = iy + dy;
+                if (yy < 0 || yy >= ny) continue;
+#pragma unroll
+                for (int dx = -2; dx <= 2; dx++) {
+                    const int xx = ix + dx;
+                    if (xx < 0 || xx >= nx) continue;
+                    const int j = yy * nx + xx;
+                    g[(size_t)((dy + 2) * 5 + (dx + 2)) * n + i] += gy * (z[j] / dg[j]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    lsum = block_sum(lsum, red);
+    if (threadIdx.x == 0) atomicAdd(loss, lsum * inv_cnt);
+}
+
+// One CTA per system.  Right preconditioning with M = diag(A) (Jacobi), or
+// the learned sparse approximate inverse when Cp is given:
 // van der Vorst's BiCGSTAB on A M^-1 u = r, d = M^-1 u accumulated directly.
-__global__ void bicgstab_kernel(LocalArgs a, const float* A9, const double* rr, double* dd,
-                                float* scratch, int maxit, float tol, int* iters, unsigned char* ok)
+__global__ void bicgstab_kernel(LocalArgs a, const float* A9, const float* Cp, const double* rr,
+                                double* dd, float* scratch, int maxit, float tol, int* iters,
+                                unsigned char* ok)
 {
     __shared__ float red[32];
     const int sys = blockIdx.x;
@@ -875,6 +1000,8 @@ __global__ void bicgstab_kernel(LocalArgs a, const float* A9, const double* rr, 
     float* t = y + n;
     double* d = dd + u0;
     const double* b = rr + u0;
+    const float* Cs = Cp ? Cp + u0 * PC_TAPS : nullptr;
+    const int ny = n / nx;
     float bn = 0.f;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const float bi = (float)b[i];
@@ -898,9 +1025,13 @@ __global__ void bicgstab_kernel(LocalArgs a, const float* A9, const double* rr, 
         const float beta = (rho1 / rho) * (alpha / omega);
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
             p[i] = r[i] + beta * (p[i] - omega * v[i]);
-            y[i] = p[i] / dg[i];
+            if (!Cs) y[i] = p[i] / dg[i];
         }
         __syncthreads();
+        if (Cs) {
+            for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = precond_row(Cs, dg, p, n, nx, ny, i);
+            __syncthreads();
+        }
         float rv = 0.f;
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
             const float vi = mv_row(A, y, n, nx, i);
@@ -922,7 +1053,12 @@ __global__ void bicgstab_kernel(LocalArgs a, const float* A9, const double* rr, 
             conv = true;
             break;
         }
-        for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = r[i] / dg[i];  // z
+        if (Cs) {
+            __syncthreads();  // every s entry is written before M reads its neighbours
+            for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = precond_row(Cs, dg, r, n, nx, ny, i);
+        } else {
+            for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = r[i] / dg[i];  // z
+        }
         __syncthreads();
         float ts = 0.f, tt = 0.f;
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -1132,10 +1268,31 @@ void launch_local_assemble32(const LocalArgs& a, float* A9, cudaStream_t s)
     local_assemble32_kernel<<<dim3((n + 255) / 256, a.d.P * a.d.R), 256, 0, s>>>(a, A9);
 }
 
-void launch_bicgstab(const LocalArgs& a, const float* A9, const double* r, double* d, float* scratch,
-                     int maxit, float tol, int* iters, unsigned char* ok, cudaStream_t s)
+void launch_precond_features(const LocalArgs& a, const float* A9, float* feat, cudaStream_t s)
 {
-    bicgstab_kernel<<<a.d.P * a.d.R, 256, 0, s>>>(a, A9, r, d, scratch, maxit, tol, iters, ok);
+    const int n = a.d.V * a.d.K;
+    precond_features_kernel<<<dim3((n + 255) / 256, a.d.P * a.d.R), 256, 0, s>>>(a, A9, feat);
+}
+
+int launch_precond_grad(const float* A9, const float* C, const float* Z, float* gC, float* loss,
+                        int nsys, int nx, int ny, int nprobe, cudaStream_t s)
+{
+    const size_t smem = (size_t)3 * nx * ny * sizeof(float);
+    allow_max_dynamic_smem((const void*)precond_grad_kernel);
+    int dev = 0, maxsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (smem + 32 * sizeof(float) > (size_t)maxsm) return VERB_ERR_SIZE;
+    precond_grad_kernel<<<nsys, 256, smem, s>>>(A9, C, Z, gC, loss, nx, ny, nprobe,
+                                                1.f / ((float)nsys * nprobe * nx * ny));
+    return VERB_OK;
+}
+
+void launch_bicgstab(const LocalArgs& a, const float* A9, const float* Cp, const double* r, double* d,
+                     float* scratch, int maxit, float tol, int* iters, unsigned char* ok,
+                     cudaStream_t s)
+{
+    bicgstab_kernel<<<a.d.P * a.d.R, 256, 0, s>>>(a, A9, Cp, r, d, scratch, maxit, tol, iters, ok);
 }
 
 void launch_gather_state(const LocalArgs& a, double* x, cudaStream_t s)

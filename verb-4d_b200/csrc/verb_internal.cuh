@@ -168,8 +168,17 @@ void launch_local_assemble32(const LocalArgs& a, float* A9, cudaStream_t s);
 // selected system, d from 0; iters[sys] += iterations, ok[sys] = converged
 // (ok may be nullptr);
 // scratch: 6 vectors of n floats per system
-void launch_bicgstab(const LocalArgs& a, const float* A9, const double* r, double* d, float* scratch,
-                     int maxit, float tol, int* iters, unsigned char* ok, cudaStream_t s);
+// Cp: the learned preconditioner's coefficients [sys][25][n] (nullptr: Jacobi)
+void launch_bicgstab(const LocalArgs& a, const float* A9, const float* Cp, const double* r, double* d,
+                     float* scratch, int maxit, float tol, int* iters, unsigned char* ok,
+                     cudaStream_t s);
+// features of the learned preconditioner, [sys][9][K'][V] (log10 |diag| dt and
+// the off-diagonal entries over the diagonal)
+void launch_precond_features(const LocalArgs& a, const float* A9, float* feat, cudaStream_t s);
+// its training gradient for nprobe probes per system (systems of nx * ny
+// unknowns, contiguous): gC [sys][25][n], loss += |A M z - z|^2 / count
+int launch_precond_grad(const float* A9, const float* C, const float* Z, float* gC, float* loss,
+                        int nsys, int nx, int ny, int nprobe, cudaStream_t s);
 // the PSD of every system in the unknown order
 void launch_gather_state(const LocalArgs& a, double* x, cudaStream_t s);
 // features of the state f (unknown order) for the warm-start CNN:

@@ -89,6 +89,11 @@ SIGNATURES = {
     "verb_local_krylov": (C.c_int, [_vp, C.c_double, C.c_double, C.c_int, _vp, C.c_int,
                                     C.c_double, C.c_int, C.c_int, C.c_double, C.c_double, _vp]),
     "verb_local_triples": (C.c_int, [_vp, C.c_double, C.c_double, _vp, _vp]),
+    "verb_cnn_backward_step": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_float]),
+    "verb_set_krylov_preconditioner": (C.c_int, [_vp, _vp]),
+    "verb_local_precond_inputs": (C.c_int, [_vp, C.c_double, C.c_double, _vp, _vp]),
+    "verb_precond_loss_grad": (C.c_int, [_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp,
+                                         C.POINTER(C.c_float), _vp]),
     "verb_set_convection_arith": (C.c_int, [_vp, C.c_int]),
     "verb_set_step_graph": (C.c_int, [_vp, C.c_int]),
     "verb_local_solve_variants": (C.c_int, [C.POINTER(C.c_int)]),

@@ -99,6 +99,76 @@ def train(net, feat, targ, epochs: int = 20, batch: int = 256, lr: float = 1e-3,
     return hist
 
 
+PC_CHANNELS = (9, 32, 32, 32, 25)
+
+
+def precond_inputs(wl, seeds=None):
+    """Features [N][9][K][V] and FP32 diagonals [N][9][V*K] of the local
+    systems of `wl` (and of the same grid with the coefficients of every
+    seed in `seeds`), device tensors."""
+    import torch
+
+    from .solver import Solver
+
+    spec = wl.spec
+    nsys, n = spec.P * spec.R, spec.V * spec.K
+    wls = [wl] + [W.make_workload(spec, seed=sd, sources=True, losses=True) for sd in (seeds or [])]
+    feat = torch.empty((len(wls) * nsys, 9, spec.K, spec.V), dtype=torch.float32, device="cuda")
+    A9 = torch.empty((len(wls) * nsys, 9, n), dtype=torch.float32, device="cuda")
+    for i, w in enumerate(wls):
+        s = Solver(w)
+        s.load()
+        s.ctx.local_precond_inputs(w.dt, w.sub_dt, feat[i * nsys:].data_ptr(), A9[i * nsys:].data_ptr())
+        s.ctx.close()
+    return feat, A9
+
+
+def precond_loss_grad(A9, Cc, Z, V, K):
+    """mean |A M z - z|^2 over the probes Z [B][nprobe][V*K] and its gradient
+    with respect to the coefficients Cc [B][25][K][V] (device tensors)."""
+    import torch
+
+    g = torch.empty_like(Cc)
+    loss = C.c_float()
+    vp = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    L.check(L.load().verb_precond_loss_grad(vp(A9), vp(Cc), vp(Z), A9.shape[0], V, K, Z.shape[1],
+                                            vp(g), C.byref(loss), None), "precond loss")
+    return loss.value, g
+
+
+def train_preconditioner(net, feat, A9, V, K, epochs=30, batch=64, nprobe=4, lr=2e-3,
+                         lr_final=2e-4, seed=0):
+    """Adam on shuffled system batches with Gaussian probe vectors: the
+    network learns coefficients C that make A M close to the identity
+    (the loss is mean |A M z - z|^2 over the probes).  Returns the mean loss of
+    every epoch."""
+    import torch
+
+    n = feat.shape[0]
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    gcpu = torch.Generator(device="cpu").manual_seed(seed)
+    out = torch.empty((batch, 25, K, V), dtype=torch.float32, device="cuda")
+    nb = max(1, n // batch)
+    decay = (lr_final / lr) ** (1.0 / max(1, epochs * nb - 1))
+    rate = lr
+    hist = []
+    for _ in range(epochs):
+        perm = torch.randperm(n, generator=gcpu).to(feat.device)
+        tot = 0.0
+        for b in range(nb):
+            idx = perm[b * batch:(b + 1) * batch]
+            xb = feat.index_select(0, idx).contiguous()
+            ab = A9.index_select(0, idx).contiguous()
+            Z = torch.randn((len(idx), nprobe, V * K), generator=gen, device="cuda")
+            net.forward(xb.data_ptr(), out.data_ptr(), len(idx))
+            loss, g = precond_loss_grad(ab, out[:len(idx)], Z, V, K)
+            net.backward_step(xb.data_ptr(), g.data_ptr(), len(idx), rate)
+            tot += loss
+            rate *= decay
+        hist.append(tot / nb)
+    return hist
+
+
 class CNN:
     def __init__(self, H, W, max_batch, channels=CHANNELS, seed=0, stream=None):
         self.lib = L.load()
@@ -140,6 +210,18 @@ class CNN:
     def forward(self, x_dev, out_dev, batch):
         L.check(self.lib.verb_cnn_forward(self.h, C.c_void_p(x_dev), C.c_void_p(out_dev), batch),
                 "cnn_forward")
+
+    def zero_last_layer(self):
+        """Zero the last layer's weights and bias (the network then outputs 0:
+        for the preconditioner, exactly the Jacobi one)."""
+        p = self.params()
+        ci, co = self.channels[-2], self.channels[-1]
+        p[self.nparams - co - co * ci * 9:] = 0.0
+        self.set_params(p)
+
+    def backward_step(self, x_dev, g_dev, batch, lr):
+        L.check(self.lib.verb_cnn_backward_step(self.h, C.c_void_p(x_dev), C.c_void_p(g_dev), batch,
+                                                C.c_float(lr)), "cnn_backward")
 
     def train_step(self, x_dev, t_dev, batch, lr):
         loss = C.c_float()

@@ -148,6 +148,21 @@ class Context:
                 "local_krylov")
         return {k: getattr(st, k) for k, _ in L.KrylovStats._fields_}
 
+    def set_krylov_preconditioner(self, net=None) -> None:
+        """The learned sparse approximate inverse (a learned.CNN with 9 input
+        and 25 output channels) as the preconditioner of local_krylov; None:
+        Jacobi."""
+        L.check(self.lib.verb_set_krylov_preconditioner(self.h, net.h if net is not None else None),
+                "krylov preconditioner")
+        self._pc = net  # keep the network alive while the context uses it
+
+    def local_precond_inputs(self, dt: float, sub_dt: float, feat_ptr: int, A9_ptr: int) -> None:
+        """The learned preconditioner's features [sys][9][K][V] and the FP32
+        diagonals [sys][9][V*K] of every local system (device pointers)."""
+        L.check(self.lib.verb_local_precond_inputs(self.h, float(dt), float(sub_dt),
+                                                   C.c_void_p(feat_ptr), C.c_void_p(A9_ptr)),
+                "precond inputs")
+
     def local_triples(self, dt: float, sub_dt: float, feat_ptr: int, target_ptr: int) -> None:
         """A local LU step that writes the CNN features and targets of every
         system into the device buffers at feat_ptr ([P*R][4][K][V] float32)
