@@ -448,8 +448,8 @@ int verb_convection_2d(double* psd, const double* P, const double* R, int nP, in
  * caller's DEVICE memory, for callers that cannot allocate device memory (a
  * host application or plugin that owns every allocation, or a path where an
  * allocation is not allowed).  It calls no allocator: the kernel's scratch is
- * a fixed array in the library's device code of 7 doubles per point of
- * VERB_NOALLOC_MAX_POINTS points (448 KiB) plus a few status words, held on
+ * a fixed array in the library's device code of 5 doubles per point of
+ * VERB_NOALLOC_MAX_POINTS points (320 KiB) plus a few status words, held on
  * every device that loads that code until exit.  CUDA loads device code
  * lazily, so the first call on a device loads it (the array and the kernel
  * take their device memory then, and the device may synchronise) and looks

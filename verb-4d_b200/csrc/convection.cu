@@ -405,61 +405,43 @@ __device__ __forceinline__ double block_max(double v, double* red)
 // Slice kernel.
 //
 // A CTA of C3_WARPS warps owns one [P][R] slice at a time; the slice stays in
-// shared memory for all of its CFL sub-steps, in a plane X of (P + 2 GST) x RS
-// doubles with GST = 5 ghost rows above and below and GST ghost columns left
-// and right of the P x R interior (QUICKEST6.cpp:89-143 extends every 1-D line
-// by five ghost cells per side).  A sweep is a set of independent lines
-// (P-lines: one per L index, along MLT; R-lines: one per MLT index, along L).
-// A warp takes 32/lpl lines per job with lpl lanes per line, and lane j of a
-// line owns the T consecutive cells jT .. jT+T-1 of the line, and their left
-// faces, for the whole job: their values live in registers.  A sub-step of a
-// job:
-//   ghosts of E          from the line's boundary types, into the plane's
-//                        ghost slots of the line (lanes 0..9 of the line)
-//   A  window W = E[jT-5 .. jT+T+3] from the plane (T+9 shared loads); the
-//      lane's T unlimited face values from it (QUICKEST6.cpp:148-241)
-//   B  unlimited cells UE = E - (c F)_right + (c F)_left with the right
-//      neighbour's first face by a shuffle; written over E in the plane,
-//      then the boundary rewrite of cells 0 and n-1 and UE's high ghosts
-//      (the low ghosts stay E's, as the reference takes them from the
-//      pre-step PSD, :283-302)                              (:243-272, 277-330)
-//   C  window UE[jT-4 .. jT+T+2] from the plane; the limited face values from
-//      it and from E's window (registers)                   (:332-447)
-//   D  final cells into the plane and their boundary rewrite (:448-477)
-// with warp synchronisation only; the CTA synchronises between sweeps.  A
-// lane thus reads T+9 + T+7 and writes about 2T doubles of shared memory per
-// sub-step for its T faces, and the face arithmetic runs on registers.
+// shared memory (plane S) for all of its CFL sub-steps.  A sweep is a set of
+// independent lines (P-lines: fixed L, R-lines: fixed MLT).  A warp takes
+// 32/lpl lines per job with lpl lanes per line, and lane j of a line owns the
+// cells x = j + lpl*t, t < T = ceil(n/lpl): at every step of a phase the lanes
+// of a line touch consecutive shared-memory words.  A job copies its lines
+// into per-warp buffers extended by the GST = 5 ghost cells of
+// QUICKEST6.cpp:89-143, stages the lines' face Courant numbers next to them,
+// and runs the four phases of one ULTIMATE-QUICKEST sub-step with warp
+// synchronisation only:
+//   A  unlimited face values into F                    (QUICKEST6.cpp:148-241)
+//   B  unlimited cells + boundary rewrite into UE      (:243-272)
+//   C  limited face values into F                      (:277-447)
+//   D  final cells + rewrite; into S on the last sub-step (:448-477)
+// The Courant factors of the face polynomial are recomputed from the face
+// Courant number with exactly rounded divisions by the constant denominators
+// (div_const).  All faces of a job usually have
+// the same upwind direction (the drift velocities are smooth along MLT and the
+// radial velocity depends on MLT only), so a job is dispatched to a
+// direction-specialised body in which the upwind stencil roles are fixed
+// registers; jobs with mixed directions select the roles per face.
 //
-// The face Courant numbers of every line are computed once per slice into a
-// per-CTA table in global memory (L2-resident), laid out [line][t][lane] so
-// that the lanes of a warp load them with contiguous accesses.  The Courant
-// factors of the face polynomial are recomputed per face from the Courant
-// number with exactly rounded divisions by the constant denominators
-// (div_const).  All faces of a job usually have the same upwind direction
-// (the drift velocities are smooth along MLT and the radial velocity depends
-// on MLT only), so a job is dispatched to a direction-specialised body in
-// which the upwind stencil roles are fixed registers; jobs with mixed
-// directions select the roles per face.
-//
-// The radial sweep works on PSD*G: with G not identically 1 on the slice a
-// pass over the plane multiplies by G before it, and a pass /G, *exp(Loss dt),
-// +S dt (interior L) follows it, in the reference's order
-// (src/Convection_2D.cpp:122-165).  With G = 1 and exp(Loss dt) = 1 on the
-// whole slice those factors are exact identities, and the sources are added by
-// the R-sweep itself after its boundary rewrite.
+// The radial sweep works on PSD*G: a pass over the plane multiplies by G
+// before it, and the epilogue pass /G, *exp(Loss dt), +S dt (interior L)
+// follows it, in the reference's order (src/Convection_2D.cpp:122-165).  The
+// per-slice planes G, exp(Loss dt), S dt and the face Courant tables live in a
+// per-CTA scratch region that stays resident in L2.
 
 // Warps per CTA (two CTAs per SM).  The contracted build needs fewer
-// registers, so nine warps per CTA fit beside the exact build's eight in the
-// same register file.  Nine warps split the 25 MLT-sweep jobs and the 24
-// L-sweep jobs of a 48 x 101 slice into three rounds each.
-#if defined(VERB_CONV_WARPS)
-constexpr int C3_WARPS = VERB_CONV_WARPS;
+// registers (113 fit), so nine warps per CTA fit beside the exact build's
+// eight in the same shared memory and register file.
+#ifdef VERB_BUILD_CONV_FMA
+constexpr int C3_WARPS = 9;
 #else
 constexpr int C3_WARPS = 8;
 #endif
 constexpr int C3_THREADS = C3_WARPS * 32;
-constexpr int GST = 5;  // ghost cells per side
-constexpr unsigned FULL = 0xffffffffu;
+constexpr int TMAX = 16;  // cells per lane: lines of up to 32*TMAX points
 
 // a / b rounded to nearest, for the constants b = 6, 120, 5040 and 362880 with
 // y = RN(1/b) (Markstein's correction step: P. Markstein, IBM J. Res. Dev.
@@ -519,21 +501,21 @@ __device__ __forceinline__ FaceCoef face_coef_exact(double cr)
 
 enum { DIR_POS = 0, DIR_NEG = 1, DIR_MIX = 2 };
 
-// Face value of face x from w_k = E[x-5+k].  Courant >= 0: upwind centre
+// Face value of face x from w[k] = E[x-5+k].  Courant >= 0: upwind centre
 // x-1, U_k = E[x-1-k], D_k = E[x-1+k]; Courant < 0: centre x, U_k = E[x+k],
 // D_k = E[x-k] (QUICKEST6.cpp:169-186).
 template <int DIR>
-__device__ __forceinline__ double face10(double w0, double w1, double w2, double w3, double w4,
-                                         double w5, double w6, double w7, double w8, double w9,
-                                         double cr)
+__device__ __forceinline__ double face3(const double (&w)[10], double cr)
 {
     const FaceCoef k = face_coef_exact(cr);
-    if (DIR == DIR_POS) return QUICKEST_FACE(w3, w2, w1, w0, w4, w5, w6, w7, w8, w9, cr, k);
-    if (DIR == DIR_NEG) return QUICKEST_FACE(w6, w7, w8, w9, w5, w4, w3, w2, w1, w0, cr, k);
+    if (DIR == DIR_POS)
+        return QUICKEST_FACE(w[3], w[2], w[1], w[0], w[4], w[5], w[6], w[7], w[8], w[9], cr, k);
+    if (DIR == DIR_NEG)
+        return QUICKEST_FACE(w[6], w[7], w[8], w[9], w[5], w[4], w[3], w[2], w[1], w[0], cr, k);
     const bool up = cr >= 0;
-    return QUICKEST_FACE(up ? w3 : w6, up ? w2 : w7, up ? w1 : w8, up ? w0 : w9, up ? w4 : w5,
-                         up ? w5 : w4, up ? w6 : w3, up ? w7 : w2, up ? w8 : w1, up ? w9 : w0, cr,
-                         k);
+    return QUICKEST_FACE(up ? w[3] : w[6], up ? w[2] : w[7], up ? w[1] : w[8], up ? w[0] : w[9],
+                           up ? w[4] : w[5], up ? w[5] : w[4], up ? w[6] : w[3], up ? w[7] : w[2],
+                           up ? w[8] : w[1], up ? w[9] : w[0], cr, k);
 }
 
 // quickest_limit with the branches turned into selects: the same comparisons
@@ -570,392 +552,380 @@ __device__ __forceinline__ double quickest_limit_sel(double f, double cr, double
     return res;
 }
 
-// Limited face value of face x from u_k = UE[x-4+k] (k = 0..7) and
-// e_k = E[x-2+k] (k = 0..3).
+// Limited face value of face x from u[k] = UE[x-4+k] and ev[k] = E[x-2+k].
 template <int DIR>
-__device__ __forceinline__ double limit12(double f, double cr, double u0, double u1, double u2,
-                                          double u3, double u4, double u5, double u6, double u7,
-                                          double e0, double e1, double e2, double e3)
+__device__ __forceinline__ double limit3(double f, double cr, const double (&u)[8],
+                                         const double (&ev)[4])
 {
-    if (DIR == DIR_POS) return quickest_limit_sel(f, cr, e0, e1, e2, u2, u1, u0, u3, u4, u5, u6);
-    if (DIR == DIR_NEG) return quickest_limit_sel(f, cr, e3, e2, e1, u5, u6, u7, u4, u3, u2, u1);
+    if (DIR == DIR_POS)
+        return quickest_limit_sel(f, cr, ev[0], ev[1], ev[2], u[2], u[1], u[0], u[3], u[4], u[5], u[6]);
+    if (DIR == DIR_NEG)
+        return quickest_limit_sel(f, cr, ev[3], ev[2], ev[1], u[5], u[6], u[7], u[4], u[3], u[2], u[1]);
     const bool up = cr >= 0;
-    return quickest_limit_sel(f, cr, up ? e0 : e3, up ? e1 : e2, up ? e2 : e1, up ? u2 : u5,
-                              up ? u1 : u6, up ? u0 : u7, up ? u3 : u4, up ? u4 : u3,
-                              up ? u5 : u2, up ? u6 : u1);
+    return quickest_limit_sel(f, cr, up ? ev[0] : ev[3], up ? ev[1] : ev[2], up ? ev[2] : ev[1],
+                              up ? u[2] : u[5], up ? u[1] : u[6], up ? u[0] : u[7],
+                              up ? u[3] : u[4], up ? u[4] : u[3], up ? u[5] : u[2],
+                              up ? u[6] : u[1]);
 }
 
-// Cells per lane the kernel is compiled for; a sweep's shape uses the
-// smallest of them that covers its lines.  Up to 8 with every direction
-// body, 10, 12 and 16 (lines of up to 512 points) with the mixed-direction
-// body only.
-__host__ __device__ inline int t_allowed(int t)
+// 8-byte asynchronous global->shared copy (cp.async, sm_80+).
+__device__ __forceinline__ void cp_async8(double* dst, const double* src)
 {
-    if (t <= 3) return 3;
-    if (t <= 8) return t;
-    if (t <= 10) return 10;
-    if (t <= 12) return 12;
-    if (t <= 16) return 16;
-    return 0;
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
 }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Work split of one sweep: nlines lines of n points, lpl lanes per line, T
 // cells per lane.  The choice models a job's cost as a fixed part (line
-// set-up, ghost cells, loads of the windows, synchronisation) plus a part per
-// cell, and counts half of the idle warp slots of the last round (the other
-// CTA on the SM fills the rest).
+// set-up, boundary cells, ghost cells, barriers: about 400 warp instructions)
+// plus about 330 per cell step, and counts half of the idle warp slots of the
+// last round (the other CTA on the SM fills the rest).
 struct SweepCfg {
-    int lpl, T, nlw, njobs;
+    int lpl, T, nlw, njobs, nb;  // nb: doubles per line buffer (E, UE, F and CR each)
 };
 
 __host__ __device__ inline SweepCfg sweep_cfg(int n, int nlines)
 {
-    SweepCfg best{0, 0, 0, 0};
+    SweepCfg best{0, 0, 0, 0, 0};
     double bc = 0.0;
-    // shapes with at most 8 cells per lane (every direction body) first; ties
-    // go to fewer lanes per line (less padding)
-    for (int pass = 0; pass < 2 && best.lpl == 0; pass++) {
-        for (int lpl = 4; lpl <= 32; lpl <<= 1) {
-            const int T = t_allowed((n + lpl - 1) / lpl);
-            if (T == 0 || (T > 8) != (pass == 1)) continue;
-            const int nlw = 32 / lpl;
-            const int jobs = (nlines + nlw - 1) / nlw;
-            const int rounds = (jobs + C3_WARPS - 1) / C3_WARPS;
-            const double job = 300.0 + 200.0 * T;
-            const double cost = job * (jobs + 0.5 * (rounds * C3_WARPS - jobs));
-            if (best.lpl == 0 || cost < bc - 1e-9) {
-                bc = cost;
-                best = SweepCfg{lpl, T, nlw, jobs};
-            }
+    for (int lpl = 32; lpl >= 8; lpl >>= 1) {
+        const int T = (n + lpl - 1) / lpl;
+        if (T > TMAX) continue;
+        const int nlw = 32 / lpl;
+        const int jobs = (nlines + nlw - 1) / nlw;
+        const int rounds = (jobs + C3_WARPS - 1) / C3_WARPS;
+        const double job = 400.0 + 330.0 * T;
+        const double cost = job * (jobs + 0.5 * (rounds * C3_WARPS - jobs));
+        if (best.lpl == 0 || cost < bc - 1e-9) {
+            bc = cost;
+            best = SweepCfg{lpl, T, nlw, jobs, lpl * T + 10};
         }
     }
-    return best;  // lpl == 0: lines longer than 32*16 points
+    return best;  // lpl == 0: lines longer than 32*TMAX points
 }
 
-// row stride of the plane: R + 2 GST, odd, so that the MLT sweep's strided
-// accesses (stride T*RS between lanes) fall on distinct banks
-__host__ __device__ inline int plane_stride(int R)
+// per-warp buffer size in doubles (both sweeps share it)
+__host__ __device__ inline int conv_wstride(int P, int R)
 {
-    const int rs = R + 2 * GST;
-    return rs | 1;
-}
-
-__host__ __device__ inline int plane_doubles(int P, int R) { return (P + 2 * GST) * plane_stride(R); }
-
-// offset (doubles) of the per-line arrays after the plane
-__host__ __device__ inline size_t conv_table_doubles(int P, int R, size_t* off_r);
-
-__host__ __device__ inline int conv_smem_doubles(int P, int R)
-{
-    const int base = plane_doubles(P, R) + 4 * R + 4 * P + 32 + (R + P) + 2;
-#ifdef VERB_CONV_CR_SMEM
-    return base + (int)conv_table_doubles(P, R, nullptr);  // Courant tables in shared memory
-#else
-    return base;
-#endif
-}
-
-// per-CTA scratch: the Courant tables of both sweeps ([line][T][lpl]) and
-// the G, exp(Loss dt) and Sources dt planes
-__host__ __device__ inline size_t conv_table_doubles(int P, int R, size_t* off_r)
-{
-    size_t tp = 0, tr = 0;
+    int w = 0;
     if (P >= 3) {
         const SweepCfg c = sweep_cfg(P, R - 1);
-        tp = (size_t)(R > 1 ? R - 1 : 1) * c.T * c.lpl;
+        w = c.nlw * 4 * c.nb;
     }
     if (R >= 3) {
         const SweepCfg c = sweep_cfg(R, P);
-        tr = (size_t)P * c.T * c.lpl;
+        if (c.nlw * 4 * c.nb > w) w = c.nlw * 4 * c.nb;
     }
-    if (off_r) *off_r = tp;
-    return tp + tr;
+    return (w + 1) & ~1;  // keep every warp's buffer 16-byte aligned
+}
+
+// One job's lines as seen by one lane.
+struct LineJob {
+    double *E, *UE, *F, *CR;  // the lane's line buffers; E/UE slot x+5 holds cell x,
+                              // F and CR slot x hold face x and its Courant number
+    int n, lpl, T, j;         // line length, lanes per line, cells per lane, lane in line
+    int li;                   // line index (P-sweep: iR, R-sweep: iP)
+    int lt, ut;               // boundary types
+    int ns, nsmax;            // the line's sub-steps; the maximum over the warp
+    int R;                    // row length of the plane S
+    bool lv;                  // the lane's line exists
+    double lbc, ubc, dxl, dxu;
+};
+
+// Flux update of cell k, E[k] - (cr[k+1]*F[k+1] - cr[k]*F[k]) (:245-249,
+// 448-452).  A non-periodic line's cell 0 is always rewritten, so its left
+// flux (zero in the reference) is never used.
+__device__ __forceinline__ double cell_raw3(const LineJob& J, int k)
+{
+    return J.E[k + 5] - (J.CR[k + 1] * J.F[k + 1] - J.CR[k] * J.F[k]);
+}
+
+// End cell of a line after the boundary rewrite (:257-272 / 457-477): lane 0
+// of a line computes cell 0 and lane 1 cell n-1, with the same code; cells
+// 1..n-2 keep their flux update.
+__device__ __forceinline__ double edge_cell3(const LineJob& J)
+{
+    const bool hi = J.j == 1;
+    const int type = hi ? J.ut : J.lt;
+    const int k = type == VERB_BC_CONSTANT_DERIVATIVE ? (hi ? J.n - 2 : 1) : 0;
+    const double raw = cell_raw3(J, k);
+    return type == VERB_BC_CONSTANT_VALUE ? (hi ? J.ubc : J.lbc) : raw;
+}
+
+__device__ __forceinline__ void store_plane(double* S, const LineJob& J, bool RS, int x, double v)
+{
+    if (RS) S[J.li * J.R + x] = v;
+    else S[x * J.R + J.li] = v;
+}
+
+// Ghost cells of the extended line X from its interior (QUICKEST6.cpp:94-140
+// for E; :281-326 for UE).  Ghost gi < 5 is low ghost gi+1, gi >= 5 high
+// ghost gi-4; the lanes of a line take the ten of them in turn, with the same
+// code at both ends.  With low unset only the high ghosts are filled (UE's low
+// ghosts are copies of E's); constant-value ghosts are written only when cv is
+// set (they do not change within a job).
+__device__ __forceinline__ void fill_ghosts3(double* X, const LineJob& J, bool low, bool cv)
+{
+    const int n = J.n;
+    for (int gi = J.j; gi < 10; gi += J.lpl) {
+        if (!low && gi < 5) continue;
+        const bool hi = gi >= 5;
+        const int ig = hi ? gi - 4 : gi + 1;
+        const int type = hi ? J.ut : J.lt;
+        double g;
+        if (type == VERB_BC_PERIODIC) {
+            g = X[hi ? 5 + ig : 5 + (n - 1) - ig];
+        } else if (type == VERB_BC_CONSTANT_VALUE) {
+            if (!cv) continue;
+            g = hi ? J.ubc : J.lbc;
+        } else {
+            const double c = hi ? J.ubc * J.dxu : J.lbc * J.dxl;
+            g = hi ? X[5 + n - 1] + c : X[5] - c;
+            for (int i = 2; i <= ig; i++) g = hi ? g + c : g - c;
+        }
+        X[hi ? 5 + (n - 1) + ig : 5 - ig] = g;
+    }
+}
+
+// All sub-steps of one job (QUICKEST6.cpp:37-52 sub-cycle, one pass per
+// sub-step).  The loops over a lane's cells stay rolled (one copy of the face
+// code per phase keeps the kernel small enough for the instruction caches);
+// the per-cell state between phases lives in the line buffers.  Cell loops
+// cover cells 0..n-2 (lane 0 rewrites cell 0); lane 1 of a line writes cell
+// n-1 with its boundary rewrite; lanes 0-9 then fill the ghost cells.
+template <bool RS, int DIR>
+__device__ __forceinline__ void job_substeps(double* S, const LineJob& J)
+{
+    const int L = J.lpl;
+    const bool edge = J.lv && J.j < 2;      // lanes 0 and 1: cells 0 and n-1
+    const int ecell = J.j == 1 ? J.n - 1 : 0;
+    const int nc = J.lv ? J.n - 1 : 0;
+    // the lane's first cell in every buffer; loops advance them by L cells
+    const double* const E0 = J.E + J.j;
+    double* const UE0 = J.UE + J.j;
+    double* const F0 = J.F + J.j;
+    const double* const CR0 = J.CR + J.j;
+    double* const SP0 = RS ? S + J.li * J.R + J.j : S + J.j * J.R + J.li;
+    const int sstep = RS ? L : L * J.R;
+    for (int sub = 0; sub < J.nsmax; sub++) {
+        // A: unlimited faces
+        {
+            const double* e = E0;
+            const double* c = CR0;
+            double* f = F0;
+#pragma unroll 1
+            for (int t = 0; t < J.T; t++, e += L, c += L, f += L) {
+                double w[10];
+#pragma unroll
+                for (int k = 0; k < 10; k++) w[k] = e[k];
+                *f = face3<DIR>(w, *c);
+            }
+        }
+        __syncwarp();
+        // B: unlimited cells into UE
+        {
+            const double* e = E0;
+            const double* c = CR0;
+            const double* f = F0;
+            double* u = UE0;
+#pragma unroll 2
+            for (int x = J.j; x < nc; x += L, e += L, c += L, f += L, u += L)
+                u[5] = e[5] - (c[1] * f[1] - c[0] * f[0]);
+        }
+        if (edge) J.UE[ecell + 5] = edge_cell3(J);
+        __syncwarp();
+        if (J.lv) {
+            if (J.j < 5) J.UE[J.j] = J.E[J.j];  // low ghosts: the pre-step ones of E
+            fill_ghosts3(J.UE, J, false, false);
+        }
+        __syncwarp();
+        // C: limited faces, in place (each lane reads only its own faces)
+        {
+            const double* e = E0;
+            const double* c = CR0;
+            double* f = F0;
+            const double* u = UE0;
+#pragma unroll 1
+            for (int t = 0; t < J.T; t++, e += L, c += L, f += L, u += L) {
+                double uu[8], ev[4];
+#pragma unroll
+                for (int k = 0; k < 8; k++) uu[k] = u[1 + k];
+#pragma unroll
+                for (int k = 0; k < 4; k++) ev[k] = e[3 + k];
+                *f = limit3<DIR>(*f, *c, uu, ev);
+            }
+        }
+        __syncwarp();
+        // D: final cells.  On a line's last sub-step they go to the plane;
+        // otherwise they are staged in UE (free after phase C) and copied into
+        // E once every lane is done reading E.
+        const bool last = sub == J.ns - 1;
+        {
+            const double* e = E0;
+            const double* c = CR0;
+            const double* f = F0;
+            double* u = UE0;
+            double* sp = SP0;
+#pragma unroll 2
+            for (int x = J.j; x < nc; x += L, e += L, c += L, f += L, u += L, sp += sstep) {
+                const double v = e[5] - (c[1] * f[1] - c[0] * f[0]);
+                if (last) *sp = v;
+                else u[5] = v;
+            }
+        }
+        if (edge) {
+            const double v = edge_cell3(J);
+            if (last) store_plane(S, J, RS, ecell, v);
+            else J.UE[ecell + 5] = v;
+        }
+        if (sub + 1 < J.nsmax) {
+            __syncwarp();
+            {
+                const double* u = UE0;
+                double* e = J.E + J.j;
+                const int ncf = J.lv ? J.n : 0;
+#pragma unroll 2
+                for (int x = J.j; x < ncf; x += L, u += L, e += L) e[5] = u[5];
+            }
+            __syncwarp();
+            if (J.lv) fill_ghosts3(J.E, J, true, false);
+            __syncwarp();
+        }
+    }
+    __syncwarp();  // the warp's next job overwrites the buffers read in phase D
+}
+
+struct LineArrays {
+    const double *lb, *ub, *dxl, *dxu;
+    const int *ns, *dir;
+};
+
+// One job of a sweep: load the lines into the warp's buffers, pick the
+// direction-specialised body, run the line sub-steps.
+template <bool RS>
+__device__ __forceinline__ void sweep_job(double* S, double* wb, const SweepCfg& c, int job, int n,
+                                          int nlines, int R, int lt, int ut, const double* crtab,
+                                          const LineArrays& la)
+{
+    const int lane = threadIdx.x & 31;
+    const int q = lane / c.lpl;
+    LineJob J;
+    J.n = n;
+    J.lpl = c.lpl;
+    J.T = c.T;
+    J.j = lane - q * c.lpl;
+    J.li = job * c.nlw + q;
+    J.lv = J.li < nlines;
+    J.lt = lt;
+    J.ut = ut;
+    J.R = R;
+    J.E = wb + (size_t)q * 4 * c.nb;
+    J.UE = J.E + c.nb;
+    J.F = J.UE + c.nb;
+    J.CR = J.F + c.nb;
+    const int L = c.lpl;
+    // the lines' face Courant numbers: asynchronous copies from the per-CTA
+    // table (L2), in flight while the lines are copied out of the plane
+    {
+        const double* src = crtab + (size_t)J.li * n + J.j;
+        double* dst = J.CR + J.j;
+        const int nv = J.lv ? n : 0;
+        int x = J.j;
+        for (; x < nv; x += L, src += L, dst += L) cp_async8(dst, src);
+        for (; x <= L * c.T; x += L, dst += L) *dst = 0.0;
+        cp_async_commit();
+    }
+    J.lbc = J.lv ? la.lb[J.li] : 0.0;
+    J.ubc = J.lv ? la.ub[J.li] : 0.0;
+    J.dxl = J.lv ? la.dxl[J.li] : 0.0;
+    J.dxu = J.lv ? la.dxu[J.li] : 0.0;
+    J.ns = J.lv ? la.ns[J.li] : 0;
+    J.nsmax = __reduce_max_sync(0xffffffffu, J.ns);
+    const unsigned dir = __reduce_or_sync(0xffffffffu, J.lv ? (unsigned)la.dir[J.li] : 0u);
+    // E (QUICKEST6.cpp:89-91), then its ghost cells
+    {
+        const double* sp = RS ? S + J.li * R + J.j : S + J.j * R + J.li;
+        const int sstep = RS ? L : L * R;
+        double* e = J.E + 5 + J.j;
+        const int nv = J.lv ? n : 0;
+#pragma unroll 2
+        for (int x = J.j; x < nv; x += L, sp += sstep, e += L) *e = *sp;
+    }
+    __syncwarp();
+    if (J.lv) {
+        fill_ghosts3(J.E, J, true, true);
+        if (ut == VERB_BC_CONSTANT_VALUE)
+            for (int gi = J.j; gi < 10; gi += L)
+                if (gi >= 5) J.UE[n + gi] = J.ubc;
+    }
+    cp_async_wait_all();
+    __syncwarp();
+    if (dir == 2u) job_substeps<RS, DIR_NEG>(S, J);
+    else if (dir == 3u) job_substeps<RS, DIR_MIX>(S, J);
+    else job_substeps<RS, DIR_POS>(S, J);
+}
+
+// offset (doubles) of the warp buffers in the dynamic shared memory: plane,
+// per-line arrays, reduction slots and the int sub-step counts, rounded up to
+// 16 bytes
+__host__ __device__ inline int conv_wall_offset(int P, int R)
+{
+    const int o = P * R + 4 * R + 4 * P + 32 + (R + P);
+    return (o + 1) & ~1;
 }
 
 __host__ __device__ inline size_t conv_scratch_per_cta(int P, int R)
 {
-    return conv_table_doubles(P, R, nullptr) + 3 * (size_t)P * R;
+    return (size_t)(R > 1 ? R - 1 : 1) * P + 4 * (size_t)P * R;
 }
 
-// One sweep as the jobs of a warp see it.
-struct SweepRun {
-    double* X;                  // the plane
-    int RS;                     // its row stride
-    bool rsw;                   // R-sweep (lines are rows) or MLT sweep (lines are columns)
-    int n, nlines, lt, ut, lpl, T;
-    const double* crtab;        // [line][T][lpl] face Courant numbers
-    const double *lb, *ub, *dxl, *dxu;  // per line
-    const int *ns, *dir;
-    // R-sweep with G = 1 and exp(Loss dt) = 1: Sources*dt of interior cells
-    // added after the line's last sub-step ([P][R], or +0 everywhere)
-    bool fuse_src;
-    const double* spl;
-    bool spl_zero;
-    int R;
-};
-
-// All sub-steps of one job (QUICKEST6.cpp:37-52 sub-cycle, one pass per
-// sub-step), with T cells per lane and the stencil roles of direction DIR.
-template <int T, int DIR>
-__device__ __forceinline__ void sweep_job(const SweepRun& s, int job)
-{
-    const int lane = threadIdx.x & 31;
-    const int lpl = s.lpl;
-    const int q = lane / lpl;
-    const int j = lane - q * lpl;
-    const int n = s.n;
-    int li = job * (32 / lpl) + q;
-    const bool lv = li < s.nlines;
-    if (!lv) li = s.nlines - 1;  // a line to read from; nothing is written
-    const int xs = s.rsw ? 1 : s.RS;
-    double* const X0 = s.X + (s.rsw ? (li + GST) * s.RS + GST : GST * s.RS + li + GST);
-    const int c0 = j * T;
-    const int xmax = n - 1 + GST;  // last ghost slot
-    const int lt = s.lt, ut = s.ut;
-    const double lbc = s.lb[li], ubc = s.ub[li], dxl = s.dxl[li], dxu = s.dxu[li];
-    const int ns = lv ? s.ns[li] : 0;
-    const int nsmax = __reduce_max_sync(FULL, ns);
-    const int jl = (n - 1) / T;  // the lane that owns cell n-1
-
-    // Courant numbers of the lane's faces and of the right neighbour's first
-    // face
-    const double* const ct0 = s.crtab + (size_t)li * T * lpl + j;
-#ifdef VERB_CONV_CR_REG
-    double crr[T];
-#pragma unroll
-    for (int t = 0; t < T; t++) crr[t] = ct0[t * lpl];
-#define CT(t) crr[t]
-#else
-#define CT(t) ct0[(t) * lpl]
-#endif
-    const double crn = __shfl_down_sync(FULL, CT(0), 1, lpl);
-
-    // ghost cells of E (QUICKEST6.cpp:94-140): ghost gi < 5 is low ghost
-    // gi+1, gi >= 5 high ghost gi-4; the lanes of a line take the ten in turn
-    auto fill_ghosts = [&](bool low) {
-        for (int gi = j; gi < 2 * GST; gi += lpl) {
-            const bool hi = gi >= GST;
-            if (!low && !hi) continue;
-            const int ig = hi ? gi - GST + 1 : gi + 1;
-            const int type = hi ? ut : lt;
-            double g;
-            if (type == VERB_BC_PERIODIC) {
-                g = X0[(hi ? ig : (n - 1) - ig) * xs];
-            } else if (type == VERB_BC_CONSTANT_VALUE) {
-                g = hi ? ubc : lbc;
-            } else {
-                const double c = hi ? ubc * dxu : lbc * dxl;
-                g = hi ? X0[(n - 1) * xs] + c : X0[0] - c;
-                for (int i = 2; i <= ig; i++) g = hi ? g + c : g - c;
-            }
-            X0[(hi ? (n - 1) + ig : -ig) * xs] = g;
-        }
-    };
-    // boundary rewrite of cells 0 and n-1 (:257-272 / 457-477)
-    auto edge_fix = [&]() {
-        if (j == 0 && lt != VERB_BC_PERIODIC)
-            X0[0] = lt == VERB_BC_CONSTANT_VALUE ? lbc : X0[xs];
-        if (j == jl) {
-            double v;
-            if (ut == VERB_BC_CONSTANT_VALUE) v = ubc;
-            else if (ut == VERB_BC_CONSTANT_DERIVATIVE) v = X0[(n - 2) * xs];
-            else v = X0[0];  // periodic: f[n-1] = f[0]
-            X0[(n - 1) * xs] = v;
-        }
-    };
-
-    if (lv) fill_ghosts(true);
-    for (int sub = 0; sub < nsmax; sub++) {
-        const bool act = lv && sub < ns;
-        __syncwarp();
-        // A: the window of E and the unlimited faces
-        double W[T + 9];
-#pragma unroll
-        for (int i = 0; i < T + 9; i++) W[i] = X0[min(c0 - GST + i, xmax) * xs];
-        double F[T];
-#pragma unroll
-        for (int t = 0; t < T; t++)
-            F[t] = face10<DIR>(W[t], W[t + 1], W[t + 2], W[t + 3], W[t + 4], W[t + 5], W[t + 6],
-                               W[t + 7], W[t + 8], W[t + 9], CT(t));
-        // B: unlimited cells (:245-249); cell 0 of a non-periodic line is
-        // rewritten below, so its left flux (zero in the reference) is unused
-        double fn = __shfl_down_sync(FULL, F[0], 1, lpl);
-        double C[T];
-#pragma unroll
-        for (int t = 0; t < T; t++) {
-            const double fr = t + 1 < T ? F[t + 1] : fn;
-            const double cg = t + 1 < T ? CT(t + 1) : crn;
-            C[t] = W[GST + t] - (cg * fr - CT(t) * F[t]);
-        }
-        __syncwarp();  // every lane has its window of E
-        if (act) {
-#pragma unroll
-            for (int t = 0; t < T; t++)
-                if (c0 + t <= n - 2) X0[(c0 + t) * xs] = C[t];
-        }
-        __syncwarp();
-        if (act) edge_fix();
-        __syncwarp();
-        // UE's high ghosts from UE; its low ghosts stay E's (:283-326)
-        if (act && ut != VERB_BC_CONSTANT_VALUE) fill_ghosts(false);
-        __syncwarp();
-        // C: the window of UE and the limited faces
-        {
-            double Uw[T + 7];
-#pragma unroll
-            for (int i = 0; i < T + 7; i++) Uw[i] = X0[min(c0 - 4 + i, xmax) * xs];
-#pragma unroll
-            for (int t = 0; t < T; t++)
-                F[t] = limit12<DIR>(F[t], CT(t), Uw[t], Uw[t + 1], Uw[t + 2], Uw[t + 3], Uw[t + 4],
-                                    Uw[t + 5], Uw[t + 6], Uw[t + 7], W[t + 3], W[t + 4], W[t + 5],
-                                    W[t + 6]);
-        }
-        // D: final cells (:448-452)
-        fn = __shfl_down_sync(FULL, F[0], 1, lpl);
-#pragma unroll
-        for (int t = 0; t < T; t++) {
-            const double fr = t + 1 < T ? F[t + 1] : fn;
-            const double cg = t + 1 < T ? CT(t + 1) : crn;
-            C[t] = W[GST + t] - (cg * fr - CT(t) * F[t]);
-        }
-        __syncwarp();  // every lane has its window of UE
-        if (act) {
-#pragma unroll
-            for (int t = 0; t < T; t++)
-                if (c0 + t <= n - 2) X0[(c0 + t) * xs] = C[t];
-        }
-        __syncwarp();
-        if (act) edge_fix();
-        __syncwarp();
-        if (act && sub + 1 < ns) {
-            fill_ghosts(true);  // the next sub-step's ghosts of E
-        } else if (act && s.fuse_src) {
-            // the line's last sub-step: + Sources*dt on interior cells
-            // (src/Convection_2D.cpp:156-165; /G and *exp(Loss dt) are
-            // identities here).  Cells 1..n-2 still hold C.
-            const double* sp = s.spl + (size_t)li * s.R;
-#pragma unroll
-            for (int t = 0; t < T; t++) {
-                const int c = c0 + t;
-                if (c >= 1 && c <= n - 2) X0[c * xs] = C[t] + (s.spl_zero ? 0.0 : sp[c]);
-            }
-        }
-    }
-    __syncwarp();  // the warp's next job overwrites what phase D wrote last
-#undef CT
-}
-
-// One job: the body for the sweep's cells per lane and the job's directions
-// (bit 0: some face Courant number >= 0, bit 1: some < 0).
-__device__ __forceinline__ void run_job(const SweepRun& s, int job)
-{
-    const int lane = threadIdx.x & 31;
-    const int li = job * (32 / s.lpl) + lane / s.lpl;
-    const unsigned d = __reduce_or_sync(FULL, li < s.nlines ? (unsigned)s.dir[li] : 0u);
-    const int dir = d == 2u ? DIR_NEG : (d == 3u ? DIR_MIX : DIR_POS);
-#define VERB_JOB3(TT)                                              \
-    case TT:                                                       \
-        if (dir == DIR_POS) sweep_job<TT, DIR_POS>(s, job);        \
-        else if (dir == DIR_NEG) sweep_job<TT, DIR_NEG>(s, job);   \
-        else sweep_job<TT, DIR_MIX>(s, job);                       \
-        break;
-    switch (s.T) {
-        VERB_JOB3(3)
-        VERB_JOB3(4)
-        VERB_JOB3(5)
-        VERB_JOB3(6)
-        VERB_JOB3(7)
-        VERB_JOB3(8)
-        case 10: sweep_job<10, DIR_MIX>(s, job); break;
-        case 12: sweep_job<12, DIR_MIX>(s, job); break;
-        default: sweep_job<16, DIR_MIX>(s, job); break;
-    }
-#undef VERB_JOB3
-}
-
-#ifndef VERB_CONV_MINB
-#define VERB_CONV_MINB 2
-#endif
-__global__ void __launch_bounds__(C3_THREADS, VERB_CONV_MINB) convection_kernel(ConvArgs a)
+__global__ void __launch_bounds__(C3_THREADS, 2) convection_kernel(ConvArgs a)
 {
     extern __shared__ double sm[];
     const Dims d = a.d;
     const int P = d.P, R = d.R, V = d.V, K = d.K;
     const int PR = P * R;
-    const int RS = plane_stride(R);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double* X = sm;                          // [P + 2 GST][RS]
-    double* lbP = X + plane_doubles(P, R);   // per P-line (index iR): lbc, ubc, dxl, dxu
+    double* S = sm;                // [P][R]
+    double* lbP = S + PR;          // per P-line (index iR): lbc, ubc, dxl, dxu
     double* ubP = lbP + R;
     double* dxP = ubP + R;
     double* dxPu = dxP + R;
-    double* lbR = dxPu + R;                  // per R-line (index iP)
+    double* lbR = dxPu + R;        // per R-line (index iP)
     double* ubR = lbR + P;
     double* dxR = ubR + P;
     double* dxRu = dxR + P;
-    double* red = dxRu + P;                  // [32]
-    int* nsP = (int*)(red + 32);             // [R] per-line sub-steps
-    int* nsR = nsP + R;                      // [P]
-    int* dirP = nsR + P;                     // [R] per-line face directions: bit 0 some Courant >= 0,
-    int* dirR = dirP + R;                    // [P]                           bit 1 some Courant < 0
-    __shared__ int s_ticket, s_flags;
-    auto xi = [&](int iP, int iR) { return (iP + GST) * RS + iR + GST; };
+    double* red = dxRu + P;        // [32]
+    int* nsP = (int*)(red + 32);   // [R] per-line sub-steps
+    int* nsR = nsP + R;            // [P]
+    int* dirP = nsR + P;           // [R] per-line face directions: bit 0 some Courant >= 0,
+    int* dirR = dirP + R;          // [P]                           bit 1 some Courant < 0
+    const int wstride = conv_wstride(P, R);
+    double* wall = sm + conv_wall_offset(P, R);  // pointer arithmetic on sm keeps LDS/STS
+    double* wb = wall + (size_t)warp * wstride;
+    __shared__ int s_ticket;
+
+    // line buffers start as zeros: ghost slots that a sweep never writes are
+    // read only by padding lanes, whose results are discarded
+    for (int i = threadIdx.x; i < C3_WARPS * wstride; i += blockDim.x) wall[i] = 0.0;
 
     const SweepCfg cP = sweep_cfg(P, R - 1), cR = sweep_cfg(R, P);
     const size_t VK = (size_t)V * K;
-    size_t offR = 0;
-    const size_t ntab = conv_table_doubles(P, R, &offR);
-    double* crP = a.scratch + (size_t)blockIdx.x * conv_scratch_per_cta(P, R);  // [R-1][TP][lplP]
-    double* gpl = crP + ntab;  // G of the slice
-#ifdef VERB_CONV_CR_SMEM
-    crP = (double*)(dirR + P) + 1;  // after the int arrays, 8-byte aligned (+1 for odd P+R)
-    crP = (double*)(((size_t)crP + 7) & ~(size_t)7);
-#endif
-    double* crR = crP + offR;                                                  // [P][TR][lplR]
+    double* crP = a.scratch + (size_t)blockIdx.x * conv_scratch_per_cta(P, R);  // [R-1][P]
+    double* crR = crP + (size_t)(R > 1 ? R - 1 : 1) * P;                       // [P][R]
+    double* gpl = crR + PR;    // G of the slice
     double* lexp = gpl + PR;   // exp(Loss dt)
     double* spl = lexp + PR;   // Sources dt
     const int nslices = V * K;
+    const LineArrays laP{lbP, ubP, dxP, dxPu, nsP, dirP};
+    const LineArrays laR{lbR, ubR, dxR, dxRu, nsR, dirR};
     // first face of a line that the reference sweeps (face 0 only when periodic)
     const int ixP0 = a.Pl_t == VERB_BC_PERIODIC ? 0 : 1;
     const int ixR0 = a.Rl_t == VERB_BC_PERIODIC ? 0 : 1;
-
-    SweepRun sP{};
-    sP.X = X;
-    sP.RS = RS;
-    sP.rsw = false;
-    sP.n = P;
-    sP.nlines = R - 1;  // the last R row is not swept (src/Convection_2D.cpp:104)
-    sP.lt = a.Pl_t;
-    sP.ut = a.Pu_t;
-    sP.lpl = cP.lpl;
-    sP.T = cP.T;
-    sP.crtab = crP;
-    sP.lb = lbP;
-    sP.ub = ubP;
-    sP.dxl = dxP;
-    sP.dxu = dxPu;
-    sP.ns = nsP;
-    sP.dir = dirP;
-    sP.fuse_src = false;
-    SweepRun sR{};
-    sR.X = X;
-    sR.RS = RS;
-    sR.rsw = true;
-    sR.n = R;
-    sR.nlines = P;
-    sR.lt = a.Rl_t;
-    sR.ut = a.Ru_t;
-    sR.lpl = cR.lpl;
-    sR.T = cR.T;
-    sR.crtab = crR;
-    sR.lb = lbR;
-    sR.ub = ubR;
-    sR.dxl = dxR;
-    sR.dxu = dxRu;
-    sR.ns = nsR;
-    sR.dir = dirR;
-    sR.spl = spl;
-    sR.R = R;
+    // the thread's first L index and its advance per C3_THREADS cells
+    const int iR0 = threadIdx.x % R, iRstep = C3_THREADS % R;
 
     for (;;) {
         if (threadIdx.x == 0) s_ticket = atomicAdd(a.ticket, 1);
@@ -973,7 +943,7 @@ __global__ void __launch_bounds__(C3_THREADS, VERB_CONV_MINB) convection_kernel(
         for (int i = threadIdx.x; i < PR; i += blockDim.x) {
             const int iP = i / R, iR = i - iP * R;
             const size_t gi = g(iP, iR);
-            X[xi(iP, iR)] = a.psd[gi];
+            S[i] = a.psd[gi];
             const double vp = fabs(a.VP[gi]), vr = fabs(a.VR[gi]);
             vpm = (vpm < vp) ? vp : vpm;
             vrm = (vrm < vr) ? vr : vrm;
@@ -1001,31 +971,13 @@ __global__ void __launch_bounds__(C3_THREADS, VERB_CONV_MINB) convection_kernel(
             continue;
         }
         const double dtc = a.dt / num_steps;
-        if (threadIdx.x == 0) {
-            a.substeps[off] = (int)num_steps;
-            s_flags = 7;
-        }
-        __syncthreads();
-        // G, exp(Loss dt), Sources dt of the slice; flags: bit 0 G == 1
-        // everywhere, bit 1 exp(Loss dt) == 1 everywhere, bit 2 Sources dt
-        // is +0 everywhere
-        {
-            int fl = 7;
-            for (int i = threadIdx.x; i < PR; i += blockDim.x) {
-                const int iP = i / R, iR = i - iP * R;
-                const size_t gi = g(iP, iR);
-                const double le = exp(a.loss[gi] * dtc);
-                const double gg = a.G[gi];
-                const double sd = a.S[gi] * dtc;
-                lexp[i] = le;
-                gpl[i] = gg;
-                spl[i] = sd;
-                if (!(gg == 1.0)) fl &= ~1;
-                if (!(le == 1.0)) fl &= ~2;
-                if (__double_as_longlong(sd) != 0) fl &= ~4;
-            }
-            fl = __reduce_and_sync(FULL, fl);
-            if (lane == 0 && fl != 7) atomicAnd(&s_flags, fl);
+        if (threadIdx.x == 0) a.substeps[off] = (int)num_steps;
+        for (int i = threadIdx.x; i < PR; i += blockDim.x) {
+            const int iP = i / R, iR = i - iP * R;
+            const size_t gi = g(iP, iR);
+            lexp[i] = exp(a.loss[gi] * dtc);
+            gpl[i] = a.G[gi];
+            spl[i] = a.S[gi] * dtc;
         }
 
         // per-line CFL sub-cycles and face Courant numbers (QUICKEST6.cpp:37-52,
@@ -1038,7 +990,7 @@ __global__ void __launch_bounds__(C3_THREADS, VERB_CONV_MINB) convection_kernel(
                     m = (m > v) ? m : v;
                 }
                 for (int o = 16; o > 0; o >>= 1) {
-                    const double q = __shfl_xor_sync(FULL, m, o);
+                    const double q = __shfl_xor_sync(0xffffffffu, m, o);
                     m = (m > q) ? m : q;
                 }
                 const double dx = a.Pg[g(1, iR)] - a.Pg[g(0, iR)];
@@ -1049,20 +1001,15 @@ __global__ void __launch_bounds__(C3_THREADS, VERB_CONV_MINB) convection_kernel(
                 const double dtl = dtc / ns;
                 if (fabs(m / dx * dtl) > 1) set_error(a.status, VERB_ERR_CFL);
                 unsigned dir = 0;
-                double* tab = crP + (size_t)iR * cP.T * cP.lpl;
-                for (int ix = lane; ix < cP.T * cP.lpl; ix += 32) {
-                    double cr = 0.0;
-                    if (ix < P) {
-                        const int i0 = ix == 0 ? P - 2 : ix - 1;
-                        const double c0 = a.VP[g(i0, iR)] / dx * dtl;
-                        const double c1 = a.VP[g(ix, iR)] / dx * dtl;
-                        cr = (c0 + c1) / 2;
-                        if (ix >= ixP0) dir |= cr >= 0 ? 1u : (cr < 0 ? 2u : 0u);
-                    }
-                    const int jj = ix / cP.T;
-                    tab[(ix - jj * cP.T) * cP.lpl + jj] = cr;
+                for (int ix = lane; ix < P; ix += 32) {
+                    const int i0 = ix == 0 ? P - 2 : ix - 1;
+                    const double c0 = a.VP[g(i0, iR)] / dx * dtl;
+                    const double c1 = a.VP[g(ix, iR)] / dx * dtl;
+                    const double cr = (c0 + c1) / 2;
+                    crP[(size_t)iR * P + ix] = cr;
+                    if (ix >= ixP0) dir |= cr >= 0 ? 1u : (cr < 0 ? 2u : 0u);
                 }
-                dir = __reduce_or_sync(FULL, dir);
+                dir = __reduce_or_sync(0xffffffffu, dir);
                 if (lane == 0) {
                     dirP[iR] = (int)dir;
                     nsP[iR] = ns;
@@ -1082,7 +1029,7 @@ __global__ void __launch_bounds__(C3_THREADS, VERB_CONV_MINB) convection_kernel(
                     m = (m > v) ? m : v;
                 }
                 for (int o = 16; o > 0; o >>= 1) {
-                    const double q = __shfl_xor_sync(FULL, m, o);
+                    const double q = __shfl_xor_sync(0xffffffffu, m, o);
                     m = (m > q) ? m : q;
                 }
                 const double dx = a.Rg[g(iP, 1)] - a.Rg[g(iP, 0)];
@@ -1093,20 +1040,15 @@ __global__ void __launch_bounds__(C3_THREADS, VERB_CONV_MINB) convection_kernel(
                 const double dtl = dtc / ns;
                 if (fabs(m / dx * dtl) > 1) set_error(a.status, VERB_ERR_CFL);
                 unsigned dir = 0;
-                double* tab = crR + (size_t)iP * cR.T * cR.lpl;
-                for (int ix = lane; ix < cR.T * cR.lpl; ix += 32) {
-                    double cr = 0.0;
-                    if (ix < R) {
-                        const int i0 = ix == 0 ? R - 2 : ix - 1;
-                        const double c0 = a.VR[g(iP, i0)] / dx * dtl;
-                        const double c1 = a.VR[g(iP, ix)] / dx * dtl;
-                        cr = (c0 + c1) / 2;
-                        if (ix >= ixR0) dir |= cr >= 0 ? 1u : (cr < 0 ? 2u : 0u);
-                    }
-                    const int jj = ix / cR.T;
-                    tab[(ix - jj * cR.T) * cR.lpl + jj] = cr;
+                for (int ix = lane; ix < R; ix += 32) {
+                    const int i0 = ix == 0 ? R - 2 : ix - 1;
+                    const double c0 = a.VR[g(iP, i0)] / dx * dtl;
+                    const double c1 = a.VR[g(iP, ix)] / dx * dtl;
+                    const double cr = (c0 + c1) / 2;
+                    crR[(size_t)iP * R + ix] = cr;
+                    if (ix >= ixR0) dir |= cr >= 0 ? 1u : (cr < 0 ? 2u : 0u);
                 }
-                dir = __reduce_or_sync(FULL, dir);
+                dir = __reduce_or_sync(0xffffffffu, dir);
                 if (lane == 0) {
                     dirR[iP] = (int)dir;
                     nsR[iP] = ns;
@@ -1119,51 +1061,48 @@ __global__ void __launch_bounds__(C3_THREADS, VERB_CONV_MINB) convection_kernel(
             }
         }
         __syncthreads();
-        const int flags = s_flags;
-        const bool fused = (flags & 3) == 3;  // G = 1 and exp(Loss dt) = 1
-        sR.fuse_src = fused;
-        sR.spl_zero = (flags & 4) != 0;
 
         for (int it = 0; it < num_steps; it++) {
             if (P >= 3) {
                 // P-lines iR = 0 .. R-2 (the last R row is not swept, :104)
-                for (int job = warp; job < cP.njobs; job += C3_WARPS) run_job(sP, job);
+                for (int job = warp; job < cP.njobs; job += C3_WARPS)
+                    sweep_job<false>(S, wb, cP, job, P, R - 1, R, a.Pl_t, a.Pu_t, crP, laP);
                 __syncthreads();
             }
             if (R >= 3) {
-                if (!(flags & 1)) {
-                    for (int i = threadIdx.x; i < PR; i += C3_THREADS) {
-                        const int iP = i / R, iR = i - iP * R;
-                        X[xi(iP, iR)] = X[xi(iP, iR)] * gpl[i];
-                    }
-                    __syncthreads();
-                }
-                for (int job = warp; job < cR.njobs; job += C3_WARPS) run_job(sR, job);
+#pragma unroll 4
+                for (int i = threadIdx.x; i < PR; i += C3_THREADS) S[i] = S[i] * gpl[i];
                 __syncthreads();
-                if (!fused) {
-                    for (int i = threadIdx.x; i < PR; i += C3_THREADS) {
-                        const int iP = i / R, iR = i - iP * R;
-                        double x = X[xi(iP, iR)] / gpl[i];
-                        x = x * lexp[i];
-                        if (iR >= 1 && iR < R - 1) x = x + spl[i];
-                        X[xi(iP, iR)] = x;
-                    }
-                    __syncthreads();
+                for (int job = warp; job < cR.njobs; job += C3_WARPS)
+                    sweep_job<true>(S, wb, cR, job, R, P, R, a.Rl_t, a.Ru_t, crR, laR);
+                __syncthreads();
+                int iR = iR0;
+#pragma unroll 4
+                for (int i = threadIdx.x; i < PR; i += C3_THREADS) {
+                    double x = S[i] / gpl[i];
+                    x = x * lexp[i];
+                    if (iR >= 1 && iR < R - 1) x = x + spl[i];
+                    S[i] = x;
+                    iR += iRstep;
+                    if (iR >= R) iR -= R;
                 }
+                __syncthreads();
             } else {
                 // no R-sweep: exp(loss dt) and sources only (:147-165)
+                int iR = iR0;
                 for (int i = threadIdx.x; i < PR; i += C3_THREADS) {
-                    const int iP = i / R, iR = i - iP * R;
-                    double x = X[xi(iP, iR)] * lexp[i];
+                    double x = S[i] * lexp[i];
                     if (iR >= 1 && iR < R - 1) x = x + spl[i];
-                    X[xi(iP, iR)] = x;
+                    S[i] = x;
+                    iR += iRstep;
+                    if (iR >= R) iR -= R;
                 }
                 __syncthreads();
             }
         }
         for (int i = threadIdx.x; i < PR; i += blockDim.x) {
             const int iP = i / R, iR = i - iP * R;
-            a.psd[g(iP, iR)] = X[xi(iP, iR)];
+            a.psd[g(iP, iR)] = S[i];
         }
         __syncthreads();
     }
@@ -1222,7 +1161,10 @@ using namespace VERB_CONV_NS;
 
 #ifdef VERB_BUILD_CONV_FMA
 
-size_t conv_smem_bytes_fma(int P, int R) { return (size_t)conv_smem_doubles(P, R) * sizeof(double); }
+size_t conv_smem_bytes_fma(int P, int R)
+{
+    return ((size_t)conv_wall_offset(P, R) + (size_t)C3_WARPS * conv_wstride(P, R)) * sizeof(double);
+}
 
 int conv_check_fma(int P, int R)
 {
@@ -1256,7 +1198,10 @@ void launch_convection_fma(const ConvArgs& a, int nctas, cudaStream_t s)
 
 #else
 
-size_t conv_smem_bytes(int P, int R) { return (size_t)conv_smem_doubles(P, R) * sizeof(double); }
+size_t conv_smem_bytes(int P, int R)
+{
+    return ((size_t)conv_wall_offset(P, R) + (size_t)C3_WARPS * conv_wstride(P, R)) * sizeof(double);
+}
 
 size_t conv_scratch_doubles(int P, int R) { return conv_scratch_per_cta(P, R); }
 

@@ -17,7 +17,7 @@
 //
 // Limits and sharing:
 //  * P_size * R_size must not exceed VERB_NOALLOC_MAX_POINTS (8192 points,
-//    7 doubles each: 448 KiB of scratch); larger slices are rejected with
+//    5 doubles each: 320 KiB of scratch); larger slices are rejected with
 //    VERB_ERR_SIZE, and so are lines longer than the kernel's 512 points.
 //  * Every GPU that loads the library holds the array until the process exits.
 //  * All calls share the one array and it keeps the last call's contents; the
@@ -40,7 +40,7 @@
 namespace {
 
 constexpr int kMaxPoints = VERB_NOALLOC_MAX_POINTS;
-constexpr int kPlaneDoubles = 7 * kMaxPoints;  // >= conv_scratch_doubles(P, R) for P*R <= kMaxPoints
+constexpr int kPlaneDoubles = 5 * kMaxPoints;  // >= conv_scratch_doubles(P, R) for P*R <= kMaxPoints
 constexpr int kWords = 8;  // ticket, sub-step count, status (+ padding)
 
 // The scratch: kPlaneDoubles doubles for one CTA, then kWords ints.
