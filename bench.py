@@ -414,7 +414,7 @@ def run_ours(args):
     fp64_peak = fp64_peak_tops()
     conv_tops = conv_ops / (conv_ms / 1e3) / 1e12
     out = {
-        "metric": METRIC if args.config == "cfg2" else "sim-hours/s at 25x31x31x24",
+        "metric": metric_name(spec),
         "value": round(value, 5), "unit": "sim-hours/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
@@ -477,6 +477,13 @@ def run_ours(args):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def metric_name(spec):
+    """The metric's label: sim-hours/s at L x E x alpha x MLT."""
+    if (spec.R, spec.V, spec.K, spec.P) == (101, 101, 91, 48):
+        return METRIC
+    return f"sim-hours/s at {spec.R}x{spec.V}x{spec.K}x{spec.P}"
 
 
 def timed_hours(args, dt):
@@ -558,6 +565,99 @@ def measure_forms(args, wl, make_solver, update_dev, stream, dev):
                      "initial state; the bar is 1e-8",
             "timing": "CUDA events, graph-replayed steps after 3 warm-up steps and the "
                       "local-solve autotuner, one context at a time"}
+
+
+# --------------------------------------------------------------------------- learned form
+def run_learned(args):
+    """The learned form at the 24 x 25 x 31 x 31 size: the CNN's training
+    step on the tensor cores (256 images of 31 x 31), the learned
+    preconditioner trained on the systems of six seeds, and the local step of
+    a held-out seed by the LU, by the Krylov form with the Jacobi
+    preconditioner and with the learned one (iterations, fallback rate, time,
+    agreement with the LU step)."""
+    import torch
+
+    from verb4d_b200 import Solver, learned
+    from verb4d_b200 import workload as W
+
+    torch.cuda.set_device(0)
+    spec = W.CONFIGS["cfg1"]
+    P, R, V, K = spec.shape
+    nsys = P * R
+    out = {"metric": "local step ms at 25x31x31x24 (learned form)", "unit": "ms",
+           "higher_is_better": False, "n_gpus": 1, "data": "synthetic (seeded)",
+           "config": {"workload": "local (V,K) step of the 24 x 25 x 31 x 31 grid, dt=5 min"}}
+    # CNN training step on the tensor cores
+    B = 256
+    net = learned.CNN(K, V, B, seed=1)
+    x = torch.randn((B, 4, K, V), device="cuda")
+    t = torch.randn((B, 1, K, V), device="cuda")
+    for _ in range(3):
+        net.train_step(x.data_ptr(), t.data_ptr(), B, 1e-3)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(10):
+        net.train_step(x.data_ptr(), t.data_ptr(), B, 1e-3)
+    e1.record()
+    torch.cuda.synchronize()
+    out["cnn_train_step_ms"] = round(e0.elapsed_time(e1) / 10, 3)
+    net.close()
+    if args.learned_epochs <= 0:
+        print(json.dumps(out), flush=True)
+        return
+    # the learned preconditioner
+    t0 = time.perf_counter()
+    base = W.make_workload(spec, seed=1, sources=True, losses=True)
+    feat, A9 = learned.precond_inputs(base, seeds=range(2, 7))
+    pc = learned.CNN(K, V, max(nsys, 64), channels=learned.PC_CHANNELS, seed=0)
+    pc.zero_last_layer()
+    hist = learned.train_preconditioner(pc, feat, A9, V, K, epochs=args.learned_epochs, batch=64)
+    out["precond_training"] = {"seconds": round(time.perf_counter() - t0, 1),
+                               "systems": int(feat.shape[0]), "epochs": args.learned_epochs,
+                               "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1]}
+    wl = W.make_workload(spec, seed=100, sources=True, losses=True)
+    fl = wl.flags
+
+    def split():
+        s = Solver(wl)
+        s.load()
+        s.ctx.step(wl.dt, wl.sub_dt, fl["run_convection"], fl["run_radial"], 0)
+        return s
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        return r, (time.perf_counter() - a) * 1e3
+
+    s = split()
+    s.ctx.local(wl.dt, wl.sub_dt)
+    s.ctx.sync()
+    s.ctx.close()
+    s = split()
+    _, lu_ms = timed(lambda: (s.ctx.local(wl.dt, wl.sub_dt), s.ctx.sync()))
+    ref = s.ctx.download()
+    s.ctx.close()
+    res = {"lu": {"ms": round(lu_ms, 2), "note": "factorisation included"}}
+    for name, net_pc in (("krylov_jacobi", None), ("krylov_learned", pc)):
+        for rep in range(2):  # the first call allocates
+            s = split()
+            s.ctx.set_krylov_preconditioner(net_pc)
+            st, ms = timed(lambda: (s.ctx.local_krylov(wl.dt, wl.sub_dt, guess="prev"),
+                                    s.ctx.sync())[0])
+            got = s.ctx.download()
+            s.ctx.close()
+        ns = max(st["systems"] - st["fallbacks"], 1)
+        res[name] = {"ms": round(ms, 2),
+                     "iterations_per_krylov_solved_system": round(st["solved_iterations"] / ns, 1),
+                     "fallback_rate": round(st["fallbacks"] / st["systems"], 4),
+                     "max_rel_err_vs_lu_step": float(np.abs(got - ref).max() / np.abs(ref).max())}
+    out["local_step"] = res
+    out["value"] = res["krylov_learned"]["ms"]
+    pc.close()
+    print(json.dumps(out), flush=True)
 
 
 # --------------------------------------------------------------------------- ensemble
@@ -762,7 +862,7 @@ def run_reference(args):
     rs.close()
     sim_h = args.steps * wl.dt * 24.0
     value = sim_h / t_total
-    out = {"metric": METRIC if args.config == "cfg2" else "sim-hours/s at 25x31x31x24",
+    out = {"metric": metric_name(spec),
            "value": value, "unit": "sim-hours/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": round(t_total / args.steps * 1e3, 1),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -798,6 +898,9 @@ def main():
     ap.add_argument("--trim", action="store_true",
                     help="ragged local systems: pitch angles outside the loss cone only")
     ap.add_argument("--ensemble", action="store_true", help="run the member ensemble instead")
+    ap.add_argument("--learned", action="store_true",
+                    help="time the learned form (CNN training step, learned preconditioner)")
+    ap.add_argument("--learned-epochs", type=int, default=12)
     ap.add_argument("--members", type=int, default=64)
     ap.add_argument("--ens-steps", type=int, default=12)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -814,6 +917,8 @@ def main():
         run_reference(args)
     elif args.ensemble:
         run_ensemble(args)
+    elif args.learned:
+        run_learned(args)
     else:
         run_ours(args)
 

@@ -320,8 +320,9 @@ int verb_local_krylov(verb_ctx* ctx, double dt, double sub_dt, int guess, verb_c
  * diagonal, [sys][9][K][V] (verb_local_precond_inputs, which also returns the
  * FP32 diagonals [sys][9][V*K]).  verb_precond_loss_grad gives its training
  * signal: for nprobe probe vectors z per system ([sys][nprobe][V*K]) the loss
- * mean |A M z - z|^2 and its gradient with respect to C ([sys][25][V*K]), to
- * pass to verb_cnn_backward_step.  net = NULL restores Jacobi.  The context
+ * mean |D^-1 A M D z - z|^2 on the Jacobi-scaled system (D = diag(A), so
+ * every row counts alike) and its gradient with respect to C
+ * ([sys][25][V*K]), to pass to verb_cnn_backward_step.  net = NULL restores Jacobi.  The context
  * keeps the pointer: the network must outlive its use. */
 int verb_set_krylov_preconditioner(verb_ctx* ctx, verb_cnn* net);
 int verb_local_precond_inputs(verb_ctx* ctx, double dt, double sub_dt, float* feat_dev,

@@ -129,8 +129,9 @@ def matvec9_t(A9, e, nx):
 
 
 def precond_loss_grad(A9s, Cs, Zs, nx, ny):
-    """Loss mean |A M z - z|^2 over systems and probes and its gradient with
-    respect to C (the definition of verb_precond_loss_grad)."""
+    """Loss mean |D^-1 A M D z - z|^2 (the Jacobi-scaled system) over systems
+    and probes, and its gradient with respect to C (the definition of
+    verb_precond_loss_grad).  M D z is the stencil of delta + C applied to z."""
     nsys, nprobe, n = Zs.shape
     cnt = nsys * nprobe * n
     loss = 0.0
@@ -139,16 +140,15 @@ def precond_loss_grad(A9s, Cs, Zs, nx, ny):
         dg = A9s[s][4]
         for q in range(nprobe):
             z = Zs[s, q]
-            y = precond_apply(A9s[s], Cs[s], z, nx, ny)
-            e = matvec9(A9s[s], y, nx) - z
+            y = precond_apply(A9s[s], Cs[s], z * dg, nx, ny)  # M (D z)
+            e = matvec9(A9s[s], y, nx) / dg - z
             loss += float(e @ e) / cnt
-            gy = 2.0 / cnt * matvec9_t(A9s[s], e, nx)
+            gy = 2.0 / cnt * matvec9_t(A9s[s], e / dg, nx)
             for i in range(n):
                 iy, ix = divmod(i, nx)
                 for dy in range(-2, 3):
                     for dx in range(-2, 3):
                         yy, xx = iy + dy, ix + dx
                         if 0 <= yy < ny and 0 <= xx < nx:
-                            j = yy * nx + xx
-                            g[s, (dy + 2) * 5 + (dx + 2), i] += gy[i] * z[j] / dg[j]
+                            g[s, (dy + 2) * 5 + (dx + 2), i] += gy[i] * z[yy * nx + xx]
     return loss, g

@@ -6,7 +6,8 @@ diagonal) and predicts, for every unknown, the 25 coefficients of a sparse
 approximate inverse on its 5 x 5 neighbourhood; C = 0 is the Jacobi
 preconditioner the Krylov form uses without it.  It is trained on the GPU by
 the project's own kernels to make A M close to the identity on random probe
-vectors (loss mean |A M z - z|^2), and then preconditions the FP32 BiCGSTAB
+vectors (loss mean |D^-1 A M D z - z|^2 on the Jacobi-scaled system,
+D = diag(A)), and then preconditions the FP32 BiCGSTAB
 inside the FP64 refinement of verb_local_krylov.
 
 * The training signal (verb_precond_loss_grad) equals its CPU definition
@@ -14,9 +15,14 @@ inside the FP64 refinement of verb_local_krylov.
 * On the 24 x 25 x 31 x 31 grid (the learned form's configuration), trained
   on the systems of six seeds and tested on a held-out seed: training lowers
   the loss below its Jacobi start, and the Krylov step with the learned
-  preconditioner agrees with the LU step to 1e-8, like the Jacobi one.  The
-  iteration counts, fallback rates and local-step times of Jacobi, the
-  learned preconditioner and the LU are printed.
+  preconditioner agrees with the LU step to 1e-8, like the Jacobi one, and
+  its BiCGSTAB needs fewer iterations per Krylov-solved system than Jacobi's.
+  Measured on a B200 (12 epochs, 2.3 s of training): loss 0.242 -> 0.112;
+  124 iterations per solved system against 216 with Jacobi, fallback rate
+  2.3 % against 18.2 %; local step 38.6 ms against 16.4 ms (Jacobi) and
+  15.4 ms for the banded LU with its factorisation.  The network's forward
+  pass and the 25-tap apply cost more than the iterations save, so the LU
+  stays the production form.
 """
 import time
 
@@ -87,6 +93,7 @@ def test_learned_preconditioner_against_jacobi(gpu):
         res[name] = (st["solved_iterations"] / ns, st["fallbacks"] / st["systems"], ms)
         print(name, "iterations per Krylov-solved system %.1f, fallback rate %.3f, local step %.1f ms"
               % res[name])
+    assert res["learned"][0] < 0.9 * res["jacobi"][0]
     c = split_ctx(wl)
     c.local(wl.dt, wl.sub_dt)
     c.sync()

@@ -913,10 +913,13 @@ __global__ void precond_features_kernel(LocalArgs a, const float* A9, float* fea
 }
 
 // Training signal of the learned preconditioner for nprobe probe vectors z
-// per system: y = M z, e = A y - z, loss += |e|^2 / cnt and
-// gC[o](i) = (2 / cnt) sum_z (A^T e)(i) z(i + o) / diag(i + o), the
-// gradient of the loss with respect to C.  One CTA per system; z, y and e
-// live in shared memory (3 n floats).
+// per system, on the Jacobi-scaled system (unit diagonal) so that every row
+// counts alike whatever its scale: with A~ = D^-1 A and M~ = M D (the
+// stencil of C without the division, so A M = I exactly when A~ M~ = I),
+// y = M~ z, e = A~ y - z, loss += |e|^2 / cnt and
+// gC[o](i) = (2 / cnt) sum_z (A^T D^-1 e)(i) z(i + o), the gradient of the
+// loss with respect to C.  One CTA per system; z, y and e live in shared
+// memory (3 n floats).
 __global__ void precond_grad_kernel(const float* A9, const float* C, const float* Z, float* gC,
                                     float* loss, int nx, int ny, int nprobe, float inv_cnt)
 {
@@ -937,16 +940,33 @@ __global__ void precond_grad_kernel(const float* A9, const float* C, const float
         const float* zq = Z + ((size_t)sys * nprobe + q) * n;
         for (int i = threadIdx.x; i < n; i += blockDim.x) z[i] = zq[i];
         __syncthreads();
-        for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = precond_row(Cs, dg, z, n, nx, ny, i);
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            // y = M~ z: the stencil of delta + C on z
+            const int iy = i / nx, ix = i - iy * nx;
+            float acc = 0.f;
+#pragma unroll
+            for (int dy = -2; dy <= 2; dy++) {
+                const int yy = iy + dy;
+                if (yy < 0 || yy >= ny) continue;
+#pragma unroll
+                for (int dx = -2; dx <= 2; dx++) {
+                    const int xx = ix + dx;
+                    if (xx < 0 || xx >= nx) continue;
+                    const int o = (dy + 2) * 5 + (dx + 2);
+                    acc = fmaf(Cs[(size_t)o * n + i] + (o == 12 ? 1.f : 0.f), z[yy * nx + xx], acc);
+                }
+            }
+            y[i] = acc;
+        }
         __syncthreads();
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            const float ei = mv_row(A, y, n, nx, i) - z[i];
-            e[i] = ei;
+            const float ei = mv_row(A, y, n, nx, i) / dg[i] - z[i];
+            e[i] = ei / dg[i];  // D^-1 e, the operand of A^T below
             lsum = fmaf(ei, ei, lsum);
         }
         __syncthreads();
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            // (A^T e)(i): rows r = i - off with A[k](r) multiplying x(r + off)
+            // (A^T D^-1 e)(i): rows r = i - off with A[k](r) multiplying x(r + off)
             float gy = 0.f;
 #pragma unroll
             for (int dy = -1; dy <= 1; dy++)
@@ -966,8 +986,7 @@ __global__ void precond_grad_kernel(const float* A9, const float* C, const float
                 for (int dx = -2; dx <= 2; dx++) {
                     const int xx = ix + dx;
                     if (xx < 0 || xx >= nx) continue;
-                    const int j = yy * nx + xx;
-                    g[(size_t)((dy + 2) * 5 + (dx + 2)) * n + i] += gy * (z[j] / dg[j]);
+                    g[(size_t)((dy + 2) * 5 + (dx + 2)) * n + i] += gy * z[yy * nx + xx];
                 }
             }
         }

@@ -124,8 +124,9 @@ def precond_inputs(wl, seeds=None):
 
 
 def precond_loss_grad(A9, Cc, Z, V, K):
-    """mean |A M z - z|^2 over the probes Z [B][nprobe][V*K] and its gradient
-    with respect to the coefficients Cc [B][25][K][V] (device tensors)."""
+    """mean |D^-1 A M D z - z|^2 (D = diag(A)) over the probes Z
+    [B][nprobe][V*K] and its gradient with respect to the coefficients Cc
+    [B][25][K][V] (device tensors)."""
     import torch
 
     g = torch.empty_like(Cc)
@@ -140,7 +141,7 @@ def train_preconditioner(net, feat, A9, V, K, epochs=30, batch=64, nprobe=4, lr=
                          lr_final=2e-4, seed=0):
     """Adam on shuffled system batches with Gaussian probe vectors: the
     network learns coefficients C that make A M close to the identity
-    (the loss is mean |A M z - z|^2 over the probes).  Returns the mean loss of
+    (the loss is mean |D^-1 A M D z - z|^2 over the probes, D = diag(A)).  Returns the mean loss of
     every epoch."""
     import torch
 
