@@ -119,6 +119,11 @@ class ClockSampler:
 
 
 FP64_OPS_PER_FACE = 179
+# FP64-pipe share of the contracted convection kernel's active cycles
+# (ncu sm__inst_executed_pipe_fp64, --set full capture of one launch at
+# 48 x 101 x 101 x 8); the op-count fraction above counts the reference's
+# operations, the pipe share the ones the kernel issues
+CONV_FP64_PIPE_NCU = 0.336
 
 
 def fp64_peak_tops():
@@ -321,6 +326,11 @@ def run_ours(args):
     forms = None
     if not args.no_forms:
         forms = measure_forms(args, wl, make_solver, update_dev, stream, dev)
+        if world == 1 and args.learned_epochs > 0:
+            # the Krylov form with the learned preconditioner is defined at the
+            # 24 x 25 x 31 x 31 size (its systems fit one CTA's shared memory)
+            torch.cuda.empty_cache()
+            forms["learned_krylov_24x25x31x31"] = measure_learned(args.learned_epochs)
 
     # ---------------- end to end through the public API with host buffers (e2e)
     e2e = None
@@ -455,6 +465,9 @@ def run_ours(args):
                           "peak_source": "nominal FP64 issue rate, 148 SMs x 64 lanes at "
                                          "MEASURED_PEAKS.json sm_max_mhz",
                           "fp64_ops_per_face": FP64_OPS_PER_FACE,
+                          "fp64_pipe_active_ncu": CONV_FP64_PIPE_NCU,
+                          "fp64_pipe_source": "ncu inst_executed_pipe_fp64 over active cycles, "
+                                              "one launch at 48x101x101x8 (fma kernel)",
                           "face_updates_per_step": int((p_faces + r_faces) * conv_substeps)},
         "autotune": tune,
         "clocks": clk.summary(),
@@ -571,19 +584,18 @@ def measure_forms(args, wl, make_solver, update_dev, stream, dev):
 def run_learned(args):
     """The learned form at the 24 x 25 x 31 x 31 size: the CNN's training
     step on the tensor cores (256 images of 31 x 31), the learned
-    preconditioner trained on the systems of six seeds, and the local step of
-    a held-out seed by the LU, by the Krylov form with the Jacobi
+    preconditioner trained on the systems of five seeds, and the local step
+    of a held-out seed by the LU, by the Krylov form with the Jacobi
     preconditioner and with the learned one (iterations, fallback rate, time,
     agreement with the LU step)."""
     import torch
 
-    from verb4d_b200 import Solver, learned
+    from verb4d_b200 import learned
     from verb4d_b200 import workload as W
 
     torch.cuda.set_device(0)
     spec = W.CONFIGS["cfg1"]
-    P, R, V, K = spec.shape
-    nsys = P * R
+    _, _, V, K = spec.shape
     out = {"metric": "local step ms at 25x31x31x24 (learned form)", "unit": "ms",
            "higher_is_better": False, "n_gpus": 1, "data": "synthetic (seeded)",
            "config": {"workload": "local (V,K) step of the 24 x 25 x 31 x 31 grid, dt=5 min"}}
@@ -606,15 +618,35 @@ def run_learned(args):
     if args.learned_epochs <= 0:
         print(json.dumps(out), flush=True)
         return
+    out.update(measure_learned(args.learned_epochs))
+    out["value"] = out["local_step"]["krylov_learned"]["ms"]
+    print(json.dumps(out), flush=True)
+
+
+def measure_learned(epochs):
+    """The learned preconditioner at the 24 x 25 x 31 x 31 size, trained on
+    the local systems of five seeds, and the local step of a held-out seed by
+    the LU (factorisation included), by the Krylov form with the Jacobi
+    preconditioner and with the learned one: time, BiCGSTAB iterations per
+    Krylov-solved system, LU-fallback rate and distance from the LU step."""
+    import torch
+
+    from verb4d_b200 import Solver, learned
+    from verb4d_b200 import workload as W
+
+    spec = W.CONFIGS["cfg1"]
+    P, R, V, K = spec.shape
+    nsys = P * R
+    out = {}
     # the learned preconditioner
     t0 = time.perf_counter()
     base = W.make_workload(spec, seed=1, sources=True, losses=True)
     feat, A9 = learned.precond_inputs(base, seeds=range(2, 7))
     pc = learned.CNN(K, V, max(nsys, 64), channels=learned.PC_CHANNELS, seed=0)
     pc.zero_last_layer()
-    hist = learned.train_preconditioner(pc, feat, A9, V, K, epochs=args.learned_epochs, batch=64)
+    hist = learned.train_preconditioner(pc, feat, A9, V, K, epochs=epochs, batch=64)
     out["precond_training"] = {"seconds": round(time.perf_counter() - t0, 1),
-                               "systems": int(feat.shape[0]), "epochs": args.learned_epochs,
+                               "systems": int(feat.shape[0]), "epochs": epochs,
                                "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1]}
     wl = W.make_workload(spec, seed=100, sources=True, losses=True)
     fl = wl.flags
@@ -642,22 +674,28 @@ def run_learned(args):
     s.ctx.close()
     res = {"lu": {"ms": round(lu_ms, 2), "note": "factorisation included"}}
     for name, net_pc in (("krylov_jacobi", None), ("krylov_learned", pc)):
-        for rep in range(2):  # the first call allocates
+        calls = []
+        for rep in range(3):  # the first call allocates; the best of the others
             s = split()
             s.ctx.set_krylov_preconditioner(net_pc)
             st, ms = timed(lambda: (s.ctx.local_krylov(wl.dt, wl.sub_dt, guess="prev"),
                                     s.ctx.sync())[0])
             got = s.ctx.download()
             s.ctx.close()
+            calls.append(round(ms, 2))
+        ms = min(calls[1:])
         ns = max(st["systems"] - st["fallbacks"], 1)
-        res[name] = {"ms": round(ms, 2),
+        res[name] = {"ms": round(ms, 2), "calls_ms": calls,
                      "iterations_per_krylov_solved_system": round(st["solved_iterations"] / ns, 1),
                      "fallback_rate": round(st["fallbacks"] / st["systems"], 4),
                      "max_rel_err_vs_lu_step": float(np.abs(got - ref).max() / np.abs(ref).max())}
+    for name in ("krylov_jacobi", "krylov_learned"):
+        res[name]["time_vs_lu"] = round(res[name]["ms"] / lu_ms, 3)
     out["local_step"] = res
-    out["value"] = res["krylov_learned"]["ms"]
+    out["timing"] = ("host wall time of one local step (synchronised on both sides) on a "
+                     "fresh context, the best of the second and third of three calls")
     pc.close()
-    print(json.dumps(out), flush=True)
+    return out
 
 
 # --------------------------------------------------------------------------- ensemble

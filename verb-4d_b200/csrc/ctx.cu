@@ -265,8 +265,7 @@ int local_factor(verb_ctx* c, LocalArgs& a)
         CK(cudaMemsetAsync(c->Uf32, 0, nu * c->kvp32 * sizeof(float), c->stream));
     else
         CK(cudaMemsetAsync(c->Uf, 0, nu * c->kvp * sizeof(double), c->stream));
-    launch_local_factor(a, c->stream);
-    c->acc.kernel_launches++;
+    c->acc.kernel_launches += launch_local_factor(a, c->stream);
     c->local_dirty = false;
     c->local_dt = a.dt;
     c->acc.local_factor_launches++;

@@ -180,9 +180,9 @@ int krylov_run(verb_ctx* c, double dt, double sub_dt, int guess, verb_cnn* cnn, 
                 CK(cudaMemsetAsync(c->Uf32, 0, nuf * c->kvp32 * sizeof(float), c->stream));
             else
                 CK(cudaMemsetAsync(c->Uf, 0, nuf * c->kvp * sizeof(double), c->stream));
-            launch_local_factor(ap, c->stream);
+            c->acc.kernel_launches += launch_local_factor(ap, c->stream);
             launch_local_solve(ap, c->stream);
-            c->acc.kernel_launches += 2;
+            c->acc.kernel_launches++;
             // the mixed form's FP64 refinement (FP32 factors), as in the LU step
             for (int it = 0; it < c->refine_iters; it++) {
                 launch_local_residual(ap, c->kb, c->lwork, c->lres, c->stream);

@@ -17,6 +17,11 @@
 //    The active (kl+1) x (kv+1) window lives in shared memory as a circular
 //    buffer over rows and columns.  Output: L multipliers (Lf, column j
 //    contiguous), U columns (Uf, rows j-kv..j contiguous) and 0-based pivots.
+//  * local_rows_kernel + local_factor_rw_kernel: the same factorisation with
+//    the window in registers (eight warps, bands up to V = 110): the rows are
+//    assembled beforehand and parked in the L columns they precede, and
+//    stream into a shared-memory ring by cp.async.  local_factor_kernel is
+//    kept for wider bands.
 //  * local_rhs_kernel / local_store_kernel: tile transposes between the PSD
 //    slab [V][K] and the unknown order, forming RHS = B o f + C.
 //  * local_solve_kernel: one warp per system, the forward (L, interleaved row
@@ -24,7 +29,8 @@
 //    substitutions.  The solution window lives in shared memory; the factor
 //    columns stream through a per-warp cp.async ring so that each warp keeps
 //    several columns in flight.  This kernel moves the whole factor cache
-//    once per sub-step and is HBM-bound.
+//    once per sub-step and is HBM-bound.  local_solve_rw_kernel keeps the
+//    solution window in registers instead.
 //
 // All arithmetic follows the CPU restatement of xGBTF2/xGBTRS/xTBSV operation
 // by operation without FMA contraction (the file is compiled with
@@ -358,6 +364,314 @@ __global__ void __launch_bounds__(FACT_THREADS) local_factor_kernel(LocalArgs a)
     }
 }
 
+// The same factorisation with the (kl+1) x (kv+1) circular window held in
+// registers for the whole run.  NW warps (eight in use); warp w owns row slots
+// w + NW q (q < NR), lane l column slots l + 32 k (k < NC), value R[q][k].  Per column
+// j there are two block barriers:
+//   top   the lanes that own column slot j % CW search their own rows for the
+//         first maximum of |x| (they updated those values themselves at
+//         column j-1, so no barrier is needed before the search) and post the
+//         column and their warp's candidate;
+//   B1    every thread combines the NW candidates (idamax: first maximum,
+//         NaN skipped unless it is the first entry); the multipliers go to
+//         Lf; the owners of row j and of the pivot row post them;
+//   B2    the swap over columns j..ju in the owners' registers, U row j out,
+//         the rank-1 update of every owned slot (multipliers from the posted
+//         column, the pivot row from shared memory), and the slide: column
+//         slot j % CW is cleared, row slot j % RW takes row j+kl+1.
+// The row and column slots of the pivot step are reached through a switch on
+// their index (registers cannot be indexed at run time), so only the rank-1
+// update touches every slot.  Every element sees the same operations in the
+// same order as in local_factor_kernel (LAPACK's xGBTF2 without FMA): factors
+// and pivots are bit-identical, and the update costs no shared-memory traffic.
+// f(R[q]) for a run-time q < NR
+template <int NR, int NC, typename F>
+__device__ __forceinline__ void frw_row(double (&R)[NR][NC], int q, F&& f)
+{
+    switch (q) {
+#define VERB_ROW(Q) \
+    case Q:         \
+        if constexpr (Q < NR) f(R[Q]); \
+        break;
+        VERB_ROW(0) VERB_ROW(1) VERB_ROW(2) VERB_ROW(3) VERB_ROW(4) VERB_ROW(5) VERB_ROW(6)
+        VERB_ROW(7) VERB_ROW(8) VERB_ROW(9) VERB_ROW(10) VERB_ROW(11) VERB_ROW(12) VERB_ROW(13)
+#undef VERB_ROW
+        default: break;
+    }
+}
+
+template <int K, int NR, int NC, typename F>
+__device__ __forceinline__ void frw_col_k(double (&R)[NR][NC], F& f)
+{
+#pragma unroll
+    for (int q = 0; q < NR; q++) f(q, R[q][K]);
+}
+
+// f(q, R[q][k]) for every q, for a run-time k < NC
+template <int NR, int NC, typename F>
+__device__ __forceinline__ void frw_col(double (&R)[NR][NC], int k, F&& f)
+{
+    switch (k) {
+#define VERB_COL(K) \
+    case K:         \
+        if constexpr (K < NC) frw_col_k<K>(R, f); \
+        break;
+        VERB_COL(0) VERB_COL(1) VERB_COL(2) VERB_COL(3) VERB_COL(4) VERB_COL(5) VERB_COL(6)
+#undef VERB_COL
+        default: break;
+    }
+}
+
+// Every row of A, assembled once before the factorisation and parked in the
+// L-factor column of the same index: row q's nine diagonal values go to
+// Lf[q][0..8] (as FP64, also when the factors are FP32).  local_factor_rw_kernel
+// reads row q at column q-kl-1 (or for the first window) and writes L column q
+// only at column q, so the parked row is always read before it is overwritten.
+template <typename T>
+__device__ __forceinline__ double* frw_row_slot(const LocalArgs& a, size_t u)
+{
+    if constexpr (sizeof(T) == sizeof(float)) return (double*)(a.Lf32 + u * a.klp32);
+    else return a.Lf + u * a.klp;
+}
+
+template <typename T>
+__global__ void local_rows_kernel(LocalArgs a)
+{
+    const int sys = blockIdx.y;
+    if (skip_system(a, sys)) return;
+    const int n = a.d.V * (a.d.K - sys_k0(a, sys));
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const SysView v = sys_view(a, sys);
+    int types[4] = {a.Vl_t, a.Vu_t, a.Kl_t, a.Ku_t};
+    double r[9];
+    const int st = assemble_row(v, types, a.dt, q, r);
+    if (st) set_error(a.status, st);
+    double* dst = frw_row_slot<T>(a, sys_uoff(a, sys) + q);
+#pragma unroll
+    for (int s2 = 0; s2 < 9; s2++) dst[s2] = r[s2];
+}
+
+__device__ __forceinline__ void cp_async_8(double* dst, const double* src)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void frw_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void frw_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+template <typename T, int NR, int NC, int NW>
+__global__ void __launch_bounds__(NW * 32, 1) local_factor_rw_kernel(LocalArgs a)
+{
+    extern __shared__ double sm[];
+    const int sys = blockIdx.x;
+    if (skip_system(a, sys)) return;
+    const int nx = a.d.V;
+    const int n = a.d.V * (a.d.K - sys_k0(a, sys));
+    const size_t u0 = sys_uoff(a, sys);
+    const int kl = a.kl, ku = a.kl, kv = a.kv;
+    const int RW = kl + 1;          // window rows
+    const int CW = kv + 1;          // window columns
+    double* stage = sm;             // [2 STAGE_ROWS][9] ring of parked rows
+    double* rowA = stage + (size_t)2 * STAGE_ROWS * 9;  // [CW] row j before the swap
+    double* rowB = rowA + CW;       // [CW] the pivot row (row j after the swap)
+    double* colv = rowB + CW;       // [2][RW] column j by offset, by parity of j
+    __shared__ double s_best[NW];
+    __shared__ int s_bi[NW];
+    const bool f32 = sizeof(T) == sizeof(float);
+    const int klp = f32 ? a.klp32 : a.klp, kvp = f32 ? a.kvp32 : a.kvp;
+    T* Lf = (f32 ? (T*)a.Lf32 : (T*)a.Lf) + u0 * klp;
+    T* Uf = (f32 ? (T*)a.Uf32 : (T*)a.Uf) + u0 * kvp;
+    int32_t* ip = a.ipiv + u0;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+
+    // rows 256 b .. 256 b + 255 (parked by local_rows_kernel) into ring half
+    // b % 2, asynchronously
+    const double* rows = frw_row_slot<T>(a, u0);
+    const size_t rstride = f32 ? (size_t)a.klp32 / 2 : (size_t)a.klp;  // doubles
+    auto fetch_block = [&](int b) {
+        const int q0 = b * STAGE_ROWS;
+        const int cnt = min(STAGE_ROWS, n - q0) * 9;
+        for (int e = tid; e < cnt; e += blockDim.x) {
+            const int q = q0 + e / 9, s2 = e - (e / 9) * 9;
+            cp_async_8(stage + (size_t)(q & (2 * STAGE_ROWS - 1)) * 9 + s2, rows + q * rstride + s2);
+        }
+        frw_commit();
+    };
+    auto row_value = [&](int q, int col) -> double {
+        const int d = col - q;
+        const int dy = (d < -1) ? -1 : (d > 1 ? 1 : 0);
+        const int dx = d - dy * nx;
+        if (dx < -1 || dx > 1 || col < 0 || col >= n) return 0.0;
+        return stage[(q & (2 * STAGE_ROWS - 1)) * 9 + dslot(dx, dy)];
+    };
+
+    double R[NR][NC];
+    fetch_block(0);
+    if (n > STAGE_ROWS) fetch_block(1);
+    frw_wait_all();
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < NR; q++)
+#pragma unroll
+        for (int k = 0; k < NC; k++) {
+            const int rs = wid + NW * q, cs = lane + 32 * k;
+            R[q][k] = (rs < RW && cs < CW && rs < n) ? row_value(rs, cs) : 0.0;
+        }
+
+    int ju = 0;
+    int rj = 0, cj = 0;   // window slots of row j and column j (j mod RW, j mod CW)
+    for (int j = 0; j < n; j++) {
+        const int km = min(kl, n - 1 - j);
+        const int lc = cj & 31, kc = cj >> 5;
+        double* cv = colv + (j & 1) * RW;
+        // [top] this warp's candidate pivot in column j
+        if (lane == lc) {
+            double best = -1.0;
+            int bi = 1 << 30;
+            frw_col(R, kc, [&](int q, double& val) {
+                const int rs = wid + NW * q;
+                int i = rs - rj;
+                if (i < 0) i += RW;
+                if (rs < RW && i <= km) {
+                    cv[i] = val;
+                    const double av = fabs(val);
+                    if (av > best || (av == best && i < bi)) {
+                        best = av;
+                        bi = i;
+                    }
+                }
+            });
+            s_best[wid] = best;
+            s_bi[wid] = bi;
+        }
+        __syncthreads();
+        // [B1] the pivot, the multipliers, the rows of the swap.  The NW
+        // candidates are combined by shuffles in every warp (lanes 0..NW-1
+        // hold them; the other lanes of each group carry empty candidates).
+        double best = lane < NW ? s_best[lane] : -1.0;
+        int jp = lane < NW ? s_bi[lane] : 1 << 30;
+        constexpr int GROUP = NW > 16 ? 32 : (NW > 8 ? 16 : 8);  // power of two >= NW
+#pragma unroll
+        for (int o = GROUP / 2; o > 0; o >>= 1) {
+            const double b = __shfl_xor_sync(0xffffffffu, best, o);
+            const int bi = __shfl_xor_sync(0xffffffffu, jp, o);
+            if (b > best || (b == best && bi < jp)) {
+                best = b;
+                jp = bi;
+            }
+        }
+        jp = __shfl_sync(0xffffffffu, jp, 0);
+        // idamax: a NaN first element is the maximum (nothing compares
+        // greater), elsewhere NaN never is
+        const double c0 = cv[0];
+        if (c0 != c0 || jp > km) jp = 0;
+        const double piv = cv[jp];
+        const bool nz = piv != 0.0;
+        const bool swap = nz && jp != 0;
+        const int rp = rj + jp < RW ? rj + jp : rj + jp - RW;
+        if (tid == 0) ip[j] = j + jp;
+        double rcp = 0.0;
+        if (nz) {
+            ju = max(ju, min(j + ku + jp, n - 1));
+            rcp = 1.0 / piv;
+            for (int i = 1 + tid; i <= km; i += blockDim.x) {
+                const double val = (i == jp) ? c0 : cv[i];
+                Lf[(size_t)j * klp + (i - 1)] = (T)(val * rcp);
+            }
+        } else {
+            if (tid == 0) set_error(a.status, VERB_ERR_PIVOT);
+            for (int i = 1 + tid; i <= km; i += blockDim.x) Lf[(size_t)j * klp + (i - 1)] = (T)cv[i];
+        }
+        const bool own_j = wid == rj % NW;
+        const bool own_p = swap && wid == rp % NW;
+        const int qj = rj / NW, qp = rp / NW;
+        auto post = [&](double* dst) {
+            return [&, dst](double (&row)[NC]) {
+#pragma unroll
+                for (int k = 0; k < NC; k++) {
+                    const int cs = lane + 32 * k;
+                    if (cs < CW) dst[cs] = row[k];
+                }
+            };
+        };
+        if (own_j) frw_row(R, qj, post(swap ? rowA : rowB));
+        if (own_p) frw_row(R, qp, post(rowB));
+        __syncthreads();
+        // [B2] swap, U row j, rank-1 update, slide
+        const int ncol = ju - j;   // columns j+1..ju take the update
+        int cofs[NC];              // column offset c - j of each owned slot
+#pragma unroll
+        for (int k = 0; k < NC; k++) {
+            int c = lane + 32 * k - cj;
+            if (c < 0) c += CW;
+            cofs[k] = c;
+        }
+        if (swap) {
+            auto take = [&](const double* src) {
+                return [&, src](double (&row)[NC]) {
+#pragma unroll
+                    for (int k = 0; k < NC; k++) {
+                        const int cs = lane + 32 * k;
+                        if (cs < CW && cofs[k] <= ncol) row[k] = src[cs];
+                    }
+                };
+            };
+            if (own_j) frw_row(R, qj, take(rowB));
+            if (own_p) frw_row(R, qp, take(rowA));
+        }
+        for (int c = j + tid; c <= ju && c <= j + kv; c += blockDim.x) {
+            const int cs = cj + (c - j) < CW ? cj + (c - j) : cj + (c - j) - CW;
+            Uf[(size_t)c * kvp + (kv - (c - j))] = (T)rowB[cs];
+        }
+        if (nz && km > 0 && ncol > 0) {
+            double ty[NC];
+#pragma unroll
+            for (int k = 0; k < NC; k++) {
+                const int cs = lane + 32 * k;
+                ty[k] = (cs < CW && cofs[k] >= 1 && cofs[k] <= ncol) ? -rowB[cs] : 0.0;
+            }
+#pragma unroll
+            for (int q = 0; q < NR; q++) {
+                const int rs = wid + NW * q;
+                int i = rs - rj;
+                if (i < 0) i += RW;
+                if (rs >= RW || i < 1 || i > km) continue;
+                const double m = ((i == jp) ? c0 : cv[i]) * rcp;
+                // xGER: A(i,k) + x(i)*temp, skipped where temp = 0 (as a
+                // select, so that the lanes do not diverge)
+#pragma unroll
+                for (int k = 0; k < NC; k++) {
+                    const double u = R[q][k] + m * ty[k];
+                    R[q][k] = ty[k] != 0.0 ? u : R[q][k];
+                }
+            }
+        }
+        const int qn = j + kl + 1;
+        if (qn < n && (qn & (STAGE_ROWS - 1)) == 0 && qn >= STAGE_ROWS) {
+            // block qn/256 (fetched one block ago) is needed from here on; the
+            // block before it is consumed, so its half takes the next block
+            frw_wait_all();
+            __syncthreads();
+            if (qn + STAGE_ROWS < n) fetch_block(qn / STAGE_ROWS + 1);
+        }
+        // column slot cj now holds column j+CW, zero in every row but the new one
+        if (lane == lc) frw_col(R, kc, [](int, double& val) { val = 0.0; });
+        // row slot rj <- row j+kl+1 over columns j+1..j+CW (slot cs holds
+        // column j+1+((cs-(j+1)) mod CW))
+        if (own_j)
+            frw_row(R, qj, [&](double (&row)[NC]) {
+#pragma unroll
+                for (int k = 0; k < NC; k++) {
+                    const int c = cofs[k] == 0 ? kv : cofs[k] - 1;  // offset from column j+1
+                    row[k] = (qn < n && lane + 32 * k < CW) ? row_value(qn, j + 1 + c) : 0.0;
+                }
+            });
+        if (++rj == RW) rj = 0;
+        if (++cj == CW) cj = 0;
+    }
+}
+
 // RHS = B o f + C in unknown order (src/MatrixSolver.cpp:309-320), through a
 // 32x32 shared-memory tile transpose of the [V][K] slab.
 __global__ void local_rhs_kernel(LocalArgs a, int from_work)
@@ -460,13 +774,18 @@ __device__ __forceinline__ void cp_wait()
 // trade depends on the grid, so the autotuner picks one per context.
 // The second group keeps the right-hand-side window in registers instead of
 // shared memory (local_solve_rw_kernel).
+// The last group caps the registers (at least minb CTAs per SM: 36 resident
+// systems per SM) so that a 48 x 101 grid's 4848 systems are resident in one
+// wave instead of 32 per SM and a tail of 112.
 struct SolveShape {
     int warps, fwd, bwd, rw;
+    int minb = 1;
 };
 constexpr SolveShape SOLVE_SHAPES[] = {
     {4, 4, 2, 0},  {4, 6, 3, 0},  {2, 6, 4, 0},  {2, 8, 6, 0},  {1, 8, 6, 0},  {1, 12, 8, 0},
     {1, 12, 10, 0}, {1, 16, 12, 0}, {1, 24, 16, 0},
-    {4, 4, 3, 1},  {4, 6, 4, 1},  {2, 8, 6, 1},  {2, 12, 8, 1}, {1, 12, 8, 1}, {1, 16, 12, 1}};
+    {4, 4, 3, 1},  {4, 6, 4, 1},  {2, 8, 6, 1},  {2, 12, 8, 1}, {1, 12, 8, 1}, {1, 16, 12, 1},
+    {4, 4, 2, 1, 9}, {2, 6, 3, 1, 18}};
 constexpr int N_SOLVE_SHAPES = sizeof(SOLVE_SHAPES) / sizeof(SOLVE_SHAPES[0]);
 constexpr int FWD_WIN = 128;   // >= kl + 1
 constexpr int BWD_WIN = 256;   // >= kv + 1
@@ -610,8 +929,8 @@ __global__ void __launch_bounds__(SOLVE_WARPS * 32) local_solve_kernel(LocalArgs
 // operations and their order are those of local_solve_kernel, so the result is
 // bit-identical; what changes is that the window no longer costs shared-memory
 // loads and stores per column, which the old kernel's column chain waited on.
-template <typename T, int SOLVE_WARPS, int FWD_DEPTH, int BWD_DEPTH, int FS, int BS>
-__global__ void __launch_bounds__(SOLVE_WARPS * 32) local_solve_rw_kernel(LocalArgs a, int nsys)
+template <typename T, int SOLVE_WARPS, int FWD_DEPTH, int BWD_DEPTH, int FS, int BS, int MINB>
+__global__ void __launch_bounds__(SOLVE_WARPS * 32, MINB) local_solve_rw_kernel(LocalArgs a, int nsys)
 {
     extern __shared__ double sm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -866,8 +1185,8 @@ __device__ __forceinline__ float mv_row(const float* A, const float* y, int n, i
 // o = (dy + 2) * 5 + (dx + 2).
 constexpr int PC_TAPS = 25;
 
-__device__ __forceinline__ float precond_row(const float* C, const float* dg, const float* v, int n,
-                                             int nx, int ny, int i)
+__device__ __forceinline__ float precond_row(const float* C, const float* w, int n, int nx, int ny,
+                                             int i)
 {
     const int iy = i / nx, ix = i - iy * nx;
     float acc = 0.f;
@@ -880,9 +1199,8 @@ __device__ __forceinline__ float precond_row(const float* C, const float* dg, co
             const int xx = ix + dx;
             if (xx < 0 || xx >= nx) continue;
             const int o = (dy + 2) * 5 + (dx + 2);
-            const int j = yy * nx + xx;
             const float c = C[(size_t)o * n + i] + (o == 12 ? 1.f : 0.f);
-            acc = fmaf(c, v[j] / dg[j], acc);
+            acc = fmaf(c, w[yy * nx + xx], acc);
         }
     }
     return acc;
@@ -1048,7 +1366,10 @@ __global__ void bicgstab_kernel(LocalArgs a, const float* A9, const float* Cp, c
         }
         __syncthreads();
         if (Cs) {
-            for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = precond_row(Cs, dg, p, n, nx, ny, i);
+            // M p = (I + C) D^-1 p: the scaled vector once (t is free here)
+            for (int i = threadIdx.x; i < n; i += blockDim.x) t[i] = p[i] / dg[i];
+            __syncthreads();
+            for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = precond_row(Cs, t, n, nx, ny, i);
             __syncthreads();
         }
         float rv = 0.f;
@@ -1073,8 +1394,9 @@ __global__ void bicgstab_kernel(LocalArgs a, const float* A9, const float* Cp, c
             break;
         }
         if (Cs) {
-            __syncthreads();  // every s entry is written before M reads its neighbours
-            for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = precond_row(Cs, dg, r, n, nx, ny, i);
+            for (int i = threadIdx.x; i < n; i += blockDim.x) t[i] = r[i] / dg[i];
+            __syncthreads();  // every scaled s entry is written before M reads its neighbours
+            for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = precond_row(Cs, t, n, nx, ny, i);
         } else {
             for (int i = threadIdx.x; i < n; i += blockDim.x) y[i] = r[i] / dg[i];  // z
         }
@@ -1367,8 +1689,56 @@ size_t local_factor_smem(int V)
     return ((size_t)(kl + 1) * (kv + 1) + 2 * (kl + 1) + STAGE_ROWS * 9) * sizeof(double);
 }
 
-void launch_local_factor(const LocalArgs& a, cudaStream_t s)
+namespace {
+
+template <typename T, int NR, int NC, int NW>
+void launch_factor_rw(const LocalArgs& a, cudaStream_t s)
 {
+    const int kl = a.d.V + 1, kv = 2 * kl;
+    dim3 g((a.d.V * a.d.K + 255) / 256, a.d.P * a.d.R);
+    local_rows_kernel<T><<<g, 256, 0, s>>>(a);
+    const size_t smem = ((size_t)2 * STAGE_ROWS * 9 + 2 * (kv + 1) + 2 * (kl + 1)) * sizeof(double);
+    allow_max_dynamic_smem((const void*)local_factor_rw_kernel<T, NR, NC, NW>);
+    local_factor_rw_kernel<T, NR, NC, NW><<<a.d.P * a.d.R, NW * 32, smem, s>>>(a);
+}
+
+// Eight warps hold the register window.  Twelve and sixteen warps (fewer
+// slots and instructions per thread) were measured no faster at V = 101
+// (1.20 s and 1.42 s against 1.19 s for 48 x 101 x 101 x 91): the column
+// chain, not the per-thread work, sets the time.
+constexpr int FRW_WARPS = 8;
+
+// Register window shape: NC = ceil((kv+1)/32) column slots per lane and
+// NR = ceil((kl+1)/8) row slots per thread, NR in {2 NC - 1, 2 NC} since
+// kv + 1 = 2 (kl+1) - 1.  NC <= 7 keeps the window in 255 registers
+// (V <= 110); wider bands take local_factor_kernel.
+template <typename T>
+bool launch_factor_rw_t(const LocalArgs& a, cudaStream_t s)
+{
+    const int RW = a.d.V + 2, CW = 2 * (a.d.V + 1) + 1;
+    const int nc = (CW + 31) / 32, nr = (RW + FRW_WARPS - 1) / FRW_WARPS;
+    if (nc > 7 || (nr != 2 * nc && nr != 2 * nc - 1)) return false;
+    // a parked row needs 9 doubles of an L column; systems index grid.y of
+    // the parking launch
+    if (a.factors32 ? a.klp32 < 18 : a.klp < 9) return false;
+    if (a.d.P * a.d.R > 65535) return false;
+#define VERB_FRW(NR, NC)                                                              \
+    if (nc == NC && nr == NR) {                                                       \
+        launch_factor_rw<T, NR, NC, FRW_WARPS>(a, s);                                 \
+        return true;                                                                  \
+    }
+    VERB_FRW(1, 1) VERB_FRW(2, 1) VERB_FRW(3, 2) VERB_FRW(4, 2) VERB_FRW(5, 3) VERB_FRW(6, 3)
+    VERB_FRW(7, 4) VERB_FRW(8, 4) VERB_FRW(9, 5) VERB_FRW(10, 5) VERB_FRW(11, 6) VERB_FRW(12, 6)
+    VERB_FRW(13, 7) VERB_FRW(14, 7)
+#undef VERB_FRW
+    return false;
+}
+
+}  // namespace
+
+int launch_local_factor(const LocalArgs& a, cudaStream_t s)
+{
+    if (a.factors32 ? launch_factor_rw_t<float>(a, s) : launch_factor_rw_t<double>(a, s)) return 2;
     const size_t smem = local_factor_smem(a.d.V);
     if (a.factors32) {
         allow_max_dynamic_smem((const void*)local_factor_kernel<float>);
@@ -1377,6 +1747,7 @@ void launch_local_factor(const LocalArgs& a, cudaStream_t s)
         allow_max_dynamic_smem((const void*)local_factor_kernel<double>);
         local_factor_kernel<double><<<a.d.P * a.d.R, FACT_THREADS, smem, s>>>(a);
     }
+    return 1;
 }
 
 void launch_local_rhs(const LocalArgs& a, bool from_work, cudaStream_t s)
@@ -1393,7 +1764,7 @@ void launch_local_store(const LocalArgs& a, cudaStream_t s)
 
 namespace {
 
-template <typename T, int W, int FD, int BD, int RW>
+template <typename T, int W, int FD, int BD, int RW, int MB>
 void launch_solve_t(const LocalArgs& a, const size_t kl_p, const size_t kv_p, cudaStream_t s)
 {
     const int nsys = a.d.P * a.d.R;
@@ -1407,8 +1778,8 @@ void launch_solve_t(const LocalArgs& a, const size_t kl_p, const size_t kv_p, cu
             sizeof(double);
 #define VERB_RW(F, B)                                                                         \
     if (fs <= F && bs <= B) {                                                                 \
-        allow_max_dynamic_smem((const void*)local_solve_rw_kernel<T, W, FD, BD, F, B>);       \
-        local_solve_rw_kernel<T, W, FD, BD, F, B><<<grid, W * 32, smem, s>>>(a, nsys);        \
+        allow_max_dynamic_smem((const void*)local_solve_rw_kernel<T, W, FD, BD, F, B, MB>);   \
+        local_solve_rw_kernel<T, W, FD, BD, F, B, MB><<<grid, W * 32, smem, s>>>(a, nsys);    \
         return;                                                                               \
     }
         VERB_RW(1, 1)
@@ -1436,7 +1807,7 @@ void launch_solve_v(const LocalArgs& a, int v, size_t klp, size_t kvp, cudaStrea
 #define VERB_SOLVE_CASE(i)                                                                \
     case i:                                                                               \
         launch_solve_t<T, SOLVE_SHAPES[i].warps, SOLVE_SHAPES[i].fwd, SOLVE_SHAPES[i].bwd, \
-                       SOLVE_SHAPES[i].rw>(a, klp, kvp, s);                               \
+                       SOLVE_SHAPES[i].rw, SOLVE_SHAPES[i].minb>(a, klp, kvp, s);         \
         break;
         VERB_SOLVE_CASE(1)
         VERB_SOLVE_CASE(2)
@@ -1452,16 +1823,18 @@ void launch_solve_v(const LocalArgs& a, int v, size_t klp, size_t kvp, cudaStrea
         VERB_SOLVE_CASE(12)
         VERB_SOLVE_CASE(13)
         VERB_SOLVE_CASE(14)
+        VERB_SOLVE_CASE(15)
+        VERB_SOLVE_CASE(16)
 #undef VERB_SOLVE_CASE
         default:
             launch_solve_t<T, SOLVE_SHAPES[0].warps, SOLVE_SHAPES[0].fwd, SOLVE_SHAPES[0].bwd,
-                           SOLVE_SHAPES[0].rw>(a, klp, kvp, s);
+                           SOLVE_SHAPES[0].rw, 1>(a, klp, kvp, s);
     }
 }
 
 }  // namespace
 
-static_assert(N_SOLVE_SHAPES == 15, "launch_solve_v lists every shape");
+static_assert(N_SOLVE_SHAPES == 17, "launch_solve_v lists every shape");
 
 int local_solve_variants() { return N_SOLVE_SHAPES; }
 

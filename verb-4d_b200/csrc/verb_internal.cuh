@@ -149,7 +149,8 @@ struct LocalArgs {
     int* status;
 };
 size_t local_factor_smem(int V);
-void launch_local_factor(const LocalArgs& a, cudaStream_t s);
+// returns the number of kernels launched
+int launch_local_factor(const LocalArgs& a, cudaStream_t s);
 void launch_local_rhs(const LocalArgs& a, bool from_work, cudaStream_t s);
 void launch_local_solve(const LocalArgs& a, cudaStream_t s);
 int local_solve_variants();
