@@ -19,8 +19,8 @@ inside the FP64 refinement of verb_local_krylov.
   its BiCGSTAB needs fewer iterations per Krylov-solved system than Jacobi's.
   Measured on a B200 (12 epochs, 2.3 s of training): loss 0.242 -> 0.112;
   124 iterations per solved system against 216 with Jacobi, fallback rate
-  2.3 % against 18.2 %; local step 38.6 ms against 16.4 ms (Jacobi) and
-  15.4 ms for the banded LU with its factorisation.  The network's forward
+  2.2 % against 18.2 %; local step 28.3 ms against 17.5 ms (Jacobi) and
+  8.3 ms for the banded LU with its factorisation.  The network's forward
   pass and the 25-tap apply cost more than the iterations save, so the LU
   stays the production form.
 """
