@@ -5,7 +5,9 @@
  * baseline leg are its only users.  It is never part of the product path.
  * Each function restates a reference routine (file:line within the reference
  * project) with the reference's evaluation order; it is compiled with
- * -ffp-contract=off so no FMA contraction changes rounding.
+ * -ffp-contract=off so no FMA contraction changes rounding.  The one fused
+ * multiply-add written out is the rank-1 update of the banded LU (orc_gbtrf),
+ * where the reference's BLAS (dger in an FMA-using OpenBLAS build) fuses too.
  *
  * Parity pin: tests/test_oracle.py compares every routine here with the
  * reference routines compiled from source (oracle/_ref, see oracle/Makefile)
@@ -254,7 +256,10 @@ void orc_band_pack(const double* diag, int nx, int ny, double* ab)
 
 /* Banded LU with partial pivoting: restatement of LAPACK's published
  * unblocked algorithm xGBTF2 (0-based; ipiv 0-based).  Returns info (0 ok,
- * j+1 for an exactly zero pivot in column j). */
+ * j+1 for an exactly zero pivot in column j).  The rank-1 update
+ * A(i,k) += x(i)*temp (xGER, skipped where temp = 0) is one fused
+ * multiply-add per element, C99 fma(): rounded once, so every platform with
+ * an IEEE fma gives the same bits. */
 long orc_gbtrf(long n, long kl, long ku, double* ab, long ldab, long* ipiv)
 {
     long kv = ku + kl, info = 0, ju = 0;
@@ -291,7 +296,8 @@ long orc_gbtrf(long n, long kl, long ku, double* ab, long ldab, long* ipiv)
                     double yk = AB(kv - k, j + k);
                     if (yk != 0.0) {
                         double temp = -yk;
-                        for (long i = 1; i <= km; i++) AB(kv + i - k, j + k) += AB(kv + i, j) * temp;
+                        for (long i = 1; i <= km; i++)
+                            AB(kv + i - k, j + k) = fma(AB(kv + i, j), temp, AB(kv + i - k, j + k));
                     }
                 }
             }

@@ -133,6 +133,35 @@ def test_cfg1_step_bitexact(gpu, oracle_lib):
     c.close()
 
 
+def test_wide_band_local_step_bitexact(gpu, oracle_lib):
+    """V = 112 energies (band kl = 113): wider than the register-window
+    factorisation holds, so the shared-memory-window kernel factors; one local
+    step on every system, pivots and PSD equal to the oracle bit for bit."""
+    wl = W.make_workload(W.GridSpec(2, 3, 112, 4), seed=6, sources=True, losses=True)
+    f = wl.fields
+    P, R, V, K = wl.spec.shape
+    c = load_ctx(wl)
+    psd0 = c.download()
+    c.local(wl.dt, wl.sub_dt)
+    c.sync()
+    psd1 = c.download()
+    piv = c.local_pivots()
+    c.close()
+    n = V * K
+    ldab = 3 * (V + 1) + 1
+    for iP in range(P):
+        for iR in range(R):
+            s2 = lambda a: a[iP, iR]  # noqa: E731
+            lu, ip = np.zeros(ldab * n), np.zeros(n, np.int64)
+            _, ref = oracle_lib.diffusion_2d(s2(psd0), s2(f["Vg"]), s2(f["Kg"]), f["Vl"][iP, iR],
+                                             f["Vu"][iP, iR], f["Kl"][iP, iR], f["Ku"][iP, iR],
+                                             (1, 1, 2, 2), s2(f["DVV"]), s2(f["DKK"]), s2(f["DVK"]),
+                                             s2(f["DVK"]), s2(f["G_local"]), s2(f["S"]),
+                                             s2(f["loss_local"]), wl.dt, wl.sub_dt, lu=lu, ipiv=ip)
+            assert np.array_equal(piv[iP, iR], ip), (iP, iR)
+            assert np.array_equal(psd1[iP, iR], ref), (iP, iR)
+
+
 def test_dll_scale_matches_scaled_field(gpu):
     # UpdatableMatrix scale (src/UpdatableMatrix.cpp:698-708): base * scale
     wl = W.make_workload(W.GridSpec(6, 12, 5, 5), seed=8)

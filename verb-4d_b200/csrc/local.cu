@@ -13,7 +13,8 @@
 //  * local_factor_kernel: one CTA per system.  Rows of A are assembled on the
 //    device with the reference's operation order (bit-identical matrix) and
 //    factored by the unblocked banded LU of LAPACK's xGBTF2 (partial pivoting,
-//    multipliers scaled by the reciprocal pivot, rank-1 updates).
+//    multipliers scaled by the reciprocal pivot, rank-1 updates as fused
+//    multiply-adds).
 //    The active (kl+1) x (kv+1) window lives in shared memory as a circular
 //    buffer over rows and columns.  Output: L multipliers (Lf, column j
 //    contiguous), U columns (Uf, rows j-kv..j contiguous) and 0-based pivots.
@@ -34,7 +35,9 @@
 //
 // All arithmetic follows the CPU restatement of xGBTF2/xGBTRS/xTBSV operation
 // by operation without FMA contraction (the file is compiled with
-// -fmad=false), so factors, pivots and solutions are bit-identical to it.
+// -fmad=false) except the factorisation's rank-1 update, which both compute
+// as one fused multiply-add per element (fma()), so factors, pivots and
+// solutions are bit-identical to it.
 #include "verb_internal.cuh"
 
 namespace verb {
@@ -336,7 +339,7 @@ __global__ void __launch_bounds__(FACT_THREADS) local_factor_kernel(LocalArgs a)
                 for (int k = 0; k < FACT_COLS; k++)
                     if (ty[k] != 0.0) {
                         double* w = Wr + csl[k];
-                        *w = *w + m * ty[k];  // xGER: A(i,k) + x(i)*temp, temp = -y(k)
+                        *w = fma(m, ty[k], *w);  // xGER: A(i,k) + x(i)*temp, temp = -y(k), fused
                     }
                 r += nw;
                 while (r >= RW) r -= RW;
@@ -382,8 +385,9 @@ __global__ void __launch_bounds__(FACT_THREADS) local_factor_kernel(LocalArgs a)
 // The row and column slots of the pivot step are reached through a switch on
 // their index (registers cannot be indexed at run time), so only the rank-1
 // update touches every slot.  Every element sees the same operations in the
-// same order as in local_factor_kernel (LAPACK's xGBTF2 without FMA): factors
-// and pivots are bit-identical, and the update costs no shared-memory traffic.
+// same order as in local_factor_kernel (LAPACK's xGBTF2, the rank-1 update
+// fused): factors and pivots are bit-identical, and the update costs no
+// shared-memory traffic.
 // f(R[q]) for a run-time q < NR
 template <int NR, int NC, typename F>
 __device__ __forceinline__ void frw_row(double (&R)[NR][NC], int q, F&& f)
@@ -527,8 +531,11 @@ __global__ void __launch_bounds__(NW * 32, 1) local_factor_rw_kernel(LocalArgs a
         double* cv = colv + (j & 1) * RW;
         // [top] this warp's candidate pivot in column j
         if (lane == lc) {
-            double best = -1.0;
-            int bi = 1 << 30;
+            // four interleaved first-maximum chains (rows q mod 4), merged at
+            // the end with the same rule: a shorter dependency chain than one
+            // pass over the thirteen rows
+            double best[4] = {-1.0, -1.0, -1.0, -1.0};
+            int bi[4] = {1 << 30, 1 << 30, 1 << 30, 1 << 30};
             frw_col(R, kc, [&](int q, double& val) {
                 const int rs = wid + NW * q;
                 int i = rs - rj;
@@ -536,14 +543,20 @@ __global__ void __launch_bounds__(NW * 32, 1) local_factor_rw_kernel(LocalArgs a
                 if (rs < RW && i <= km) {
                     cv[i] = val;
                     const double av = fabs(val);
-                    if (av > best || (av == best && i < bi)) {
-                        best = av;
-                        bi = i;
+                    if (av > best[q & 3] || (av == best[q & 3] && i < bi[q & 3])) {
+                        best[q & 3] = av;
+                        bi[q & 3] = i;
                     }
                 }
             });
-            s_best[wid] = best;
-            s_bi[wid] = bi;
+#pragma unroll
+            for (int c = 1; c < 4; c++)
+                if (best[c] > best[0] || (best[c] == best[0] && bi[c] < bi[0])) {
+                    best[0] = best[c];
+                    bi[0] = bi[c];
+                }
+            s_best[wid] = best[0];
+            s_bi[wid] = bi[0];
         }
         __syncthreads();
         // [B1] the pivot, the multipliers, the rows of the swap.  The NW
@@ -638,11 +651,12 @@ __global__ void __launch_bounds__(NW * 32, 1) local_factor_rw_kernel(LocalArgs a
                 if (i < 0) i += RW;
                 if (rs >= RW || i < 1 || i > km) continue;
                 const double m = ((i == jp) ? c0 : cv[i]) * rcp;
-                // xGER: A(i,k) + x(i)*temp, skipped where temp = 0 (as a
-                // select, so that the lanes do not diverge)
+                // xGER: A(i,k) + x(i)*temp with temp = -y(k), one fused
+                // multiply-add, skipped where temp = 0 (as a select, so that
+                // the lanes do not diverge)
 #pragma unroll
                 for (int k = 0; k < NC; k++) {
-                    const double u = R[q][k] + m * ty[k];
+                    const double u = fma(m, ty[k], R[q][k]);
                     R[q][k] = ty[k] != 0.0 ? u : R[q][k];
                 }
             }
@@ -785,7 +799,7 @@ constexpr SolveShape SOLVE_SHAPES[] = {
     {4, 4, 2, 0},  {4, 6, 3, 0},  {2, 6, 4, 0},  {2, 8, 6, 0},  {1, 8, 6, 0},  {1, 12, 8, 0},
     {1, 12, 10, 0}, {1, 16, 12, 0}, {1, 24, 16, 0},
     {4, 4, 3, 1},  {4, 6, 4, 1},  {2, 8, 6, 1},  {2, 12, 8, 1}, {1, 12, 8, 1}, {1, 16, 12, 1},
-    {4, 4, 2, 1, 9}, {2, 6, 3, 1, 18}};
+    {4, 4, 2, 1, 9}, {2, 6, 3, 1, 18}, {4, 6, 3, 1, 9}};
 constexpr int N_SOLVE_SHAPES = sizeof(SOLVE_SHAPES) / sizeof(SOLVE_SHAPES[0]);
 constexpr int FWD_WIN = 128;   // >= kl + 1
 constexpr int BWD_WIN = 256;   // >= kv + 1
@@ -1825,6 +1839,7 @@ void launch_solve_v(const LocalArgs& a, int v, size_t klp, size_t kvp, cudaStrea
         VERB_SOLVE_CASE(14)
         VERB_SOLVE_CASE(15)
         VERB_SOLVE_CASE(16)
+        VERB_SOLVE_CASE(17)
 #undef VERB_SOLVE_CASE
         default:
             launch_solve_t<T, SOLVE_SHAPES[0].warps, SOLVE_SHAPES[0].fwd, SOLVE_SHAPES[0].bwd,
@@ -1834,7 +1849,7 @@ void launch_solve_v(const LocalArgs& a, int v, size_t klp, size_t kvp, cudaStrea
 
 }  // namespace
 
-static_assert(N_SOLVE_SHAPES == 17, "launch_solve_v lists every shape");
+static_assert(N_SOLVE_SHAPES == 18, "launch_solve_v lists every shape");
 
 int local_solve_variants() { return N_SOLVE_SHAPES; }
 
