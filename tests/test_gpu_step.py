@@ -134,10 +134,11 @@ def test_cfg1_step_bitexact(gpu, oracle_lib):
 
 
 def test_wide_band_local_step_bitexact(gpu, oracle_lib):
-    """V = 112 energies (band kl = 113): wider than the register-window
-    factorisation holds, so the shared-memory-window kernel factors; one local
-    step on every system, pivots and PSD equal to the oracle bit for bit."""
-    wl = W.make_workload(W.GridSpec(2, 3, 112, 4), seed=6, sources=True, losses=True)
+    """V = 111 energies (band kl = 112, the widest the context accepts): wider
+    than the register-window factorisation holds, so the shared-memory-window
+    kernel factors; one local step on every system, pivots and PSD equal to the
+    oracle bit for bit."""
+    wl = W.make_workload(W.GridSpec(2, 3, 111, 4), seed=6, sources=True, losses=True)
     f = wl.fields
     P, R, V, K = wl.spec.shape
     c = load_ctx(wl)

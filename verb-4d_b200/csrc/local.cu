@@ -377,11 +377,13 @@ __global__ void __launch_bounds__(FACT_THREADS) local_factor_kernel(LocalArgs a)
 //         column and their warp's candidate;
 //   B1    every thread combines the NW candidates (idamax: first maximum,
 //         NaN skipped unless it is the first entry); the multipliers go to
-//         Lf; the owners of row j and of the pivot row post them;
+//         Lf; every thread forms one window slot of the row that enters at
+//         the next column; the owners of row j and of the pivot row post them;
 //   B2    the swap over columns j..ju in the owners' registers, U row j out,
 //         the rank-1 update of every owned slot (multipliers from the posted
 //         column, the pivot row from shared memory), and the slide: column
-//         slot j % CW is cleared, row slot j % RW takes row j+kl+1.
+//         slot j % CW is cleared, row slot j % RW takes row j+kl+1 (formed at
+//         the previous column).
 // The row and column slots of the pivot step are reached through a switch on
 // their index (registers cannot be indexed at run time), so only the rank-1
 // update touches every slot.  Every element sees the same operations in the
@@ -480,6 +482,7 @@ __global__ void __launch_bounds__(NW * 32, 1) local_factor_rw_kernel(LocalArgs a
     double* rowA = stage + (size_t)2 * STAGE_ROWS * 9;  // [CW] row j before the swap
     double* rowB = rowA + CW;       // [CW] the pivot row (row j after the swap)
     double* colv = rowB + CW;       // [2][RW] column j by offset, by parity of j
+    double* nrow = colv + 2 * RW;   // [2][CW] the window row that enters at column j, by parity
     __shared__ double s_best[NW];
     __shared__ int s_bi[NW];
     const bool f32 = sizeof(T) == sizeof(float);
@@ -515,6 +518,17 @@ __global__ void __launch_bounds__(NW * 32, 1) local_factor_rw_kernel(LocalArgs a
     if (n > STAGE_ROWS) fetch_block(1);
     frw_wait_all();
     __syncthreads();
+    // the row entering at column jj (row jj+kl+1) over window slots: slot cs
+    // holds column jj+1+((cs-(jj+1)) mod CW); cjj = jj mod CW
+    auto fill_row = [&](int jj, int cjj) {
+        const int qr = jj + kl + 1;
+        for (int cs = tid; cs < CW; cs += blockDim.x) {
+            int c = cs - cjj - 1;
+            if (c < 0) c += CW;
+            nrow[(jj & 1) * CW + cs] = qr < n ? row_value(qr, jj + 1 + c) : 0.0;
+        }
+    };
+    fill_row(0, 0);
 #pragma unroll
     for (int q = 0; q < NR; q++)
 #pragma unroll
@@ -533,7 +547,7 @@ __global__ void __launch_bounds__(NW * 32, 1) local_factor_rw_kernel(LocalArgs a
         if (lane == lc) {
             // four interleaved first-maximum chains (rows q mod 4), merged at
             // the end with the same rule: a shorter dependency chain than one
-            // pass over the thirteen rows
+            // pass over the thread's NR rows
             double best[4] = {-1.0, -1.0, -1.0, -1.0};
             int bi[4] = {1 << 30, 1 << 30, 1 << 30, 1 << 30};
             frw_col(R, kc, [&](int q, double& val) {
@@ -595,6 +609,16 @@ __global__ void __launch_bounds__(NW * 32, 1) local_factor_rw_kernel(LocalArgs a
         } else {
             if (tid == 0) set_error(a.status, VERB_ERR_PIVOT);
             for (int i = 1 + tid; i <= km; i += blockDim.x) Lf[(size_t)j * klp + (i - 1)] = (T)cv[i];
+        }
+        {
+            // next column's entering row; its ring block must be present
+            const int qf = j + 1 + kl + 1;
+            if (j + 1 < n && qf < n && (qf & (STAGE_ROWS - 1)) == 0 && qf >= STAGE_ROWS) {
+                frw_wait_all();
+                __syncthreads();
+                if (qf + STAGE_ROWS < n) fetch_block(qf / STAGE_ROWS + 1);
+            }
+            if (j + 1 < n) fill_row(j + 1, cj + 1 == CW ? 0 : cj + 1);
         }
         const bool own_j = wid == rj % NW;
         const bool own_p = swap && wid == rp % NW;
@@ -661,14 +685,6 @@ __global__ void __launch_bounds__(NW * 32, 1) local_factor_rw_kernel(LocalArgs a
                 }
             }
         }
-        const int qn = j + kl + 1;
-        if (qn < n && (qn & (STAGE_ROWS - 1)) == 0 && qn >= STAGE_ROWS) {
-            // block qn/256 (fetched one block ago) is needed from here on; the
-            // block before it is consumed, so its half takes the next block
-            frw_wait_all();
-            __syncthreads();
-            if (qn + STAGE_ROWS < n) fetch_block(qn / STAGE_ROWS + 1);
-        }
         // column slot cj now holds column j+CW, zero in every row but the new one
         if (lane == lc) frw_col(R, kc, [](int, double& val) { val = 0.0; });
         // row slot rj <- row j+kl+1 over columns j+1..j+CW (slot cs holds
@@ -677,8 +693,8 @@ __global__ void __launch_bounds__(NW * 32, 1) local_factor_rw_kernel(LocalArgs a
             frw_row(R, qj, [&](double (&row)[NC]) {
 #pragma unroll
                 for (int k = 0; k < NC; k++) {
-                    const int c = cofs[k] == 0 ? kv : cofs[k] - 1;  // offset from column j+1
-                    row[k] = (qn < n && lane + 32 * k < CW) ? row_value(qn, j + 1 + c) : 0.0;
+                    const int cs = lane + 32 * k;
+                    row[k] = cs < CW ? nrow[(j & 1) * CW + cs] : 0.0;
                 }
             });
         if (++rj == RW) rj = 0;
@@ -1711,7 +1727,7 @@ void launch_factor_rw(const LocalArgs& a, cudaStream_t s)
     const int kl = a.d.V + 1, kv = 2 * kl;
     dim3 g((a.d.V * a.d.K + 255) / 256, a.d.P * a.d.R);
     local_rows_kernel<T><<<g, 256, 0, s>>>(a);
-    const size_t smem = ((size_t)2 * STAGE_ROWS * 9 + 2 * (kv + 1) + 2 * (kl + 1)) * sizeof(double);
+    const size_t smem = ((size_t)2 * STAGE_ROWS * 9 + 4 * (kv + 1) + 2 * (kl + 1)) * sizeof(double);
     allow_max_dynamic_smem((const void*)local_factor_rw_kernel<T, NR, NC, NW>);
     local_factor_rw_kernel<T, NR, NC, NW><<<a.d.P * a.d.R, NW * 32, smem, s>>>(a);
 }
