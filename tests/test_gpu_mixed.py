@@ -63,6 +63,17 @@ def test_mixed_local_solve_converges_to_fp64(gpu):
     assert corrs[1] > corrs[3]
 
 
+def test_mixed_production_band(gpu):
+    # the production band (V = 101, kl = 102: 13 x 7 register slots per thread)
+    # on short systems: FP32 factors parked and stored in the FP32 L/U arrays
+    wl = W.make_workload(W.GridSpec(4, 6, 101, 6), seed=7, sources=True, losses=True)
+    ref, piv, mem64, _ = local_steps(wl, "fp64", 0, steps=1)
+    psd, piv32, mem32, _ = local_steps(wl, "mixed", 10, steps=1)
+    assert np.array_equal(piv32, piv)
+    assert mem32 < mem64
+    assert rel(psd, ref) < MIXED_RTOL
+
+
 def test_fp64_refinement(gpu):
     # FP64 factors plus FP64 refinement: the corrections are at the FP64
     # path's rounding level and the result stays within it
