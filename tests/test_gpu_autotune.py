@@ -41,3 +41,34 @@ def test_shapes_identical_and_tuning_side_effect_free(gpu, form):
             ref = out
         assert np.array_equal(out, ref), v
     assert np.array_equal(tuned, ref)
+
+
+def test_every_shape_at_the_production_band(gpu, oracle_lib):
+    # V = 101 (kl = 102): the register-window shapes run with 4 / 7 slots per
+    # lane, the capped ones with 56 registers; all equal the oracle bit for bit
+    wl = W.make_workload(W.GridSpec(2, 3, 101, 5), seed=96, sources=True, losses=True)
+    f = wl.fields
+    P, R, V, K = wl.spec.shape
+    c = load_ctx(wl)
+    shapes = c.solve_variants()
+    psd0 = c.download()
+    c.close()
+    n, ldab = V * K, 3 * (V + 1) + 1
+    want = np.empty_like(psd0)
+    for iP in range(P):
+        for iR in range(R):
+            s2 = lambda a: a[iP, iR]  # noqa: E731
+            lu, ip = np.zeros(ldab * n), np.zeros(n, np.int64)
+            _, want[iP, iR] = oracle_lib.diffusion_2d(
+                s2(psd0), s2(f["Vg"]), s2(f["Kg"]), f["Vl"][iP, iR], f["Vu"][iP, iR],
+                f["Kl"][iP, iR], f["Ku"][iP, iR], (1, 1, 2, 2), s2(f["DVV"]), s2(f["DKK"]),
+                s2(f["DVK"]), s2(f["DVK"]), s2(f["G_local"]), s2(f["S"]), s2(f["loss_local"]),
+                wl.dt, wl.sub_dt, lu=lu, ipiv=ip)
+    for v in range(len(shapes)):
+        c = load_ctx(wl)
+        c.set_local_solve_variant(v)
+        c.local(wl.dt, wl.sub_dt)
+        c.sync()
+        out = c.download()
+        c.close()
+        assert np.array_equal(out, want), shapes[v]
