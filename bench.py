@@ -52,6 +52,13 @@ HBM_FALLBACK = 6650.0
 SOLVE_TRAFFIC_PER_ALG_BYTE = (9735437568 + 66170624) / 9698947584
 
 
+CONV_LABEL = {
+    "fma": "fma: multiply-add contraction, within 1e-12 of the reference per step",
+    "stream": ("stream: one thread per line, all stages of a pass in registers, multiply-add "
+               "contraction, within 1e-12 of the reference per step"),
+    "exact": "exact: bit-identical to the reference",
+}
+
 def rank_info():
     return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
             int(os.environ.get("LOCAL_RANK", "0")))
@@ -434,9 +441,7 @@ def run_ours(args):
         "impl": {"local_systems": "loss-cone trimmed (ragged)" if args.trim else "full",
                  "local_precision": args.form,
                  "step_launch": "CUDA graph replay" if args.graph else "eager launches",
-                 "convection_arith": ("fma: multiply-add contraction, within 1e-12 of the "
-                                      "reference per step" if args.conv == "fma" else
-                                      "exact: bit-identical to the reference")},
+                 "convection_arith": CONV_LABEL[args.conv]},
         "phases_ms_per_step": {"convection": round(conv_ms, 3),
                                "radial": round(tph["radial_ms"] / nph, 3),
                                "local_solve": round(tph["local_solve_ms"] / nph, 3),
@@ -931,8 +936,8 @@ def main():
     ap.add_argument("--graph", type=int, default=1, choices=[0, 1],
                     help="replay steady-state steps from a captured CUDA graph (1) or launch "
                          "them eagerly with per-phase events (0)")
-    ap.add_argument("--conv", default="fma", choices=["fma", "exact"],
-                    help="convection arithmetic: fma (contracted) or exact (bit-identical)")
+    ap.add_argument("--conv", default="fma", choices=["fma", "exact", "stream"],
+                    help="convection kernel: fma (contracted), stream (one thread per line, contracted) or exact (bit-identical)")
     ap.add_argument("--trim", action="store_true",
                     help="ragged local systems: pitch angles outside the loss cone only")
     ap.add_argument("--ensemble", action="store_true", help="run the member ensemble instead")

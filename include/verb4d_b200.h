@@ -267,10 +267,17 @@ int verb_autotune_local_solve(verb_ctx* ctx, double dt, double sub_dt, double* t
  * bit-identical to it (exp() of loss rates aside).  VERB_CONV_FMA runs the
  * same kernel compiled with multiply-add contraction (and nine warps per
  * block): about 18 % faster, and within a few units in the last place of the
- * exact form per step.  Convection_2D (src/Convection_2D.cpp:36-169) has one
- * arithmetic; the switch has no counterpart in the reference. */
+ * exact form per step.  VERB_CONV_STREAM runs one thread per line through all
+ * four stages of a pass at once (register windows, nothing staged between
+ * stages), contracted, with the G product and the loss/source epilogue
+ * applied as the sweeps store; it needs both sweeps (P and R >= 11) and
+ * otherwise runs the VERB_CONV_FMA kernel; within a few units in the last
+ * place of the reference per step.  Convection_2D
+ * (src/Convection_2D.cpp:36-169) has one arithmetic; the switch has no
+ * counterpart in the reference. */
 #define VERB_CONV_EXACT 0
 #define VERB_CONV_FMA 1
+#define VERB_CONV_STREAM 2
 int verb_set_convection_arith(verb_ctx* ctx, int mode);
 
 /* ---- Krylov form of the local (V,K) solve ----------------------------------

@@ -341,10 +341,20 @@ int conv_run(verb_ctx* c, double dt)
         int s = need_bc(c, b);
         if (s) return s;
     }
-    if (int s = (c->conv_arith == VERB_CONV_FMA ? conv_check_fma : conv_check)(d.P, d.R)) return s;
-    if (!c->conv_nctas) c->conv_nctas = std::max(conv_ctas(d.P, d.R), conv_ctas_fma(d.P, d.R));
-    CK(alloc((void**)&c->conv_scratch,
-             (size_t)c->conv_nctas * conv_scratch_doubles(d.P, d.R) * sizeof(double)));
+    // the streaming kernel needs both sweeps; other shapes run the contracted
+    // kernel of convection.cu
+    const bool stream = c->conv_arith == VERB_CONV_STREAM && conv_stream_check(d.P, d.R) == VERB_OK;
+    if (!stream)
+        if (int s = (c->conv_arith == VERB_CONV_EXACT ? conv_check : conv_check_fma)(d.P, d.R)) return s;
+    if (!c->conv_nctas) {
+        c->conv_nctas = std::max(conv_ctas(d.P, d.R), conv_ctas_fma(d.P, d.R));
+        // one allocation serves every arithmetic mode of the context
+        size_t b = (size_t)c->conv_nctas * conv_scratch_doubles(d.P, d.R);
+        if (conv_stream_check(d.P, d.R) == VERB_OK)
+            b = std::max(b, (size_t)conv_stream_ctas_max(d.P, d.R) * conv_stream_scratch_doubles(d.P, d.R));
+        c->conv_scratch_bytes = b * sizeof(double);
+    }
+    CK(alloc((void**)&c->conv_scratch, c->conv_scratch_bytes));
     CK(alloc((void**)&c->conv_substeps, (size_t)d.V * d.K * sizeof(int)));
     CK(alloc((void**)&c->ticket, sizeof(int)));
     ConvArgs a{};
@@ -372,10 +382,12 @@ int conv_run(verb_ctx* c, double dt)
     a.status = c->status;
     PhaseTimer t(c, PH_CONV);
     CK(cudaMemsetAsync(c->ticket, 0, sizeof(int), c->stream));
-    if (c->conv_arith == VERB_CONV_FMA)
-        launch_convection_fma(a, c->conv_nctas, c->stream);
-    else
+    if (stream)
+        launch_convection_stream(a, conv_stream_ctas(d.P, d.R), c->stream);
+    else if (c->conv_arith == VERB_CONV_EXACT)
         launch_convection(a, c->conv_nctas, c->stream);
+    else
+        launch_convection_fma(a, c->conv_nctas, c->stream);
     c->acc.kernel_launches++;
     return check_launch();
 }
@@ -545,8 +557,7 @@ int verb_device_bytes(const verb_ctx* c, size_t* bytes)
     if (c->kout) b += ns * sizeof(float);
     for (const double* p : {c->kb, c->kx, c->kr, c->kd}) if (p) b += ns * sizeof(double);
     if (c->kscale) b += nsys * sizeof(double);
-    if (c->conv_scratch)
-        b += (size_t)c->conv_nctas * conv_scratch_doubles(c->d.P, c->d.R) * sizeof(double);
+    if (c->conv_scratch) b += c->conv_scratch_bytes;
     if (c->Pa)
         b += (size_t)(c->pa_p_index >= 0 ? 1 : c->d.P) * c->d.V * c->d.K * c->d.R * c->d.R *
              sizeof(double);
@@ -837,7 +848,8 @@ int verb_autotune_local_solve(verb_ctx* c, double dt, double sub_dt, double* tim
 
 int verb_set_convection_arith(verb_ctx* c, int mode)
 {
-    if (!c || (mode != VERB_CONV_EXACT && mode != VERB_CONV_FMA)) return VERB_ERR_ARG;
+    if (!c || (mode != VERB_CONV_EXACT && mode != VERB_CONV_FMA && mode != VERB_CONV_STREAM))
+        return VERB_ERR_ARG;
     graph_invalidate(c);
     c->conv_arith = mode;
     return VERB_OK;
@@ -1632,7 +1644,10 @@ int verb_estimate_device_bytes(int P, int R, int V, int K, int precision, int re
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        b += (size_t)2 * sms * conv_scratch_doubles(P, R) * sizeof(double);
+        size_t cb = (size_t)2 * sms * conv_scratch_doubles(P, R);
+        if (conv_stream_check(P, R) == VERB_OK)
+            cb = std::max(cb, (size_t)conv_stream_ctas_max(P, R) * conv_stream_scratch_doubles(P, R));
+        b += cb * sizeof(double);
     }
     if (kf_columns > 0)
         b += ((size_t)kf_columns * R * R + np) * sizeof(double) +

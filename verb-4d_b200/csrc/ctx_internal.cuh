@@ -113,6 +113,7 @@ struct verb_ctx {
     int* conv_substeps = nullptr;
     int* ticket = nullptr;
     int conv_nctas = 0;
+    size_t conv_scratch_bytes = 0;  // for every arithmetic mode's kernel
     int conv_arith = VERB_CONV_EXACT;
     // reductions / status
     unsigned long long* red = nullptr;  // [0] negatives, [1] tensor min key

@@ -111,6 +111,12 @@ int conv_ctas_fma(int P, int R);
 int conv_check_fma(int P, int R);
 size_t conv_smem_bytes_fma(int P, int R);
 void launch_convection_fma(const ConvArgs& a, int nctas, cudaStream_t s);
+// one thread per line, streaming register windows (convection_stream.cu)
+int conv_stream_check(int P, int R);  // VERB_ERR_SIZE: the shape needs convection.cu
+size_t conv_stream_scratch_doubles(int P, int R);
+int conv_stream_ctas(int P, int R);
+int conv_stream_ctas_max(int P, int R);
+void launch_convection_stream(const ConvArgs& a, int nctas, cudaStream_t s);
 void launch_convection_line(double* psd, const double* x, int n, double lbc, double ubc, int lbc_t,
                             int ubc_t, const double* ux, double dt, int* status, cudaStream_t s);
 

@@ -21,7 +21,7 @@ STATUS_NAMES = {
     9: "VERB_ERR_GRID", 10: "VERB_TIMEOUT", 11: "VERB_ERR_SIZE", 12: "VERB_ERR_IO",
 }
 VERB_GUESS_ZERO, VERB_GUESS_PREV, VERB_GUESS_CNN = 0, 1, 2
-CONV_ARITH = {"exact": 0, "fma": 1}
+CONV_ARITH = {"exact": 0, "fma": 1, "stream": 2}
 GUESS_IDS = {"zero": VERB_GUESS_ZERO, "prev": VERB_GUESS_PREV, "cnn": VERB_GUESS_CNN}
 
 

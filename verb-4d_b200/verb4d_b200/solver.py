@@ -128,7 +128,10 @@ class Context:
 
     def set_convection_arith(self, mode: str = "exact"):
         """"exact": bit-identical to the reference; "fma": multiply-add
-        contraction, ~10 % faster, a few ulp per step from "exact"."""
+        contraction, ~18 % faster, a few ulp per step from "exact";
+        "stream": one thread per line, all stages of a pass at once in
+        registers, contracted like "fma" (needs P and R >= 11, else runs
+        the "fma" kernel)."""
         L.check(self.lib.verb_set_convection_arith(self.h, L.CONV_ARITH[mode]), "conv_arith")
 
     def local_krylov(self, dt: float, sub_dt: float, guess: str = "prev", cnn=None,
