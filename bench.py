@@ -126,11 +126,14 @@ class ClockSampler:
 
 
 FP64_OPS_PER_FACE = 179
-# FP64-pipe share of the contracted convection kernel's active cycles
-# (ncu sm__inst_executed_pipe_fp64, --set full capture of one launch at
-# 48 x 101 x 101 x 8); the op-count fraction above counts the reference's
-# operations, the pipe share the ones the kernel issues
-CONV_FP64_PIPE_NCU = 0.336
+# FP64-pipe share of each convection kernel's active cycles (ncu
+# sm__inst_executed_pipe_fp64 over one launch at 48 x 101 x 101 x 8); the
+# op-count fraction above counts the reference's operations, the pipe share
+# the ones the kernel issues
+CONV_FP64_PIPE_NCU = {"fma": 0.336, "stream": 0.351, "exact": 0.471}
+CONV_KERNEL = {"fma": "conv_fma::convection_kernel (nine warps per line job set)",
+               "stream": "convection_stream_kernel (one thread per line)",
+               "exact": "conv_exact::convection_kernel"}
 
 
 def fp64_peak_tops():
@@ -464,15 +467,15 @@ def run_ours(args):
                                         else "algorithmic bytes x 1.0106, the DRAM/algorithmic "
                                              "ratio of one ncu-captured launch at 48x101x101x8 "
                                              "(the 48x101x101x91 band, kl = 102)")},
-        "roofline_fp64": {"kernel": "convection_kernel (ULTIMATE-QUICKEST sweeps, FP64 vector)",
+        "roofline_fp64": {"kernel": CONV_KERNEL[args.conv] + ", ULTIMATE-QUICKEST sweeps, FP64",
                           "bound": "fp64", "achieved": round(conv_tops, 3), "peak": fp64_peak,
                           "unit": "TOP/s", "frac": round(conv_tops / fp64_peak, 4),
                           "peak_source": "nominal FP64 issue rate, 148 SMs x 64 lanes at "
                                          "MEASURED_PEAKS.json sm_max_mhz",
                           "fp64_ops_per_face": FP64_OPS_PER_FACE,
-                          "fp64_pipe_active_ncu": CONV_FP64_PIPE_NCU,
+                          "fp64_pipe_active_ncu": CONV_FP64_PIPE_NCU[args.conv],
                           "fp64_pipe_source": "ncu inst_executed_pipe_fp64 over active cycles, "
-                                              "one launch at 48x101x101x8 (fma kernel)",
+                                              "one launch of this kernel at 48x101x101x8",
                           "face_updates_per_step": int((p_faces + r_faces) * conv_substeps)},
         "autotune": tune,
         "clocks": clk.summary(),
@@ -528,7 +531,8 @@ FORMS = {
     # name: (local precision, FP64 refinement steps, convection arithmetic)
     "plain_fp64": ("fp64", 0, "exact"),
     "fp64_fma": ("fp64", 0, "fma"),
-    "mixed_fma": ("mixed", 2, "fma"),
+    "fp64_stream": ("fp64", 0, "stream"),
+    "mixed_stream": ("mixed", 2, "stream"),
     # the accuracy reference: FP64 factors and three FP64 refinement steps
     # (the plain LU itself carries kappa*eps64 ~ 1e-7 on these systems)
     "fp64_refined_exact": ("fp64", 3, "exact"),
@@ -936,7 +940,7 @@ def main():
     ap.add_argument("--graph", type=int, default=1, choices=[0, 1],
                     help="replay steady-state steps from a captured CUDA graph (1) or launch "
                          "them eagerly with per-phase events (0)")
-    ap.add_argument("--conv", default="fma", choices=["fma", "exact", "stream"],
+    ap.add_argument("--conv", default="stream", choices=["fma", "exact", "stream"],
                     help="convection kernel: fma (contracted), stream (one thread per line, contracted) or exact (bit-identical)")
     ap.add_argument("--trim", action="store_true",
                     help="ragged local systems: pitch angles outside the loss cone only")

@@ -140,38 +140,37 @@ CS_FN void fill_slots(const LineDesc& L)
 // differences t_k of the points k cells behind and k+1 cells ahead of face x).
 CS_FN double face_df(const double* w, double c)
 {
+    // factors of the even and odd difference pairs, each with the 1/2 of
+    // the even differences folded in: k3 (D2 + c/4 d3) = K3 ((2 D2) + c/2 d3)
     const double cs = c * c;
     const double q1 = cs - 1;
     const double p2 = q1 * (cs - 4);
     const double p3 = p2 * (cs - 9);
-    const double p4 = p3 * (cs - 16);
-    const double k3 = q1 * (1.0 / 6.0);
-    const double c6 = c * (1.0 / 6.0);
-    const double k5 = p2 * (1.0 / 120.0);
-    const double k7 = p3 * (1.0 / 5040.0);
-    const double k9 = p4 * (1.0 / 362880.0);
+    const double p4 = p2 * ((cs - 9) * (cs - 16));
+    const double K3 = q1 * (1.0 / 12.0);
+    const double K5 = p2 * (1.0 / 240.0);
+    const double K7 = p3 * (1.0 / 10080.0);
+    const double K9 = p4 * (1.0 / 725760.0);
     const double s0 = w[4] + w[5], t0 = w[4] - w[5];
     const double s1 = w[3] + w[6], t1 = w[3] - w[6];
     const double s2 = w[2] + w[7], t2 = w[2] - w[7];
     const double s3 = w[1] + w[8], t3 = w[1] - w[8];
     const double s4 = w[0] + w[9], t4 = w[0] - w[9];
-    const double D2 = (s1 - s0) * 0.5;
+    const double E2 = s1 - s0;                                      // 2 D2
     const double d3 = t1 - 3 * t0;
-    const double D4 = ((s2 - 3 * s1) + 2 * s0) * 0.5;
+    const double E4 = (s2 - 3 * s1) + 2 * s0;                      // 2 D4
     const double d5 = (t2 - 5 * t1) + 10 * t0;
-    const double D6 = ((s3 - 5 * s2) + (9 * s1 - 5 * s0)) * 0.5;
+    const double E6 = (s3 - 5 * s2) + (9 * s1 - 5 * s0);           // 2 D6
     const double d7 = (t3 - 7 * t2) + (21 * t1 - 35 * t0);
-    const double D8 = ((s4 - 7 * s3) + (20 * s2 - 28 * s1) + 14 * s0) * 0.5;
-    const double d9 = (t4 - 9 * t3) + (36 * t2 - 84 * t1) + 126 * t0;
-    double f = 0.5 * s0;
-    f += 0.5 * c * t0;
-    f += k3 * (D2 + c * 0.25 * d3);
-    f += k5 * (D4 + c6 * d5);
-    f += k7 * (D6 + c * 0.125 * d7);
+    const double E8 = (s4 - 7 * s3) + ((20 * s2 - 28 * s1) + 14 * s0);  // 2 D8
+    const double d9 = (t4 - 9 * t3) + ((36 * t2 - 84 * t1) + 126 * t0);
     // the ninth-order odd term carries 1/2 instead of |c|/2k: its sign follows
     // the direction explicitly (c = -0 counts as positive, as in :169)
-    f += k9 * (D8 + d9 * (c >= 0 ? 0.5 : -0.5));
-    return f;
+    const double g3 = K3 * (E2 + (c * 0.5) * d3);
+    const double g5 = K5 * (E4 + (c * (1.0 / 3.0)) * d5);
+    const double g7 = K7 * (E6 + (c * 0.25) * d7);
+    const double g9 = K9 * (E8 + (c >= 0 ? d9 : -d9));
+    return 0.5 * (s0 + c * t0) + ((g3 + g5) + (g7 + g9));
 }
 
 // Peak test of the unlimited line at four consecutive differences (a,b,c,d)
@@ -243,8 +242,8 @@ CS_FN void load_epi(const LineDesc& L, int epi, int c, bool checked, double& f1,
 // One step (local index j = b + s) of the pipeline.  `edge` (uniform over
 // the block) selects the boundary logic: reads past the thread's range,
 // rewrites at the line ends, stage ranges and store bounds.
-template <int U>
-CS_FN void step(const LineDesc& L, const StepRange& R, Win<U>& w, int b, int s, bool edge,
+template <int U, bool edge>
+CS_FN void step(const LineDesc& L, const StepRange& R, Win<U>& w, int b, int s,
                 const double (&PC)[U], const double (&P1)[U], const double (&P2)[U])
 {
     const int j = b + s;
@@ -381,30 +380,42 @@ CS_FN void stream_pass(const LineDesc& L, const StepRange& R, int epi)
     double PC[U];
 #pragma unroll
     for (int s = 0; s < U; s++) PC[s] = getC(L, R.jb + s);
-    for (int b = R.jb; b <= R.je; b += U) {
-        // fast: the front (cell j+4) stays inside the thread's range, cells
-        // and rewrites stay clear of the line ends, and the next block's
-        // Courant numbers lie inside the range too
-        const bool edge = !(b >= 8 && b + (2 * U > U + 4 ? 2 * U : U + 4) <= R.own_min);
-        double NC[U], P1[U], P2[U];
-        if (edge) {
+    // fast block: the front (cell j+4) stays inside the thread's range,
+    // cells and rewrites stay clear of the line ends, and the next block's
+    // Courant numbers lie inside the range too.  The fast blocks form one
+    // run in the middle of the pass; they run without any boundary logic.
+    auto fast = [&](int b) { return b >= 8 && b + (2 * U > U + 4 ? 2 * U : U + 4) <= R.own_min; };
+    int b = R.jb;
+    while (b <= R.je) {
+        if (fast(b)) {
+            do {
+                double NC[U], P1[U], P2[U];
+#pragma unroll
+                for (int s = 0; s < U; s++) {
+                    NC[s] = L.cr[(L.a + b + U + s) * L.crs];
+                    load_epi(L, epi, b + s - 7, false, P1[s], P2[s]);
+                }
+#pragma unroll
+                for (int s = 0; s < U; s++) step<U, false>(L, R, w, b, s, PC, P1, P2);
+                shift<U>(w);
+#pragma unroll
+                for (int s = 0; s < U; s++) PC[s] = NC[s];
+                b += U;
+            } while (b <= R.je && fast(b));
+        } else {
+            double NC[U], P1[U], P2[U];
 #pragma unroll
             for (int s = 0; s < U; s++) {
                 NC[s] = getC(L, b + U + s);
                 load_epi(L, epi, b + s - 7, true, P1[s], P2[s]);
             }
-        } else {
 #pragma unroll
-            for (int s = 0; s < U; s++) {
-                NC[s] = L.cr[(L.a + b + U + s) * L.crs];
-                load_epi(L, epi, b + s - 7, false, P1[s], P2[s]);
-            }
+            for (int s = 0; s < U; s++) step<U, true>(L, R, w, b, s, PC, P1, P2);
+            shift<U>(w);
+#pragma unroll
+            for (int s = 0; s < U; s++) PC[s] = NC[s];
+            b += U;
         }
-#pragma unroll
-        for (int s = 0; s < U; s++) step<U>(L, R, w, b, s, edge, PC, P1, P2);
-        shift<U>(w);
-#pragma unroll
-        for (int s = 0; s < U; s++) PC[s] = NC[s];
     }
 }
 

@@ -25,8 +25,6 @@
 // Compiled with multiply-add contraction: a step is within a few units in
 // the last place of the reference's (not bit-identical), like the contracted
 // form of convection.cu.
-#include <cstdlib>
-
 #include "conv_stream.cuh"
 #include "verb_internal.cuh"
 
@@ -328,23 +326,13 @@ __global__ void __launch_bounds__(CS_THREADS, CS_MINB) convection_stream_kernel(
     }
 }
 
-// Launch shapes (steps per unrolled block, resident CTAs per SM).
-struct CsShape {
-    void (*fn)(ConvArgs);
-    int minb;
-};
-
-CsShape cs_shape()
-{
-    const char* e = getenv("VERB_CS_VARIANT");
-    const int v = e ? atoi(e) : 0;
-    switch (v) {
-    case 1: return {convection_stream_kernel<4, 3>, 3};
-    case 2: return {convection_stream_kernel<6, 3>, 3};
-    case 3: return {convection_stream_kernel<4, 4>, 4};
-    default: return {convection_stream_kernel<2, 3>, 3};
-    }
-}
+// Launch shape: two steps per unrolled block and the registers capped for
+// three resident CTAs per SM (164 registers, no spills).  Measured at
+// 48x101x101x91: one step per block 175.5 ms, two 172.2 ms, three 215 ms,
+// four 270 ms per convection step (wider blocks need more live registers
+// and larger code); four CTAs per SM spill at 128 registers.
+constexpr int CS_U = 2;
+constexpr int CS_MINB = 3;
 
 }  // namespace
 
@@ -367,15 +355,15 @@ int conv_stream_ctas(int P, int R)
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const CsShape sh = cs_shape();
-    allow_max_dynamic_smem((const void*)sh.fn);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, sh.fn, CS_THREADS, cs_smem(P, R));
+    const auto fn = convection_stream_kernel<CS_U, CS_MINB>;
+    allow_max_dynamic_smem((const void*)fn);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, CS_THREADS, cs_smem(P, R));
     if (per < 1) per = 1;
-    if (per > sh.minb) per = sh.minb;
+    if (per > CS_MINB) per = CS_MINB;
     return sms * per;
 }
 
-// the most CTAs any launch shape runs (scratch is sized for it)
+// the most CTAs a launch runs (scratch is sized for it)
 int conv_stream_ctas_max(int P, int R)
 {
     int dev = 0, sms = 0;
@@ -383,14 +371,14 @@ int conv_stream_ctas_max(int P, int R)
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     (void)P;
     (void)R;
-    return sms * 4;
+    return sms * CS_MINB;
 }
 
 void launch_convection_stream(const ConvArgs& a, int nctas, cudaStream_t s)
 {
-    const CsShape sh = cs_shape();
-    allow_max_dynamic_smem((const void*)sh.fn);
-    sh.fn<<<nctas, CS_THREADS, cs_smem(a.d.P, a.d.R), s>>>(a);
+    const auto fn = convection_stream_kernel<CS_U, CS_MINB>;
+    allow_max_dynamic_smem((const void*)fn);
+    fn<<<nctas, CS_THREADS, cs_smem(a.d.P, a.d.R), s>>>(a);
 }
 
 }  // namespace verb
