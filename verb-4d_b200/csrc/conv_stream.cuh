@@ -244,14 +244,16 @@ CS_FN void load_epi(const LineDesc& L, int epi, int c, bool checked, double& f1,
 // rewrites at the line ends, stage ranges and store bounds.
 template <int U, bool edge>
 CS_FN void step(const LineDesc& L, const StepRange& R, Win<U>& w, int b, int s,
-                const double (&PC)[U], const double (&P1)[U], const double (&P2)[U])
+                const double (&PC)[U], const double (&P1)[U], const double (&P2)[U],
+                double* blk)
 {
+    // blk: cell b-7 of the line (fast blocks address the plane from it)
     const int j = b + s;
     const bool lo_end = L.a == 0, hi_end = L.a + L.own == L.n;
     // front: cell j+4
     double e;
     if (edge) e = (j + 4 < L.own + 9) ? getE(L, j + 4) : 0.0;
-    else e = L.pl[(L.a + j + 4) * L.st];
+    else e = blk[(s + 11) * L.st];
     w.E[11 + s] = e;
     w.C[5 + s] = PC[s];
     // unlimited face j
@@ -312,7 +314,11 @@ CS_FN void step(const LineDesc& L, const StepRange& R, Win<U>& w, int b, int s,
         }
         store = oj >= 0 && oj < L.own;
     }
-    if (store) L.pl[(L.a + oj) * L.st] = o * P1[s] + P2[s];
+    if (edge) {
+        if (store) L.pl[(L.a + oj) * L.st] = o * P1[s] + P2[s];
+    } else {
+        blk[s * L.st] = o * P1[s] + P2[s];
+    }
 }
 
 template <int U>
@@ -386,21 +392,35 @@ CS_FN void stream_pass(const LineDesc& L, const StepRange& R, int epi)
     // run in the middle of the pass; they run without any boundary logic.
     auto fast = [&](int b) { return b >= 8 && b + (2 * U > U + 4 ? 2 * U : U + 4) <= R.own_min; };
     int b = R.jb;
+    // one block of the fast run: Courant numbers of the next block and the
+    // epilogue factors of this one from running pointers, then the steps
+    auto fast_block = [&](const double*& cp, const double*& e1p, const double*& e2p, double*& bp) {
+        double NC[U], P1[U], P2[U];
+#pragma unroll
+        for (int s = 0; s < U; s++) {
+            NC[s] = cp[s * L.crs];
+            P1[s] = epi ? e1p[s * L.es] : 1.0;
+            P2[s] = epi == 2 ? e2p[s * L.es] : 0.0;
+        }
+#pragma unroll
+        for (int s = 0; s < U; s++) step<U, false>(L, R, w, b, s, PC, P1, P2, bp);
+        shift<U>(w);
+#pragma unroll
+        for (int s = 0; s < U; s++) PC[s] = NC[s];
+        b += U;
+        cp += U * L.crs;
+        e1p += U * L.es;
+        e2p += U * L.es;
+        bp += U * L.st;
+    };
     while (b <= R.je) {
         if (fast(b)) {
+            const double* cp = L.cr + (L.a + b + U) * L.crs;
+            const double* e1p = epi ? L.e1 + (L.a + b - 7) * L.es : nullptr;
+            const double* e2p = epi == 2 ? L.e2 + (L.a + b - 7) * L.es : nullptr;
+            double* bp = L.pl + (L.a + b - 7) * L.st;
             do {
-                double NC[U], P1[U], P2[U];
-#pragma unroll
-                for (int s = 0; s < U; s++) {
-                    NC[s] = L.cr[(L.a + b + U + s) * L.crs];
-                    load_epi(L, epi, b + s - 7, false, P1[s], P2[s]);
-                }
-#pragma unroll
-                for (int s = 0; s < U; s++) step<U, false>(L, R, w, b, s, PC, P1, P2);
-                shift<U>(w);
-#pragma unroll
-                for (int s = 0; s < U; s++) PC[s] = NC[s];
-                b += U;
+                fast_block(cp, e1p, e2p, bp);
             } while (b <= R.je && fast(b));
         } else {
             double NC[U], P1[U], P2[U];
@@ -410,7 +430,7 @@ CS_FN void stream_pass(const LineDesc& L, const StepRange& R, int epi)
                 load_epi(L, epi, b + s - 7, true, P1[s], P2[s]);
             }
 #pragma unroll
-            for (int s = 0; s < U; s++) step<U, true>(L, R, w, b, s, PC, P1, P2);
+            for (int s = 0; s < U; s++) step<U, true>(L, R, w, b, s, PC, P1, P2, nullptr);
             shift<U>(w);
 #pragma unroll
             for (int s = 0; s < U; s++) PC[s] = NC[s];
