@@ -792,6 +792,17 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+// cnt 16-byte chunks, cnt <= 32 * MAXT, by the 32 lanes of a warp: a fixed
+// number of predicated copies instead of a loop with a run-time trip count
+template <int MAXT>
+__device__ __forceinline__ void warp_copy16(void* dst, const void* src, int cnt, int lane)
+{
+#pragma unroll
+    for (int t = 0; t < MAXT; t++) {
+        const int c = lane + 32 * t;
+        if (c < cnt) cp_async16((char*)dst + 16 * c, (const char*)src + 16 * c);
+    }
+}
 template <int N>
 __device__ __forceinline__ void cp_wait()
 {
@@ -854,7 +865,7 @@ __global__ void __launch_bounds__(SOLVE_WARPS * 32) local_solve_kernel(LocalArgs
         if (col < n - 1) {
             T* dst = ring + (col % FWD_DEPTH) * klp;
             const T* src = Lf + (size_t)col * klp;
-            for (int c = lane; c < klp / VEC; c += 32) cp_async16(dst + VEC * c, src + VEC * c);
+            warp_copy16<FWD_WIN * 8 / 16 / 32>(dst, src, klp / VEC, lane);
         }
     };
     for (int c = 0; c < FWD_DEPTH; c++) {
@@ -909,7 +920,7 @@ __global__ void __launch_bounds__(SOLVE_WARPS * 32) local_solve_kernel(LocalArgs
         if (col >= 0) {
             T* dst = ring + ((n - 1 - col) % BWD_DEPTH) * kvp;
             const T* src = Uf + (size_t)col * kvp;
-            for (int c = lane; c < kvp / VEC; c += 32) cp_async16(dst + VEC * c, src + VEC * c);
+            warp_copy16<BWD_WIN * 8 / 16 / 32>(dst, src, kvp / VEC, lane);
         }
     };
     for (int c = 0; c < BWD_DEPTH; c++) {
@@ -994,7 +1005,7 @@ __global__ void __launch_bounds__(SOLVE_WARPS * 32, MINB) local_solve_rw_kernel(
         if (col < n - 1) {
             T* dst = ring + (col % FWD_DEPTH) * klp;
             const T* src = Lf + (size_t)col * klp;
-            for (int c = lane; c < klp / VEC; c += 32) cp_async16(dst + VEC * c, src + VEC * c);
+            warp_copy16<FWD_WIN * 8 / 16 / 32>(dst, src, klp / VEC, lane);
             if (lane == 0) {
                 double* st = &stage[col % FWD_DEPTH];
                 if (col + FWIN < n) cp_async8(st, &w[col + FWIN]);
@@ -1065,7 +1076,7 @@ __global__ void __launch_bounds__(SOLVE_WARPS * 32, MINB) local_solve_rw_kernel(
         if (col >= 0) {
             T* dst = ring + ((n - 1 - col) % BWD_DEPTH) * kvp;
             const T* src = Uf + (size_t)col * kvp;
-            for (int c = lane; c < kvp / VEC; c += 32) cp_async16(dst + VEC * c, src + VEC * c);
+            warp_copy16<BWD_WIN * 8 / 16 / 32>(dst, src, kvp / VEC, lane);
             if (lane == 0) {
                 double* st = &stage[(n - 1 - col) % BWD_DEPTH];
                 if (col - BWIN >= 0) cp_async8(st, &w[col - BWIN]);
