@@ -1001,22 +1001,24 @@ __global__ void __launch_bounds__(SOLVE_WARPS * 32, MINB) local_solve_rw_kernel(
     }
     // column col's multipliers, and b[col + FWIN] (which enters the window
     // when column col is done)
-    auto issue_L = [&](int col) {
+    // (slot: col mod FWD_DEPTH, kept as a running index by the caller)
+    auto issue_L = [&](int col, int slot) {
         if (col < n - 1) {
-            T* dst = ring + (col % FWD_DEPTH) * klp;
+            T* dst = ring + slot * klp;
             const T* src = Lf + (size_t)col * klp;
             warp_copy16<FWD_WIN * 8 / 16 / 32>(dst, src, klp / VEC, lane);
             if (lane == 0) {
-                double* st = &stage[col % FWD_DEPTH];
+                double* st = &stage[slot];
                 if (col + FWIN < n) cp_async8(st, &w[col + FWIN]);
                 else *st = 0.0;
             }
         }
     };
     for (int c = 0; c < FWD_DEPTH; c++) {
-        issue_L(c);
+        issue_L(c, c);
         cp_commit();
     }
+    int fslot = 0;  // j mod FWD_DEPTH
     int pv_cur = (lane < n) ? ip[lane] : 0;
     int pv_next = (32 + lane < n) ? ip[32 + lane] : 0;
     for (int j = 0; j < n - 1; j++) {
@@ -1029,20 +1031,22 @@ __global__ void __launch_bounds__(SOLVE_WARPS * 32, MINB) local_solve_rw_kernel(
         __syncwarp();
         const int lm = min(kl, n - 1 - j);
         const int l = __shfl_sync(0xffffffffu, pv_cur, j & 31);
-        const int sl = (l - j) >> 5;  // slot of position l in lane l & 31
-        double v = s[0];
-#pragma unroll
-        for (int m = 1; m < FS; m++) v = (sl == m) ? s[m] : v;
-        const double bl = __shfl_sync(0xffffffffu, v, l & 31);
         const double bj_old = __shfl_sync(0xffffffffu, s[0], j & 31);
-        const double bj = (l != j) ? bl : bj_old;
-        if (l != j && lane == (l & 31)) {
+        double bj = bj_old;
+        if (l != j) {  // the same for the whole warp: an interchange
+            const int sl = (l - j) >> 5;  // slot of position l in lane l & 31
+            double v = s[0];
 #pragma unroll
-            for (int m = 0; m < FS; m++)
-                if (sl == m) s[m] = bj_old;
+            for (int m = 1; m < FS; m++) v = (sl == m) ? s[m] : v;
+            bj = __shfl_sync(0xffffffffu, v, l & 31);
+            if (lane == (l & 31)) {
+#pragma unroll
+                for (int m = 0; m < FS; m++)
+                    if (sl == m) s[m] = bj_old;
+            }
         }
         if (bj != 0.0) {
-            const T* Lc = ring + (j % FWD_DEPTH) * klp;
+            const T* Lc = ring + fslot * klp;
             const double tmp = -bj;
             const int o = (lane - j) & 31;
 #pragma unroll
@@ -1055,11 +1059,12 @@ __global__ void __launch_bounds__(SOLVE_WARPS * 32, MINB) local_solve_rw_kernel(
             w[j] = bj;
 #pragma unroll
             for (int m = 0; m + 1 < FS; m++) s[m] = s[m + 1];
-            s[FS - 1] = stage[j % FWD_DEPTH];
+            s[FS - 1] = stage[fslot];
         }
         __syncwarp();
-        issue_L(j + FWD_DEPTH);
+        issue_L(j + FWD_DEPTH, fslot);
         cp_commit();
+        fslot = fslot + 1 == FWD_DEPTH ? 0 : fslot + 1;
     }
     cp_wait<0>();
     __syncwarp();
@@ -1072,26 +1077,28 @@ __global__ void __launch_bounds__(SOLVE_WARPS * 32, MINB) local_solve_rw_kernel(
         const int p = (n - 1) - ((n - 1 - lane) & 31) - 32 * m;
         s[m] = p >= 0 ? w[p] : 0.0;
     }
-    auto issue_U = [&](int col) {
+    // (slot: (n-1-col) mod BWD_DEPTH, kept as a running index by the caller)
+    auto issue_U = [&](int col, int slot) {
         if (col >= 0) {
-            T* dst = ring + ((n - 1 - col) % BWD_DEPTH) * kvp;
+            T* dst = ring + slot * kvp;
             const T* src = Uf + (size_t)col * kvp;
             warp_copy16<BWD_WIN * 8 / 16 / 32>(dst, src, kvp / VEC, lane);
             if (lane == 0) {
-                double* st = &stage[(n - 1 - col) % BWD_DEPTH];
+                double* st = &stage[slot];
                 if (col - BWIN >= 0) cp_async8(st, &w[col - BWIN]);
                 else *st = 0.0;
             }
         }
     };
     for (int c = 0; c < BWD_DEPTH; c++) {
-        issue_U(n - 1 - c);
+        issue_U(n - 1 - c, c);
         cp_commit();
     }
+    int bslot = 0;  // (n-1-j) mod BWD_DEPTH
     for (int j = n - 1; j >= 0; j--) {
         cp_wait<BWD_DEPTH - 1>();
         __syncwarp();
-        const T* Uc = ring + ((n - 1 - j) % BWD_DEPTH) * kvp;
+        const T* Uc = ring + bslot * kvp;
         double bj = __shfl_sync(0xffffffffu, s[0], j & 31);
         if (bj != 0.0) {
             bj = bj / (double)Uc[kv];
@@ -1107,11 +1114,12 @@ __global__ void __launch_bounds__(SOLVE_WARPS * 32, MINB) local_solve_rw_kernel(
             w[j] = bj;
 #pragma unroll
             for (int m = 0; m + 1 < BS; m++) s[m] = s[m + 1];
-            s[BS - 1] = stage[(n - 1 - j) % BWD_DEPTH];
+            s[BS - 1] = stage[bslot];
         }
         __syncwarp();
-        issue_U(j - BWD_DEPTH);
+        issue_U(j - BWD_DEPTH, bslot);
         cp_commit();
+        bslot = bslot + 1 == BWD_DEPTH ? 0 : bslot + 1;
     }
     cp_wait<0>();
 }
