@@ -1051,8 +1051,8 @@ __global__ void __launch_bounds__(SOLVE_WARPS * 32, MINB) local_solve_rw_kernel(
             const int o = (lane - j) & 31;
 #pragma unroll
             for (int m = 0; m < FS; m++) {
-                const int e = o + 32 * m - 1;  // position j + 1 + e
-                if (e >= 0 && e < lm) s[m] = s[m] + (double)Lc[e] * tmp;  // xGER in xGBTRS
+                const int e = o + 32 * m - 1;  // position j + 1 + e; 0 <= e < lm
+                if ((unsigned)e < (unsigned)lm) s[m] = s[m] + (double)Lc[e] * tmp;  // xGER in xGBTRS
             }
         }
         if (lane == (j & 31)) {
@@ -1103,10 +1103,11 @@ __global__ void __launch_bounds__(SOLVE_WARPS * 32, MINB) local_solve_rw_kernel(
         if (bj != 0.0) {
             bj = bj / (double)Uc[kv];
             const int o = (j - lane) & 31;
+            const unsigned dmax = (unsigned)min(kv, j);
 #pragma unroll
             for (int m = 0; m < BS; m++) {
-                const int d = o + 32 * m;  // position j - d
-                if (d >= 1 && d <= kv && d <= j)
+                const int d = o + 32 * m;  // position j - d; 1 <= d <= min(kv, j)
+                if ((unsigned)(d - 1) < dmax)
                     s[m] = s[m] - bj * (double)Uc[kv - d];  // xTBSV: X(I) - TEMP*A(L+I,J)
             }
         }
