@@ -202,6 +202,9 @@ CS_FN double limit_df(double f, double c, double em2, double em1, double e0, dou
     const double ref = ou + (oc - ou) * rcp_rn(ca);
     const double sg = rise ? 1.0 : -1.0;
     const double a = sg * f, lo = sg * oc, h1 = sg * ref, h2 = sg * od;
+    // fmax/fmin as selects: the same values unless the second operand is NaN
+    // (then the select keeps it where fmax/fmin would drop it); a NaN PSD is
+    // reported by the step's NaN check either way
     double t = a > lo ? a : lo;               // fmax(f, oc)
     const double hi = h1 < h2 ? h1 : h2;      // fmin(ref, od)
     t = t < hi ? t : hi;                      // fmin(., .)
