@@ -66,17 +66,6 @@ __device__ __forceinline__ double cs_block_max(double v, double* red)
     return m;
 }
 
-// One thread's passes over its line: the line's own CFL sub-cycles
-// (QUICKEST6.cpp:37-52), the epilogue on the last one only.
-template <int CS_U>
-__device__ __forceinline__ void run_line(LineDesc& D, const StepRange& rg, int ns, int epi)
-{
-    for (int k = 0; k < ns; k++) {
-        cstream::fill_slots(D);
-        cstream::stream_pass<CS_U>(D, rg, k == ns - 1 ? epi : 0);
-    }
-}
-
 // CS_U: steps per unrolled block; CS_MINB: resident CTAs per SM the
 // registers are capped for
 template <int CS_U, int CS_MINB>
@@ -235,88 +224,83 @@ __global__ void __launch_bounds__(CS_THREADS, CS_MINB) convection_stream_kernel(
         // the L sweep runs in segments when no L line sub-cycles on its own
         const bool seg = seg_shape && __syncthreads_and(tid >= P || nsR[tid] == 1);
 
-        for (int it = 0; it < num_steps; it++) {
-            // MLT sweep, stored times G
-            for (int iR = tid; iR < R - 1; iR += CS_THREADS) {
-                LineDesc D;
-                D.pl = S + iR;
+        // thread li's line of a sweep: P-line iR = li (stored times G), or
+        // R-line iP (in segments: iP = li mod P, segment li / P), stored as
+        // v exp(Loss dt)/G + S dt
+        auto line_desc = [&](bool pr, bool sg, int li) {
+            LineDesc D;
+            D.sl = slots + tid;
+            D.sls = CS_THREADS;
+            if (pr) {
+                D.pl = S + li;
                 D.st = Rs;
                 D.a = 0;
                 D.own = P;
                 D.n = P;
                 D.lt = a.Pl_t;
                 D.ut = a.Pu_t;
-                D.lbc = lnP[iR];
-                D.ubc = lnP[(R - 1) + iR];
-                D.dxl = lnP[2 * (R - 1) + iR];
-                D.dxu = lnP[3 * (R - 1) + iR];
-                D.cr = crP + iR;
+                D.lbc = lnP[li];
+                D.ubc = lnP[(R - 1) + li];
+                D.dxl = lnP[2 * (R - 1) + li];
+                D.dxu = lnP[3 * (R - 1) + li];
+                D.cr = crP + li;
                 D.crs = R - 1;
-                D.sl = slots + tid;
-                D.sls = CS_THREADS;
-                D.e1 = Gp + iR;
+                D.e1 = Gp + li;
                 D.e2 = nullptr;
                 D.es = R;
-                run_line<CS_U>(D, rgP, nsP[iR], 1);
+            } else {
+                const int iP = li < P ? li : li - P;
+                const bool hi = sg && li >= P;
+                D.pl = S + (size_t)iP * Rs;
+                D.st = 1;
+                D.a = hi ? m0 : 0;
+                D.own = sg ? (hi ? R - m0 : m0) : R;
+                D.n = R;
+                D.lt = a.Rl_t;
+                D.ut = a.Ru_t;
+                D.lbc = lnR[iP];
+                D.ubc = lnR[P + iP];
+                D.dxl = lnR[2 * P + iP];
+                D.dxu = lnR[3 * P + iP];
+                D.cr = crR + iP;
+                D.crs = P;
+                D.e1 = hqT + iP;
+                D.e2 = spT + iP;
+                D.es = P;
             }
-            for (int iP = tid - (R - 1); iP < P; iP += CS_THREADS) {
-                if (iP >= 0) S[iP * Rs + R - 1] = S[iP * Rs + R - 1] * Gp[(size_t)iP * R + R - 1];
-            }
-            __syncthreads();
-            // L sweep, stored as v exp(Loss dt)/G + S dt
-            if (seg) {
-                const bool act = tid < 2 * P;
-                LineDesc D;
-                if (act) {
-                    const int iP = tid < P ? tid : tid - P;
-                    const int sgi = tid < P ? 0 : 1;
-                    D.pl = S + (size_t)iP * Rs;
-                    D.st = 1;
-                    D.a = sgi ? m0 : 0;
-                    D.own = sgi ? R - m0 : m0;
-                    D.n = R;
-                    D.lt = a.Rl_t;
-                    D.ut = a.Ru_t;
-                    D.lbc = lnR[iP];
-                    D.ubc = lnR[P + iP];
-                    D.dxl = lnR[2 * P + iP];
-                    D.dxu = lnR[3 * P + iP];
-                    D.cr = crR + iP;
-                    D.crs = P;
-                    D.sl = slots + tid;
-                    D.sls = CS_THREADS;
-                    D.e1 = hqT + iP;
-                    D.e2 = spT + iP;
-                    D.es = P;
-                    cstream::fill_slots(D);
+            return D;
+        };
+        for (int it = 0; it < num_steps; it++) {
+            // the MLT sweep (ph 0) and the L sweep (ph 1) go through one call
+            // of the pass, so the kernel holds one copy of its code
+            for (int ph = 0; ph < 2; ph++) {
+                const bool pr = ph == 0;
+                const bool sg = !pr && seg;
+                const int nl = pr ? R - 1 : (sg ? 2 * P : P);
+                if (sg) {
+                    // each segment saves the cells of the other half it reads
+                    // before either half starts writing
+                    if (tid < nl) cstream::fill_slots(line_desc(false, true, tid));
+                    __syncthreads();
+                }
+                for (int li = tid; li < nl; li += CS_THREADS) {
+                    const LineDesc D = line_desc(pr, sg, li);
+                    const int ns = pr ? nsP[li] : (sg ? 1 : nsR[li]);
+                    const StepRange rg = pr ? rgP : (sg ? rgRs : rgRw);
+                    // the line's own CFL sub-cycles (QUICKEST6.cpp:37-52), the
+                    // epilogue on the last one only
+                    for (int k = 0; k < ns; k++) {
+                        if (!sg) cstream::fill_slots(D);
+                        cstream::stream_pass<CS_U>(D, rg, k == ns - 1 ? (pr ? 1 : 2) : 0);
+                    }
+                }
+                if (pr) {
+                    // the last L row, which the MLT sweep does not touch (:104)
+                    for (int iP = tid - (R - 1); iP < P; iP += CS_THREADS)
+                        if (iP >= 0) S[iP * Rs + R - 1] = S[iP * Rs + R - 1] * Gp[(size_t)iP * R + R - 1];
                 }
                 __syncthreads();
-                if (act) cstream::stream_pass<CS_U>(D, rgRs, 2);
-            } else {
-                for (int iP = tid; iP < P; iP += CS_THREADS) {
-                    LineDesc D;
-                    D.pl = S + (size_t)iP * Rs;
-                    D.st = 1;
-                    D.a = 0;
-                    D.own = R;
-                    D.n = R;
-                    D.lt = a.Rl_t;
-                    D.ut = a.Ru_t;
-                    D.lbc = lnR[iP];
-                    D.ubc = lnR[P + iP];
-                    D.dxl = lnR[2 * P + iP];
-                    D.dxu = lnR[3 * P + iP];
-                    D.cr = crR + iP;
-                    D.crs = P;
-                    D.sl = slots + tid;
-                    D.sls = CS_THREADS;
-                    D.e1 = hqT + iP;
-                    D.e2 = spT + iP;
-                    D.es = P;
-                    run_line<CS_U>(D, rgRw, nsR[iP], 2);
-                }
             }
-            __syncthreads();
         }
         for (int i = tid; i < PR; i += CS_THREADS) {
             const int iP = i / R, iR = i - iP * R;
@@ -327,7 +311,7 @@ __global__ void __launch_bounds__(CS_THREADS, CS_MINB) convection_stream_kernel(
 }
 
 // Launch shape: two steps per unrolled block and the registers capped for
-// three resident CTAs per SM (164 registers, no spills).  Measured at
+// three resident CTAs per SM (no spills).  Measured at
 // 48x101x101x91: one step per block 175.5 ms, two 172.2 ms, three 215 ms,
 // four 270 ms per convection step (wider blocks need more live registers
 // and larger code); four CTAs per SM spill at 128 registers.
