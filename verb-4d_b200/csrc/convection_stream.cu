@@ -9,13 +9,15 @@
 //   * MLT sweep: thread t streams P-line iR = t (R-1 lines); its final cells
 //     are stored already multiplied by G, which is the reference's PSD*G pass
 //     before the L sweep (:122-126); the last L row, which the MLT sweep does
-//     not touch (:104), is multiplied by the spare threads;
+//     not touch (:104), is multiplied by the threads once their lines are done;
 //   * L sweep: thread t streams half of R-line iP (two segments per line, so
 //     2P threads work; each saves the 9 cells of the other half it reads
 //     before the segments start writing), and stores the final cells as
 //     v * exp(Loss dt)/G + S dt (the epilogue of :126-165; S dt for interior
 //     L only).  Lines with their own CFL sub-cycles, and periodic L, run
 //     whole, one thread per line.
+// Both sweeps go through a single call of the pass: the kernel then holds one
+// copy of its (unrolled) code, which keeps it in the instruction cache.
 // Slice tables (face Courant numbers, G, exp(Loss dt)/G, S dt, boundary data)
 // are formed once per slice into a per-CTA region that stays in L2, laid out
 // line-fastest so that a sweep's loads are coalesced across its threads.
